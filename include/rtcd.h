@@ -1,0 +1,211 @@
+/*
+ * rtcd.h - C ABI of the B200 batched collision-query engine.
+ *
+ * The upstream RTCollisionDetection exposes a header-only C++ template API
+ * (RTCD::CollisionDetector<NSTREAM, LinkType>, RTCD/CollisionDetector/
+ * CollisionDetector.h:18-157) driven as
+ *     construct -> setupScene -> setupOptix -> setupRobot -> buildSBT ->
+ *     per query: robot->prepareUpdateData(poses, n); setNCheck(n); check();
+ *                downloadResult(result)
+ * (RTCD/Demo/DemoCollisionDetectorDisc.cpp:56-76).  This ABI carries the same
+ * objects - a robot, a resident scene, a detector of one of the four kinds -
+ * as opaque handles with plain pointers and sizes, so any language with a C
+ * FFI can bind it.  include/rtcd/CollisionDetector.hpp re-creates the upstream
+ * method names on top of it.
+ *
+ * Conventions
+ *  - Every call returns an rtcd_status; no exception crosses the ABI.
+ *    rtcd_last_error() returns the calling thread's last message.
+ *  - Outputs are caller-owned.  Handles own all device memory they allocate.
+ *  - A handle may be used from several threads; calls on one detector are
+ *    serialised by the detector.
+ *  - Units: metres, radians.  Transforms are 3x4 row-major [R | t].
+ */
+#ifndef RTCD_H
+#define RTCD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTCD_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RTCD_API __attribute__((visibility("default")))
+#else
+#define RTCD_API
+#endif
+
+typedef enum {
+    RTCD_OK = 0,
+    RTCD_ERR_INVALID_ARGUMENT = 1,
+    RTCD_ERR_CUDA = 2,
+    RTCD_ERR_OUT_OF_MEMORY = 3,
+    RTCD_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait ran out */
+    RTCD_ERR_CAPACITY = 5,       /* a structure exceeded a compiled limit */
+    RTCD_ERR_INTERNAL = 6
+} rtcd_status;
+
+/* The four detectors (upstream LinkType, RTCD/Meshes/meshTypes.h:37-48). */
+typedef enum {
+    RTCD_OBS_TO_ROBOT = 0, /* LinkType::MESH: obstacle edges vs link triangles */
+    RTCD_ROBOT_TO_OBS = 1, /* LinkType::RAY_ONLINE: link edges vs scene triangles */
+    RTCD_LINEAR_SWEEP = 2, /* LinkType::LINEAR_CURVE: obstacle edges vs swept capsules */
+    RTCD_QUAD_SWEEP = 3    /* LinkType::QUADRATIC_CURVE: obstacle edges vs quadratic B-spline sweeps */
+} rtcd_detector_kind;
+
+/* rtcd_check flags */
+#define RTCD_CHECK_COUNTS (1u << 0)        /* also produce the upstream hit counts (no early exit) */
+#define RTCD_CHECK_HOST_BUFFERS (1u << 1)  /* q, traj offsets and outputs are host memory */
+#define RTCD_CHECK_NO_CULL (1u << 2)       /* skip the OBB prefilter of the discrete detectors */
+#define RTCD_CHECK_PLAIN (1u << 3)         /* frame-by-frame path with a host sync per frame */
+#define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
+
+typedef struct rtcd_ctx rtcd_ctx;
+typedef struct rtcd_robot rtcd_robot;
+typedef struct rtcd_scene rtcd_scene;
+typedef struct rtcd_detector rtcd_detector;
+
+/* Serial-chain robot (upstream robotConfig + robot<DOF>, RTCD/Robot/robotConfig.h:14-38,
+ * RTCD/Robot/robot.h:91-124).  Link i (0 = fixed base) has transform
+ * T_0 = base_tf, T_{i+1} = T_i * (cos q_i C_i + sin q_i S_i + O_i). */
+typedef struct {
+    uint32_t dof;                      /* joints; the robot has dof + 1 links */
+    const float* base_tf;              /* 12 */
+    const float* cos_mask;             /* dof * 12 */
+    const float* sin_mask;             /* dof * 12 */
+    const float* one_mask;             /* dof * 12 */
+    const float* link_verts;           /* link-local xyz */
+    const uint32_t* link_vert_offsets; /* dof + 2 */
+    const uint32_t* link_tris;         /* per-link vertex indices */
+    const uint32_t* link_tri_offsets;  /* dof + 2 */
+    const uint32_t* link_edges;        /* optional; NULL: unique edges are extracted */
+    const uint32_t* link_edge_offsets; /* dof + 2 when link_edges is given */
+    const float* link_obbs;            /* optional 15 floats per link (centre, half sizes, x/y/z axes); NULL: PCA fit */
+    uint32_t n_spheres;                /* sphere model used by the sweep detectors */
+    const float* sphere_centers;       /* link-local xyz */
+    const float* sphere_radii;
+    const uint32_t* sphere_links;
+    int32_t skip_base;                 /* nonzero: link 0 is never checked (upstream SKIP_BASE) */
+} rtcd_robot_desc;
+
+typedef struct {
+    uint32_t frame_size; /* poses (or trajectories) per frame of the plain path; 0 = 64 */
+    uint32_t reserved[7];
+} rtcd_config;
+
+/* Replaces the OptiX context + streams of createContextStream
+ * (RTCD/Utils/Test/cudaCtxUtils.h:63-74). */
+RTCD_API rtcd_status rtcd_context_create(int device, rtcd_ctx** out);
+RTCD_API rtcd_status rtcd_context_destroy(rtcd_ctx* ctx);
+
+/* Replaces robot<DOF>(robotConfig) and the link GAS builds
+ * (RTCD/Robot/robot.h:91-124, RTCD/Robot/batchIASRobot.h:310-365): uploads
+ * the chain and builds one triangle and one edge LBVH per link. */
+RTCD_API rtcd_status rtcd_robot_create(rtcd_ctx* ctx, const rtcd_robot_desc* desc, rtcd_robot** out);
+RTCD_API rtcd_status rtcd_robot_destroy(rtcd_robot* robot);
+
+/* Replaces scene::addObstacle / uploadToDevice / wrapScene
+ * (RTCD/CollisionScenes/scene.h:60-147): obstacle i owns triangles
+ * [obstacle_tri_offsets[i], obstacle_tri_offsets[i+1]).  Builds the resident
+ * triangle and edge LBVHs, the unique obstacle edges and one PCA OBB per
+ * obstacle (RTCD/CollisionScenes/obstacle.h:186-219). */
+RTCD_API rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_verts, const uint32_t* tris,
+                              uint32_t n_tris, const uint32_t* obstacle_tri_offsets, uint32_t n_obstacles,
+                              rtcd_scene** out);
+RTCD_API rtcd_status rtcd_scene_destroy(rtcd_scene* scene);
+RTCD_API rtcd_status rtcd_scene_info(const rtcd_scene* scene, uint32_t* n_tris, uint32_t* n_edges, uint32_t* n_obstacles);
+
+/* Replaces CollisionDetector(ctx, streams, robot, scene) + setupScene +
+ * setupRobot + buildSBT (RTCD/CollisionDetector/CollisionDetector.h:166-305,
+ * :777-835).  config may be NULL. */
+RTCD_API rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_robot* robot, rtcd_scene* scene,
+                                 const rtcd_config* config, rtcd_detector** out);
+RTCD_API rtcd_status rtcd_detector_destroy(rtcd_detector* det);
+
+/*
+ * Replaces prepareUpdateData + setNCheck + check + downloadResult
+ * (RTCD/CollisionDetector/CCRobotWrapper.h:39-70,
+ *  RTCD/CollisionDetector/CollisionDetector.h:354-471, :62).
+ *
+ * Discrete kinds: q is float[n][dof]; flags_out[i] = 1 when pose i collides.
+ * Sweep kinds:    q is float[traj_offsets[n]][dof] waypoints; trajectory i
+ *                 owns rows [traj_offsets[i], traj_offsets[i+1]);
+ *                 flags_out[i] = 1 when trajectory i collides.  traj_offsets
+ *                 is always host memory.  seg_flags_out (optional) receives
+ *                 one flag per segment, laid out as rtcd_segment_offsets()
+ *                 describes.
+ * counts_out (optional, with RTCD_CHECK_COUNTS) receives the upstream hit
+ * counts: ObsToRobot - intersecting (obstacle edge, link, link triangle)
+ * triples; RobotToObs - link edges with at least one hit; sweeps -
+ * intersecting (obstacle edge, sphere segment) pairs.
+ *
+ * Without RTCD_CHECK_HOST_BUFFERS, q and the outputs are device pointers and
+ * the call is asynchronous on `stream` (a cudaStream_t; NULL = the
+ * detector's stream).  With it, the call copies through pinned staging
+ * buffers and returns after the results are in the host buffers.
+ */
+RTCD_API rtcd_status rtcd_check(rtcd_detector* det, const float* q, const uint32_t* traj_offsets, uint32_t n,
+                       uint8_t* flags_out, uint8_t* seg_flags_out, uint32_t* counts_out, uint32_t flags,
+                       void* stream);
+
+/* Waits for the detector's work and reports device-side errors
+ * (upstream final CUDA_SYNC_CHECK, CollisionDetector.h:470). */
+RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
+
+/* Segments per trajectory for the sweep kinds: linear n_wp - 1; quadratic
+ * max(3, ceil(n_wp/2)) - 2 (+2 start/end spheres unless RTCD_CHECK_NO_ENDPOINTS).
+ * offsets_out (n + 1 entries, host) is the exclusive prefix sum. */
+RTCD_API rtcd_status rtcd_segment_offsets(rtcd_detector_kind kind, const uint32_t* traj_offsets, uint32_t n, uint32_t flags,
+                                 uint32_t* offsets_out);
+
+/* Statistics of the last completed check: items after the cull, etc. */
+typedef struct {
+    uint64_t work_items;   /* (pose, link) items or sweep units processed */
+    uint64_t culled_items; /* items the OBB prefilter removed */
+    uint64_t fp64_retests; /* candidates re-tested in FP64 */
+    uint64_t reserved[5];
+} rtcd_stats;
+RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
+
+/* ---- building blocks, exposed for callers that compose their own pipelines ---- */
+
+/* Batched forward kinematics (upstream batchFkineAdj, RTCD/Robot/robot.cu:202-241;
+ * declared in RTCD/Robot/robot.cuh:10-46).  q_dev: float[n][dof] on the device;
+ * T_dev: float[n][dof+1][12] on the device, link transforms 3x4 row-major.
+ * Asynchronous on `stream` (NULL = the context stream). */
+RTCD_API rtcd_status rtcd_robot_fk(rtcd_robot* robot, const float* q_dev, uint32_t n, float* T_dev, void* stream);
+
+/* Exclusive scan of n uint32 (upstream exclusiveScan,
+ * RTCD/Utils/cuda/cudaAlgorithms.cuh:33-114).  Device pointers; in != out;
+ * total_dev (optional) receives the sum.  Asynchronous on `stream`. */
+RTCD_API rtcd_status rtcd_exclusive_scan_u32(rtcd_ctx* ctx, const uint32_t* in_dev, uint32_t* out_dev, uint32_t n,
+                                             uint32_t* total_dev, void* stream);
+
+/* Stable compaction of the indices of nonzero bytes (upstream streamCompact /
+ * compactCpy, RTCD/Utils/cuda/streamCompact.inl:12-89).  Device pointers;
+ * count_dev receives how many.  Asynchronous on `stream`. */
+RTCD_API rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
+                                          uint32_t* count_dev, void* stream);
+
+/* Canonical LBVH over n boxes (replaces optixAccelBuild, RTCD/Meshes/mesh.h:725-740).
+ * Host arrays: lo/hi float[n][3] in; codes_out[n] (sorted Morton codes),
+ * perm_out[n] (sorted position -> box), child_out[2(n-1)] (bit 31 set = leaf
+ * with sorted position, else internal node), node_lo/node_hi float[n-1][3]
+ * out (any output may be NULL).  *depth_out: longest root-leaf path.
+ * Synchronous. */
+RTCD_API rtcd_status rtcd_lbvh_build(rtcd_ctx* ctx, const float* lo, const float* hi, uint32_t n, uint32_t* codes_out,
+                                     uint32_t* perm_out, uint32_t* child_out, float* node_lo, float* node_hi,
+                                     uint32_t* depth_out);
+
+/* Thread-local message of the last failing call (empty when none). */
+RTCD_API rtcd_status rtcd_last_error(char* buf, size_t n);
+RTCD_API int rtcd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTCD_H */

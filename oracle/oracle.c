@@ -1,0 +1,915 @@
+/*
+ * oracle.c - FP64 CPU restatement of the RTCollisionDetection query path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the correctness checker for the
+ * CUDA detectors: only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline load it.  The product library never links or calls it.
+ *
+ * What it restates (upstream file:line):
+ *  - forward kinematics T_{i+1} = T_i * (cos q_i C_i + sin q_i S_i + O_i), base
+ *    transform T_0 (RTCD/Robot/robot.cu:202-231, affine product :34-47) - here
+ *    in double precision;
+ *  - unique undirected mesh edges in first-seen orientation
+ *    (RTCD/Meshes/mesh.h:200-216);
+ *  - ObsToRobot: every obstacle edge is a segment [v0, v1] tested against
+ *    every link triangle of every pose; the upstream any-hit program counts
+ *    every (edge, link instance, triangle) hit (RTCD/CollisionDetector/
+ *    CCCuda.cu:31-35, :56-77);
+ *  - RobotToObs: every link edge, moved to the world by its link transform,
+ *    is tested against the scene triangles; the upstream closest-hit path
+ *    counts one per hitting edge (RTCD/CollisionDetector/CCRay.cu:74-116);
+ *  - linear sweep: a sphere swept between consecutive waypoints is a capsule
+ *    (round end caps, RTCD/Robot/batchCurveRobot.h:230), hit by an obstacle
+ *    edge when their distance is <= r (solid semantics);
+ *  - quadratic sweep: control points C = W P with W = pinv(B), B the uniform
+ *    unclamped quadratic B-spline basis sampled at u = linspace(2, nC, nT)
+ *    (RTCD/Robot/sweptVolume.cu:22-83, weight tables RTCD/data/weights/quad/
+ *    normal/), segments of three consecutive control points
+ *    (RTCD/Robot/batchCurveRobot.h:49-51); a segment is hit when an obstacle
+ *    edge comes within r of the curve piece.  The start and end waypoint
+ *    spheres, which the upstream test adds from a separate sphere check
+ *    (RTCD/CollisionDetector/Test/testCollisionCheckerCurve.cpp:157-172), are
+ *    optional extra pieces.
+ *
+ * The upstream OBB prefilter (RTCD/CollisionDetector/BBCollisionDetection.cu:
+ * 4-37) is not applied: the oracle defines the truth the cull must preserve.
+ * A canonical LBVH (30-bit Morton codes of float centroids, stable sort by
+ * (code, index), Karras 2012 hierarchy, one primitive per leaf) accelerates the
+ * queries without changing any result; its float arithmetic is spelled out so
+ * the device builder can be compared with it bit for bit.
+ *
+ * epsilon band: a pose (segment, trajectory) is "in band" when no robust hit
+ * exists and some primitive pair lies within eps of flipping: a hit whose
+ * crossing point is within eps of the triangle boundary or whose segment
+ * endpoint is within eps of the triangle plane, a miss within distance eps,
+ * or a sweep distance within eps of the radius.  Flags must match the device
+ * detectors on every pose outside the band.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef unsigned int u32;
+
+/* ------------------------------------------------------------------ vectors */
+typedef struct { double x, y, z; } d3;
+static inline d3 v3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
+static inline d3 sub(d3 a, d3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline d3 add(d3 a, d3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline d3 mul(d3 a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
+static inline double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline d3 cross(d3 a, d3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline double len(d3 a) { return sqrt(dot(a, a)); }
+static inline double clamp01(double t) { return t < 0 ? 0 : (t > 1 ? 1 : t); }
+static inline d3 fv(const float* p) { return v3(p[0], p[1], p[2]); }
+
+/* affine 3x4 row-major */
+static inline d3 xform(const double* T, d3 p) {
+    return v3(T[0] * p.x + T[1] * p.y + T[2] * p.z + T[3], T[4] * p.x + T[5] * p.y + T[6] * p.z + T[7],
+              T[8] * p.x + T[9] * p.y + T[10] * p.z + T[11]);
+}
+static inline d3 xform_inv(const double* T, d3 p) { /* rigid inverse: R^T (p - t) */
+    d3 q = v3(p.x - T[3], p.y - T[7], p.z - T[11]);
+    return v3(T[0] * q.x + T[4] * q.y + T[8] * q.z, T[1] * q.x + T[5] * q.y + T[9] * q.z,
+              T[2] * q.x + T[6] * q.y + T[10] * q.z);
+}
+
+/* ---------------------------------------------------------------- kinematics */
+/* T[(dof+1)*12] for one pose: link 0 = base, link i+1 = T_i * L_i(q_i). */
+void orc_fk_pose(int dof, const float* cos_m, const float* sin_m, const float* one_m, const float* base,
+                 const float* q, double* T) {
+    for (int k = 0; k < 12; ++k) T[k] = base[k];
+    for (int i = 0; i < dof; ++i) {
+        double s = sin((double) q[i]), c = cos((double) q[i]);
+        double L[12];
+        for (int k = 0; k < 12; ++k)
+            L[k] = c * cos_m[i * 12 + k] + s * sin_m[i * 12 + k] + one_m[i * 12 + k];
+        const double* A = T + i * 12;
+        double* R = T + (i + 1) * 12;
+        for (int r = 0; r < 3; ++r) {
+            for (int col = 0; col < 4; ++col) {
+                double v = A[r * 4 + 0] * L[0 * 4 + col] + A[r * 4 + 1] * L[1 * 4 + col] + A[r * 4 + 2] * L[2 * 4 + col];
+                if (col == 3) v += A[r * 4 + 3];
+                R[r * 4 + col] = v;
+            }
+        }
+    }
+}
+
+void orc_fk(int dof, const float* cos_m, const float* sin_m, const float* one_m, const float* base, const float* q,
+            int n, double* T) {
+    for (int p = 0; p < n; ++p) orc_fk_pose(dof, cos_m, sin_m, one_m, base, q + (size_t) p * dof, T + (size_t) p * (dof + 1) * 12);
+}
+
+/* -------------------------------------------------------------- mesh edges */
+/* Unique undirected edges, first-seen orientation, triangles visited in order,
+ * edges of a triangle in order (v0v1, v1v2, v2v0).  Returns the edge count;
+ * `edges` must hold 3 * n_tris pairs. */
+typedef struct { u32 a, b, id; int used; } edge_slot;
+
+static uint64_t hash_pair(u32 a, u32 b) {
+    uint64_t k = ((uint64_t) a << 32) | b;
+    k ^= k >> 33; k *= 0xff51afd7ed558ccdULL; k ^= k >> 33; k *= 0xc4ceb9fe1a85ec53ULL; k ^= k >> 33;
+    return k;
+}
+
+int orc_unique_edges(const u32* tris, int n_tris, u32* edges) {
+    size_t cap = 1;
+    while (cap < (size_t) n_tris * 6 + 16) cap <<= 1;
+    edge_slot* tab = (edge_slot*) calloc(cap, sizeof(edge_slot));
+    if (!tab) return -1;
+    int ne = 0;
+    for (int t = 0; t < n_tris; ++t) {
+        for (int k = 0; k < 3; ++k) {
+            u32 a = tris[t * 3 + k], b = tris[t * 3 + (k + 1) % 3];
+            u32 lo = a < b ? a : b, hi = a < b ? b : a;
+            size_t h = hash_pair(lo, hi) & (cap - 1);
+            int found = 0;
+            while (tab[h].used) {
+                if (tab[h].a == lo && tab[h].b == hi) { found = 1; break; }
+                h = (h + 1) & (cap - 1);
+            }
+            if (!found) {
+                tab[h].used = 1; tab[h].a = lo; tab[h].b = hi;
+                edges[2 * ne] = a; edges[2 * ne + 1] = b;
+                ++ne;
+            }
+        }
+    }
+    free(tab);
+    return ne;
+}
+
+/* ------------------------------------------------------------ canonical LBVH */
+static u32 expand_bits(u32 v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+static u32 quantize(float c, float lo, float ext) {
+    float t = ext > 0.0f ? (c - lo) / ext : 0.0f;
+    float v = t * 1024.0f;
+    if (!(v >= 0.0f)) v = 0.0f;
+    u32 q = (u32) floorf(v);
+    return q > 1023u ? 1023u : q;
+}
+
+typedef struct { u32 code, idx; } key_t2;
+static int key_cmp(const void* a, const void* b) {
+    const key_t2* x = (const key_t2*) a; const key_t2* y = (const key_t2*) b;
+    if (x->code != y->code) return x->code < y->code ? -1 : 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+static int delta(const u32* codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    u32 x = codes[i] ^ codes[j];
+    if (x) return __builtin_clz(x);
+    return 32 + __builtin_clz((u32) i ^ (u32) j);
+}
+
+/* BVH over n primitive boxes (plo/phi: n*3 floats).
+ * Outputs: codes[n] (sorted), perm[n] (sorted position -> primitive),
+ * child[2*(n-1)] (>=0 internal node, <0 leaf ~sorted position),
+ * node_lo/node_hi[(n-1)*3] internal node boxes.  Returns 0 on success. */
+int orc_lbvh_build(const float* plo, const float* phi, int n, u32* codes_out, u32* perm, int* child, float* node_lo,
+                   float* node_hi) {
+    if (n <= 0) return 0;
+    float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float* cen = (float*) malloc(sizeof(float) * 3 * (size_t) n);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            float c = 0.5f * (plo[i * 3 + k] + phi[i * 3 + k]);
+            cen[i * 3 + k] = c;
+            if (c < clo[k]) clo[k] = c;
+            if (c > chi[k]) chi[k] = c;
+        }
+    float ext[3] = {chi[0] - clo[0], chi[1] - clo[1], chi[2] - clo[2]};
+    key_t2* keys = (key_t2*) malloc(sizeof(key_t2) * (size_t) n);
+    for (int i = 0; i < n; ++i) {
+        u32 qx = quantize(cen[i * 3 + 0], clo[0], ext[0]);
+        u32 qy = quantize(cen[i * 3 + 1], clo[1], ext[1]);
+        u32 qz = quantize(cen[i * 3 + 2], clo[2], ext[2]);
+        keys[i].code = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
+        keys[i].idx = (u32) i;
+    }
+    qsort(keys, (size_t) n, sizeof(key_t2), key_cmp);
+    u32* codes = codes_out;
+    for (int i = 0; i < n; ++i) { codes[i] = keys[i].code; perm[i] = keys[i].idx; }
+    free(keys);
+    free(cen);
+    if (n == 1) return 0;
+    int* parent = (int*) malloc(sizeof(int) * (size_t) (2 * n));  /* internal 0..n-2, leaves n-1+s */
+    for (int i = 0; i < n - 1; ++i) {
+        int d = (delta(codes, n, i, i + 1) - delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+        int dmin = delta(codes, n, i, i - d);
+        int lmax = 2;
+        while (delta(codes, n, i, i + lmax * d) > dmin) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = delta(codes, n, i, j);
+        int s = 0;
+        for (int div = 2;; div *= 2) {
+            int t = (l + div - 1) / div;
+            if (delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+            if (t <= 1) break;
+        }
+        int g = i + s * d + (d < 0 ? -1 : 0);
+        int lo = i < j ? i : j, hi = i < j ? j : i;
+        int left = (lo == g) ? ~g : g;
+        int right = (hi == g + 1) ? ~(g + 1) : g + 1;
+        child[2 * i] = left;
+        child[2 * i + 1] = right;
+        parent[left >= 0 ? left : (n - 1 + ~left)] = i;
+        parent[right >= 0 ? right : (n - 1 + ~right)] = i;
+    }
+    /* bottom-up boxes: post-order over the tree with an explicit stack */
+    int* stack = (int*) malloc(sizeof(int) * (size_t) (2 * n + 4));
+    char* done = (char*) calloc((size_t) n, 1);
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        int nd = stack[sp - 1];
+        int ready = 1;
+        for (int c = 0; c < 2; ++c) {
+            int ch = child[2 * nd + c];
+            if (ch >= 0 && !done[ch]) { stack[sp++] = ch; ready = 0; }
+        }
+        if (!ready) continue;
+        --sp;
+        for (int k = 0; k < 3; ++k) { node_lo[nd * 3 + k] = INFINITY; node_hi[nd * 3 + k] = -INFINITY; }
+        for (int c = 0; c < 2; ++c) {
+            int ch = child[2 * nd + c];
+            const float *lo, *hi;
+            if (ch >= 0) { lo = node_lo + ch * 3; hi = node_hi + ch * 3; }
+            else { u32 pr = perm[~ch]; lo = plo + pr * 3; hi = phi + pr * 3; }
+            for (int k = 0; k < 3; ++k) {
+                if (lo[k] < node_lo[nd * 3 + k]) node_lo[nd * 3 + k] = lo[k];
+                if (hi[k] > node_hi[nd * 3 + k]) node_hi[nd * 3 + k] = hi[k];
+            }
+        }
+        done[nd] = 1;
+    }
+    free(done);
+    free(stack);
+    free(parent);
+    return 0;
+}
+
+/* a BVH with its primitive boxes, for queries */
+typedef struct {
+    int n;
+    float *plo, *phi;
+    u32 *codes, *perm;
+    int* child;
+    float *nlo, *nhi;
+} bvh_t;
+
+static void bvh_free(bvh_t* b) {
+    free(b->plo); free(b->phi); free(b->codes); free(b->perm); free(b->child); free(b->nlo); free(b->nhi);
+    memset(b, 0, sizeof(*b));
+}
+
+static void bvh_make(bvh_t* b, int n, float* plo, float* phi) {
+    b->n = n; b->plo = plo; b->phi = phi;
+    b->codes = (u32*) malloc(sizeof(u32) * (size_t) (n > 0 ? n : 1));
+    b->perm = (u32*) malloc(sizeof(u32) * (size_t) (n > 0 ? n : 1));
+    b->child = (int*) malloc(sizeof(int) * (size_t) (2 * (n > 1 ? n : 1)));
+    b->nlo = (float*) malloc(sizeof(float) * 3 * (size_t) (n > 1 ? n : 1));
+    b->nhi = (float*) malloc(sizeof(float) * 3 * (size_t) (n > 1 ? n : 1));
+    orc_lbvh_build(plo, phi, n, b->codes, b->perm, b->child, b->nlo, b->nhi);
+}
+
+static int box_hit(const float* lo, const float* hi, const double* qlo, const double* qhi) {
+    return !(qlo[0] > hi[0] || qhi[0] < lo[0] || qlo[1] > hi[1] || qhi[1] < lo[1] || qlo[2] > hi[2] || qhi[2] < lo[2]);
+}
+
+/* visits every primitive whose box overlaps [qlo, qhi]; returns #nodes tested */
+typedef int (*visit_fn)(void* ctx, u32 prim);  /* nonzero return stops the query */
+
+static uint64_t bvh_query(const bvh_t* b, const double* qlo, const double* qhi, visit_fn fn, void* ctx) {
+    if (b->n <= 0) return 0;
+    uint64_t tests = 0;
+    if (b->n == 1) {
+        ++tests;
+        if (box_hit(b->plo, b->phi, qlo, qhi)) fn(ctx, b->perm[0]);
+        return tests;
+    }
+    int stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        int nd = stack[--sp];
+        for (int c = 0; c < 2; ++c) {
+            int ch = b->child[2 * nd + c];
+            ++tests;
+            if (ch >= 0) {
+                if (box_hit(b->nlo + ch * 3, b->nhi + ch * 3, qlo, qhi)) stack[sp++] = ch;
+            } else {
+                u32 pr = b->perm[~ch];
+                if (box_hit(b->plo + pr * 3, b->phi + pr * 3, qlo, qhi))
+                    if (fn(ctx, pr)) return tests;
+            }
+        }
+    }
+    return tests;
+}
+
+/* ----------------------------------------------------------- distances */
+static double pt_seg2(d3 p, d3 a, d3 b) {
+    d3 ab = sub(b, a);
+    double L = dot(ab, ab);
+    double t = L > 0 ? clamp01(dot(sub(p, a), ab) / L) : 0.0;
+    d3 c = add(a, mul(ab, t));
+    d3 d = sub(p, c);
+    return dot(d, d);
+}
+
+/* squared distance between segments p1q1 and p2q2 (Ericson, RTCD 5.1.9) */
+static double seg_seg2(d3 p1, d3 q1, d3 p2, d3 q2) {
+    d3 d1 = sub(q1, p1), d2 = sub(q2, p2), r = sub(p1, p2);
+    double a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    double s, t;
+    if (a <= 1e-300 && e <= 1e-300) return dot(r, r);
+    if (a <= 1e-300) { s = 0; t = clamp01(f / e); }
+    else {
+        double c = dot(d1, r);
+        if (e <= 1e-300) { t = 0; s = clamp01(-c / a); }
+        else {
+            double b = dot(d1, d2), den = a * e - b * b;
+            s = den > 0 ? clamp01((b * f - c * e) / den) : 0.0;
+            t = (b * s + f) / e;
+            if (t < 0) { t = 0; s = clamp01(-c / a); }
+            else if (t > 1) { t = 1; s = clamp01((b - c) / a); }
+        }
+    }
+    d3 c1 = add(p1, mul(d1, s)), c2 = add(p2, mul(d2, t));
+    d3 d = sub(c1, c2);
+    return dot(d, d);
+}
+
+/* squared distance from p to triangle abc (Ericson 5.1.5), degenerate-safe */
+static double pt_tri2(d3 p, d3 a, d3 b, d3 c) {
+    d3 ab = sub(b, a), ac = sub(c, a);
+    d3 n = cross(ab, ac);
+    double nn = dot(n, n);
+    double scale = dot(ab, ab) * dot(ac, ac);
+    if (!(nn > 1e-24 * scale) || nn <= 0) {
+        double d = pt_seg2(p, a, b), e = pt_seg2(p, b, c), f = pt_seg2(p, c, a);
+        return d < e ? (d < f ? d : f) : (e < f ? e : f);
+    }
+    d3 ap = sub(p, a);
+    double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0 && d2 <= 0) return dot(ap, ap);
+    d3 bp = sub(p, b);
+    double d3_ = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3_ >= 0 && d4 <= d3_) return dot(bp, bp);
+    double vc = d1 * d4 - d3_ * d2;
+    if (vc <= 0 && d1 >= 0 && d3_ <= 0) { double v = d1 / (d1 - d3_); d3 q = sub(p, add(a, mul(ab, v))); return dot(q, q); }
+    d3 cp = sub(p, c);
+    double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0 && d5 <= d6) return dot(cp, cp);
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0) { double w = d2 / (d2 - d6); d3 q = sub(p, add(a, mul(ac, w))); return dot(q, q); }
+    double va = d3_ * d6 - d5 * d4;
+    if (va <= 0 && (d4 - d3_) >= 0 && (d5 - d6) >= 0) {
+        double w = (d4 - d3_) / ((d4 - d3_) + (d5 - d6));
+        d3 q = sub(p, add(b, mul(sub(c, b), w)));
+        return dot(q, q);
+    }
+    double dn = 1.0 / (va + vb + vc);
+    double v = vb * dn, w = vc * dn;
+    d3 q = sub(p, add(a, add(mul(ab, v), mul(ac, w))));
+    return dot(q, q);
+}
+
+/*
+ * Segment pq vs triangle abc.  Returns 1 when the closed segment properly
+ * crosses the triangle (through its plane, crossing point inside the closed
+ * triangle) or touches it; *m receives the robustness margin of a hit (the
+ * smallest of: endpoint distances to the plane, in-plane distance of the
+ * crossing point to the three edge lines) or the distance of a miss.
+ */
+static int seg_tri(d3 p, d3 q, d3 a, d3 b, d3 c, double* m) {
+    d3 n = cross(sub(b, a), sub(c, a));
+    double nl = len(n);
+    if (nl > 0) {
+        double dp = dot(n, sub(p, a)) / nl, dq = dot(n, sub(q, a)) / nl;
+        if ((dp > 0 && dq < 0) || (dp < 0 && dq > 0) || (dp == 0) != (dq == 0)) {
+            double t = dp / (dp - dq);
+            d3 x = add(p, mul(sub(q, p), t));
+            d3 nu = mul(n, 1.0 / nl);
+            /* signed in-plane distances of x to the three edge lines (positive inside) */
+            d3 e0 = sub(b, a), e1 = sub(c, b), e2 = sub(a, c);
+            double l0 = len(e0), l1 = len(e1), l2 = len(e2);
+            if (l0 > 0 && l1 > 0 && l2 > 0) {
+                double s0 = dot(cross(e0, sub(x, a)), nu) / l0;
+                double s1 = dot(cross(e1, sub(x, b)), nu) / l1;
+                double s2 = dot(cross(e2, sub(x, c)), nu) / l2;
+                if (s0 >= 0 && s1 >= 0 && s2 >= 0) {
+                    double mm = fabs(dp);
+                    if (fabs(dq) < mm) mm = fabs(dq);
+                    if (s0 < mm) mm = s0;
+                    if (s1 < mm) mm = s1;
+                    if (s2 < mm) mm = s2;
+                    *m = mm;
+                    return 1;
+                }
+            }
+        }
+    }
+    /* no proper crossing: distance from the boundary features */
+    double d = pt_tri2(p, a, b, c), t;
+    if ((t = pt_tri2(q, a, b, c)) < d) d = t;
+    if ((t = seg_seg2(p, q, a, b)) < d) d = t;
+    if ((t = seg_seg2(p, q, b, c)) < d) d = t;
+    if ((t = seg_seg2(p, q, c, a)) < d) d = t;
+    d = sqrt(d);
+    if (d <= 1e-12) { *m = 0.0; return 1; }  /* touching (to rounding): a hit with zero margin */
+    *m = d;
+    return 0;
+}
+
+/* --------------------------------------------------------------- thread pool */
+typedef struct {
+    int n;
+    int next;
+    pthread_mutex_t mu;
+    void (*work)(void* ctx, int i, void* scratch);
+    void* ctx;
+    size_t scratch_bytes;
+} pool_t;
+
+static void* pool_main(void* arg) {
+    pool_t* p = (pool_t*) arg;
+    void* scratch = p->scratch_bytes ? malloc(p->scratch_bytes) : NULL;
+    for (;;) {
+        pthread_mutex_lock(&p->mu);
+        int i = p->next++;
+        pthread_mutex_unlock(&p->mu);
+        if (i >= p->n) break;
+        p->work(p->ctx, i, scratch);
+    }
+    free(scratch);
+    return NULL;
+}
+
+static void run_pool(int n, int threads, void (*work)(void*, int, void*), void* ctx, size_t scratch_bytes) {
+    pool_t p;
+    p.n = n; p.next = 0; p.work = work; p.ctx = ctx; p.scratch_bytes = scratch_bytes;
+    pthread_mutex_init(&p.mu, NULL);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    pthread_t th[256];
+    for (int t = 0; t < threads; ++t) pthread_create(&th[t], NULL, pool_main, &p);
+    for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
+    pthread_mutex_destroy(&p.mu);
+}
+
+/* ---------------------------------------------------------------- robot/scene */
+typedef struct {
+    int dof;
+    const float *cos_mask, *sin_mask, *one_mask, *base_tf;
+    int n_links;
+    const float* link_verts;
+    const u32 *link_vert_off, *link_tris, *link_tri_off, *link_edges, *link_edge_off;
+    int skip_base;
+    int n_spheres;
+    const float *sphere_centers, *sphere_radii;
+    const u32* sphere_links;
+} orc_robot;
+
+typedef struct {
+    int n_verts;
+    const float* verts;
+    int n_tris;
+    const u32* tris;
+    int n_edges;
+    const u32* edges;
+} orc_scene;
+
+typedef struct {
+    uint64_t node_tests;  /* BVH child-box tests */
+    uint64_t prim_tests;  /* exact primitive tests */
+} orc_work;
+
+static void tri_boxes(const float* verts, const u32* tris, int n, float** lo, float** hi) {
+    *lo = (float*) malloc(sizeof(float) * 3 * (size_t) (n ? n : 1));
+    *hi = (float*) malloc(sizeof(float) * 3 * (size_t) (n ? n : 1));
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            float a = verts[tris[i * 3] * 3 + k], b = verts[tris[i * 3 + 1] * 3 + k], c = verts[tris[i * 3 + 2] * 3 + k];
+            (*lo)[i * 3 + k] = fminf(a, fminf(b, c));
+            (*hi)[i * 3 + k] = fmaxf(a, fmaxf(b, c));
+        }
+}
+
+static void edge_boxes(const float* verts, const u32* edges, int n, float** lo, float** hi) {
+    *lo = (float*) malloc(sizeof(float) * 3 * (size_t) (n ? n : 1));
+    *hi = (float*) malloc(sizeof(float) * 3 * (size_t) (n ? n : 1));
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            float a = verts[edges[i * 2] * 3 + k], b = verts[edges[i * 2 + 1] * 3 + k];
+            (*lo)[i * 3 + k] = fminf(a, b);
+            (*hi)[i * 3 + k] = fmaxf(a, b);
+        }
+}
+
+/* ------------------------------------------------------------ discrete check */
+enum { ORC_OBS_TO_ROBOT = 0, ORC_ROBOT_TO_OBS = 1 };
+
+typedef struct {
+    int kind;
+    const orc_robot* R;
+    const orc_scene* S;
+    const float* q;
+    double eps;
+    bvh_t scene_tri, scene_edge;
+    bvh_t* link_tri;
+    unsigned char *hit, *band, *marg;
+    u32* count;
+    orc_work* work;  /* per pose, optional */
+} disc_ctx;
+
+typedef struct {
+    /* query-local state */
+    d3 p, q;        /* segment, in the frame of the target triangles */
+    const float* tv; const u32* tt; /* target triangle verts / indices */
+    const double* T;  /* transform from target-local to world, or NULL */
+    double eps;
+    int any_hit, robust, marginal;
+    u32 hits;
+    uint64_t prim_tests;
+} seg_query;
+
+static int visit_tri(void* vctx, u32 t) {
+    seg_query* s = (seg_query*) vctx;
+    const u32* ix = s->tt + (size_t) t * 3;
+    d3 a = fv(s->tv + ix[0] * 3), b = fv(s->tv + ix[1] * 3), c = fv(s->tv + ix[2] * 3);
+    if (s->T) { a = xform(s->T, a); b = xform(s->T, b); c = xform(s->T, c); }
+    double m;
+    ++s->prim_tests;
+    int h = seg_tri(s->p, s->q, a, b, c, &m);
+    if (h) {
+        s->any_hit = 1;
+        s->hits++;
+        if (m > s->eps) s->robust = 1; else s->marginal = 1;
+    } else if (m <= s->eps) {
+        s->marginal = 1;
+    }
+    return 0;
+}
+
+static void disc_pose(void* vctx, int pose, void* scratch) {
+    (void) scratch;
+    disc_ctx* C = (disc_ctx*) vctx;
+    const orc_robot* R = C->R;
+    const orc_scene* S = C->S;
+    double T[9 * 12];
+    double* Tp = (C->R->dof + 1) * 12 <= 9 * 12 ? T : (double*) malloc(sizeof(double) * (size_t) (R->dof + 1) * 12);
+    orc_fk_pose(R->dof, R->cos_mask, R->sin_mask, R->one_mask, R->base_tf, C->q + (size_t) pose * R->dof, Tp);
+    int any = 0, robust = 0, marginal = 0;
+    u32 count = 0;
+    uint64_t ntests = 0, ptests = 0;
+    double eps = C->eps;
+    for (int l = R->skip_base ? 1 : 0; l < R->n_links; ++l) {
+        const double* TL = Tp + l * 12;
+        const float* lv = R->link_verts + (size_t) R->link_vert_off[l] * 3;
+        if (C->kind == ORC_ROBOT_TO_OBS) {
+            /* every link edge, moved to the world, against the scene triangles */
+            u32 e0 = R->link_edge_off[l], e1 = R->link_edge_off[l + 1];
+            for (u32 e = e0; e < e1; ++e) {
+                seg_query s;
+                memset(&s, 0, sizeof(s));
+                s.p = xform(TL, fv(lv + R->link_edges[e * 2] * 3));
+                s.q = xform(TL, fv(lv + R->link_edges[e * 2 + 1] * 3));
+                s.tv = S->verts; s.tt = S->tris; s.T = NULL; s.eps = eps;
+                double qlo[3] = {fmin(s.p.x, s.q.x) - eps, fmin(s.p.y, s.q.y) - eps, fmin(s.p.z, s.q.z) - eps};
+                double qhi[3] = {fmax(s.p.x, s.q.x) + eps, fmax(s.p.y, s.q.y) + eps, fmax(s.p.z, s.q.z) + eps};
+                ntests += bvh_query(&C->scene_tri, qlo, qhi, visit_tri, &s);
+                ptests += s.prim_tests;
+                if (s.any_hit) { any = 1; ++count; }
+                robust |= s.robust; marginal |= s.marginal;
+            }
+        } else {
+            /* every obstacle edge, moved into the link frame, against the link triangles */
+            const u32* lt = R->link_tris + (size_t) R->link_tri_off[l] * 3;
+            for (int e = 0; e < S->n_edges; ++e) {
+                d3 pw = fv(S->verts + S->edges[e * 2] * 3), qw = fv(S->verts + S->edges[e * 2 + 1] * 3);
+                seg_query s;
+                memset(&s, 0, sizeof(s));
+                s.p = xform_inv(TL, pw);
+                s.q = xform_inv(TL, qw);
+                s.tv = lv; s.tt = lt; s.T = NULL; s.eps = eps;
+                double qlo[3] = {fmin(s.p.x, s.q.x) - eps, fmin(s.p.y, s.q.y) - eps, fmin(s.p.z, s.q.z) - eps};
+                double qhi[3] = {fmax(s.p.x, s.q.x) + eps, fmax(s.p.y, s.q.y) + eps, fmax(s.p.z, s.q.z) + eps};
+                ntests += bvh_query(&C->link_tri[l], qlo, qhi, visit_tri, &s);
+                ptests += s.prim_tests;
+                if (s.any_hit) { any = 1; count += s.hits; }
+                robust |= s.robust; marginal |= s.marginal;
+            }
+        }
+    }
+    if (Tp != T) free(Tp);
+    C->hit[pose] = (unsigned char) any;
+    if (C->count) C->count[pose] = count;
+    if (C->band) C->band[pose] = (unsigned char) (!robust && marginal);
+    if (C->marg) C->marg[pose] = (unsigned char) marginal;
+    if (C->work) { C->work[pose].node_tests = ntests; C->work[pose].prim_tests = ptests; }
+}
+
+int orc_discrete(int kind, const orc_robot* R, const orc_scene* S, const float* q, int n, double eps, int threads,
+                 unsigned char* hit, u32* count, unsigned char* band, unsigned char* marg, orc_work* work) {
+    disc_ctx C;
+    memset(&C, 0, sizeof(C));
+    C.kind = kind; C.R = R; C.S = S; C.q = q; C.eps = eps;
+    C.hit = hit; C.count = count; C.band = band; C.marg = marg; C.work = work;
+    float *lo, *hi;
+    if (kind == ORC_ROBOT_TO_OBS) {
+        tri_boxes(S->verts, S->tris, S->n_tris, &lo, &hi);
+        bvh_make(&C.scene_tri, S->n_tris, lo, hi);
+    } else {
+        C.link_tri = (bvh_t*) calloc((size_t) R->n_links, sizeof(bvh_t));
+        for (int l = 0; l < R->n_links; ++l) {
+            int nt = (int) (R->link_tri_off[l + 1] - R->link_tri_off[l]);
+            tri_boxes(R->link_verts + (size_t) R->link_vert_off[l] * 3, R->link_tris + (size_t) R->link_tri_off[l] * 3, nt,
+                      &lo, &hi);
+            bvh_make(&C.link_tri[l], nt, lo, hi);
+        }
+    }
+    run_pool(n, threads, disc_pose, &C, 0);
+    if (kind == ORC_ROBOT_TO_OBS) bvh_free(&C.scene_tri);
+    else {
+        for (int l = 0; l < R->n_links; ++l) bvh_free(&C.link_tri[l]);
+        free(C.link_tri);
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------- sweep checks */
+typedef struct {
+    d3 a, b;        /* capsule axis (linear) */
+    d3 B0, B1, B2;  /* quadratic Bezier piece */
+    int quad;
+    double r, eps;
+    const float* sv; const u32* se;  /* scene verts / edges */
+    int any_hit, robust, marginal;
+    u32 hits;
+    uint64_t prim_tests;
+} sweep_query;
+
+/* classify d (distance) against radius r with band eps */
+static void classify(sweep_query* s, double d) {
+    if (d <= s->r) { s->any_hit = 1; s->hits++; if (d < s->r - s->eps) s->robust = 1; else s->marginal = 1; }
+    else if (d <= s->r + s->eps) s->marginal = 1;
+}
+
+/* distance from segment pq to quadratic Bezier (B0,B1,B2) by branch and bound:
+ * the convex hull (triangle) of a piece's control points bounds it from below,
+ * its end points from above.  Stops once the distance is certainly below
+ * hit_below or a piece is certainly beyond miss_above, or the bracket is
+ * tighter than 1e-12 m. */
+static double seg_quad_dist(d3 p, d3 q, d3 B0, d3 B1, d3 B2, double hit_below, double miss_above) {
+    typedef struct { d3 a, b, c; double lb; int depth; } piece;
+    piece st[256];
+    int sp = 0;
+    double ub = sqrt(seg_seg2(p, q, B0, B0));
+    double t = sqrt(seg_seg2(p, q, B2, B2));
+    if (t < ub) ub = t;
+    double m;
+    double lb0 = seg_tri(p, q, B0, B1, B2, &m) ? 0.0 : m;
+    st[sp].a = B0; st[sp].b = B1; st[sp].c = B2; st[sp].lb = lb0; st[sp].depth = 0; ++sp;
+    while (sp) {
+        piece pc = st[--sp];
+        if (pc.lb >= ub) continue;
+        if (ub < hit_below) return ub;               /* decided: robust hit */
+        if (pc.lb > miss_above) continue;            /* cannot reach the band: a certain miss */
+        if (ub - pc.lb < 1e-12 || pc.depth > 48) continue;
+        /* de Casteljau split at 1/2 */
+        d3 ab = mul(add(pc.a, pc.b), 0.5), bc = mul(add(pc.b, pc.c), 0.5), mid = mul(add(ab, bc), 0.5);
+        double dm = sqrt(seg_seg2(p, q, mid, mid));
+        if (dm < ub) ub = dm;
+        piece L = {pc.a, ab, mid, 0, pc.depth + 1}, Rr = {mid, bc, pc.c, 0, pc.depth + 1};
+        L.lb = seg_tri(p, q, L.a, L.b, L.c, &m) ? 0.0 : m;
+        Rr.lb = seg_tri(p, q, Rr.a, Rr.b, Rr.c, &m) ? 0.0 : m;
+        if (Rr.lb < ub) st[sp++] = Rr;
+        if (L.lb < ub) st[sp++] = L;
+    }
+    return ub;
+}
+
+static int visit_edge(void* vctx, u32 e) {
+    sweep_query* s = (sweep_query*) vctx;
+    d3 p = fv(s->sv + s->se[e * 2] * 3), q = fv(s->sv + s->se[e * 2 + 1] * 3);
+    ++s->prim_tests;
+    double d;
+    if (!s->quad) d = sqrt(seg_seg2(p, q, s->a, s->b));
+    else d = seg_quad_dist(p, q, s->B0, s->B1, s->B2, s->r - s->eps, s->r + s->eps);
+    classify(s, d);
+    return 0;
+}
+
+typedef struct {
+    const orc_robot* R;
+    const orc_scene* S;
+    const float* q;
+    const u32* traj_off;
+    int quad, endpoints;
+    double eps;
+    bvh_t scene_edge;
+    unsigned char *traj_hit, *traj_band, *seg_hit, *seg_band, *traj_marg;
+    u32* traj_count;
+    const u32* seg_off;  /* per-trajectory offsets into seg_hit / seg_band */
+    orc_work* work;
+} sweep_ctx;
+
+/* W = pinv(B) = (B^T B)^{-1} B^T for the nt x nc uniform quadratic B-spline basis */
+static int fit_weights(int nc, int nt, double* W /* nc*nt */) {
+    double* B = (double*) calloc((size_t) nt * nc, sizeof(double));
+    for (int t = 0; t < nt; ++t) {
+        double x = nt > 1 ? 2.0 + (double) (nc - 2) * t / (nt - 1) : 2.0;
+        int seg = (int) floor(x) - 2;
+        if (seg > nc - 3) seg = nc - 3;
+        if (seg < 0) seg = 0;
+        double s = x - (seg + 2);
+        B[t * nc + seg] += 0.5 * (1 - s) * (1 - s);
+        B[t * nc + seg + 1] += 0.5 + s - s * s;
+        B[t * nc + seg + 2] += 0.5 * s * s;
+    }
+    /* G = B^T B (nc x nc), Cholesky, solve G W = B^T */
+    double* G = (double*) calloc((size_t) nc * nc, sizeof(double));
+    for (int i = 0; i < nc; ++i)
+        for (int j = 0; j < nc; ++j) {
+            double acc = 0;
+            for (int t = 0; t < nt; ++t) acc += B[t * nc + i] * B[t * nc + j];
+            G[i * nc + j] = acc;
+        }
+    for (int j = 0; j < nc; ++j) {
+        double d = G[j * nc + j];
+        for (int k = 0; k < j; ++k) d -= G[j * nc + k] * G[j * nc + k];
+        if (d <= 0) { free(B); free(G); return -1; }
+        d = sqrt(d);
+        G[j * nc + j] = d;
+        for (int i = j + 1; i < nc; ++i) {
+            double v = G[i * nc + j];
+            for (int k = 0; k < j; ++k) v -= G[i * nc + k] * G[j * nc + k];
+            G[i * nc + j] = v / d;
+        }
+    }
+    for (int t = 0; t < nt; ++t) {
+        double y[256];
+        for (int i = 0; i < nc; ++i) {  /* L y = b */
+            double v = B[t * nc + i];
+            for (int k = 0; k < i; ++k) v -= G[i * nc + k] * y[k];
+            y[i] = v / G[i * nc + i];
+        }
+        for (int i = nc - 1; i >= 0; --i) {  /* L^T x = y */
+            double v = y[i];
+            for (int k = i + 1; k < nc; ++k) v -= G[k * nc + i] * y[k];
+            y[i] = v / G[i * nc + i];
+        }
+        for (int i = 0; i < nc; ++i) W[i * nt + t] = y[i];
+    }
+    free(B);
+    free(G);
+    return 0;
+}
+
+int orc_fit_weights(int nc, int nt, double* W) { return (nc < 3 || nc > 256 || nt < nc) ? -1 : fit_weights(nc, nt, W); }
+
+int orc_quad_ctrl_count(int n_wp) { int c = (n_wp + 1) / 2; return c < 3 ? 3 : c; }
+
+static void sweep_traj(void* vctx, int tr, void* scratch) {
+    (void) scratch;
+    sweep_ctx* C = (sweep_ctx*) vctx;
+    const orc_robot* R = C->R;
+    int nwp = (int) (C->traj_off[tr + 1] - C->traj_off[tr]);
+    int ns = R->n_spheres;
+    int nl = R->dof + 1;
+    double* T = (double*) malloc(sizeof(double) * (size_t) nl * 12);
+    d3* cen = (d3*) malloc(sizeof(d3) * (size_t) nwp * ns);   /* [wp][sphere] */
+    for (int w = 0; w < nwp; ++w) {
+        orc_fk_pose(R->dof, R->cos_mask, R->sin_mask, R->one_mask, R->base_tf, C->q + (size_t) (C->traj_off[tr] + w) * R->dof, T);
+        for (int s = 0; s < ns; ++s) cen[w * ns + s] = xform(T + R->sphere_links[s] * 12, fv(R->sphere_centers + s * 3));
+    }
+    int trob = 0, trmarg = 0, trhit = 0;
+    u32 trcount = 0;
+    uint64_t ntests = 0, ptests = 0;
+    unsigned char* seg_hit = C->seg_hit ? C->seg_hit + C->seg_off[tr] : NULL;
+    unsigned char* seg_band = C->seg_band ? C->seg_band + C->seg_off[tr] : NULL;
+    if (!C->quad) {
+        for (int g = 0; g + 1 < nwp; ++g) {
+            int srob = 0, smarg = 0, shit = 0;
+            for (int s = 0; s < ns; ++s) {
+                sweep_query Q;
+                memset(&Q, 0, sizeof(Q));
+                Q.a = cen[g * ns + s]; Q.b = cen[(g + 1) * ns + s]; Q.r = R->sphere_radii[s]; Q.eps = C->eps;
+                Q.sv = C->S->verts; Q.se = C->S->edges;
+                double pad = Q.r + C->eps;
+                double qlo[3] = {fmin(Q.a.x, Q.b.x) - pad, fmin(Q.a.y, Q.b.y) - pad, fmin(Q.a.z, Q.b.z) - pad};
+                double qhi[3] = {fmax(Q.a.x, Q.b.x) + pad, fmax(Q.a.y, Q.b.y) + pad, fmax(Q.a.z, Q.b.z) + pad};
+                ntests += bvh_query(&C->scene_edge, qlo, qhi, visit_edge, &Q);
+                ptests += Q.prim_tests;
+                shit |= Q.any_hit; srob |= Q.robust; smarg |= Q.marginal;
+                trcount += Q.hits;
+            }
+            if (seg_hit) seg_hit[g] = (unsigned char) shit;
+            if (seg_band) seg_band[g] = (unsigned char) (!srob && smarg);
+            trhit |= shit; trob |= srob; trmarg |= smarg;
+        }
+    } else {
+        int nc = orc_quad_ctrl_count(nwp);
+        double* W = (double*) malloc(sizeof(double) * (size_t) nc * nwp);
+        d3* ctrl = (d3*) malloc(sizeof(d3) * (size_t) nc * ns);
+        if (nwp < 3 || fit_weights(nc, nwp, W)) {
+            /* too short to fit: flag as hit-and-band so it cannot pass silently */
+            C->traj_hit[tr] = 1;
+            if (C->traj_band) C->traj_band[tr] = 1;
+            free(W); free(ctrl); free(T); free(cen);
+            return;
+        }
+        for (int k = 0; k < nc; ++k)
+            for (int s = 0; s < ns; ++s) {
+                d3 acc = v3(0, 0, 0);
+                for (int w = 0; w < nwp; ++w) acc = add(acc, mul(cen[w * ns + s], W[k * nwp + w]));
+                ctrl[k * ns + s] = acc;
+            }
+        int npieces = nc - 2 + (C->endpoints ? 2 : 0);
+        for (int g = 0; g < npieces; ++g) {
+            int srob = 0, smarg = 0, shit = 0;
+            for (int s = 0; s < ns; ++s) {
+                sweep_query Q;
+                memset(&Q, 0, sizeof(Q));
+                Q.quad = 1; Q.r = R->sphere_radii[s]; Q.eps = C->eps; Q.sv = C->S->verts; Q.se = C->S->edges;
+                if (g < nc - 2) {
+                    d3 P0 = ctrl[g * ns + s], P1 = ctrl[(g + 1) * ns + s], P2 = ctrl[(g + 2) * ns + s];
+                    Q.B0 = mul(add(P0, P1), 0.5); Q.B1 = P1; Q.B2 = mul(add(P1, P2), 0.5);
+                } else {
+                    d3 c = cen[(g == nc - 2 ? 0 : nwp - 1) * ns + s];
+                    Q.B0 = c; Q.B1 = c; Q.B2 = c;
+                }
+                double pad = Q.r + C->eps;
+                double qlo[3] = {fmin(Q.B0.x, fmin(Q.B1.x, Q.B2.x)) - pad, fmin(Q.B0.y, fmin(Q.B1.y, Q.B2.y)) - pad,
+                                 fmin(Q.B0.z, fmin(Q.B1.z, Q.B2.z)) - pad};
+                double qhi[3] = {fmax(Q.B0.x, fmax(Q.B1.x, Q.B2.x)) + pad, fmax(Q.B0.y, fmax(Q.B1.y, Q.B2.y)) + pad,
+                                 fmax(Q.B0.z, fmax(Q.B1.z, Q.B2.z)) + pad};
+                ntests += bvh_query(&C->scene_edge, qlo, qhi, visit_edge, &Q);
+                ptests += Q.prim_tests;
+                shit |= Q.any_hit; srob |= Q.robust; smarg |= Q.marginal;
+                trcount += Q.hits;
+            }
+            if (seg_hit) seg_hit[g] = (unsigned char) shit;
+            if (seg_band) seg_band[g] = (unsigned char) (!srob && smarg);
+            trhit |= shit; trob |= srob; trmarg |= smarg;
+        }
+        free(W);
+        free(ctrl);
+    }
+    C->traj_hit[tr] = (unsigned char) trhit;
+    if (C->traj_band) C->traj_band[tr] = (unsigned char) (!trob && trmarg);
+    if (C->traj_marg) C->traj_marg[tr] = (unsigned char) trmarg;
+    if (C->traj_count) C->traj_count[tr] = trcount;
+    if (C->work) { C->work[tr].node_tests = ntests; C->work[tr].prim_tests = ptests; }
+    free(T);
+    free(cen);
+}
+
+/* quad = 0: piecewise-linear capsules, seg_off[t] = sum of (nwp - 1);
+ * quad = 1: quadratic pieces, seg_off[t] = sum of (nc - 2 + 2 * endpoints). */
+int orc_sweep(int quad, int endpoints, const orc_robot* R, const orc_scene* S, const float* q, const u32* traj_off,
+              int n_traj, double eps, int threads, unsigned char* traj_hit, unsigned char* traj_band,
+              unsigned char* traj_marg, u32* traj_count, const u32* seg_off, unsigned char* seg_hit,
+              unsigned char* seg_band, orc_work* work) {
+    sweep_ctx C;
+    memset(&C, 0, sizeof(C));
+    C.R = R; C.S = S; C.q = q; C.traj_off = traj_off; C.quad = quad; C.endpoints = endpoints; C.eps = eps;
+    C.traj_hit = traj_hit; C.traj_band = traj_band; C.seg_hit = seg_hit; C.seg_band = seg_band; C.seg_off = seg_off;
+    C.traj_marg = traj_marg; C.traj_count = traj_count;
+    C.work = work;
+    float *lo, *hi;
+    edge_boxes(S->verts, S->edges, S->n_edges, &lo, &hi);
+    bvh_make(&C.scene_edge, S->n_edges, lo, hi);
+    run_pool(n_traj, threads, sweep_traj, &C, 0);
+    bvh_free(&C.scene_edge);
+    return 0;
+}
+
+/* ---------------------------------------------------------- small exports */
+int orc_seg_tri(const double* p, const double* q, const double* a, const double* b, const double* c, double* m) {
+    return seg_tri(v3(p[0], p[1], p[2]), v3(q[0], q[1], q[2]), v3(a[0], a[1], a[2]), v3(b[0], b[1], b[2]),
+                   v3(c[0], c[1], c[2]), m);
+}
+double orc_seg_seg(const double* p1, const double* q1, const double* p2, const double* q2) {
+    return sqrt(seg_seg2(v3(p1[0], p1[1], p1[2]), v3(q1[0], q1[1], q1[2]), v3(p2[0], p2[1], p2[2]), v3(q2[0], q2[1], q2[2])));
+}
+double orc_seg_quad(const double* p, const double* q, const double* b0, const double* b1, const double* b2) {
+    return seg_quad_dist(v3(p[0], p[1], p[2]), v3(q[0], q[1], q[2]), v3(b0[0], b0[1], b0[2]), v3(b1[0], b1[1], b1[2]),
+                         v3(b2[0], b2[1], b2[2]), -INFINITY, INFINITY);
+}

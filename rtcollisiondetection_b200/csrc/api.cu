@@ -1,0 +1,1077 @@
+// api.cu - the C ABI (include/rtcd.h) over the device engine.
+//
+// Host-side responsibilities: validate inputs, extract unique edges and fit
+// PCA OBBs (RTCD/Meshes/mesh.h:200-216, RTCD/Meshes/Obb.h:29-114), build and
+// keep the robot and scene LBVHs resident, size the per-detector workspaces,
+// stage host buffers through pinned memory, and launch the query pipeline on a
+// stream without any host round trip (the plain path adds one per frame, the
+// shape of the upstream check(), RTCD/CollisionDetector/CollisionDetector.h:
+// 354-471).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <unordered_set>
+
+#include "../../include/rtcd.h"
+#include "kernels.h"
+
+namespace rtcd {
+
+static thread_local std::string g_last_error;
+
+void fail(int status, const std::string& msg) { throw Error{status, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+    int st = (e == cudaErrorMemoryAllocation) ? RTCD_ERR_OUT_OF_MEMORY : RTCD_ERR_CUDA;
+    fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void DevBuf::ensure(size_t n) {
+    if (n <= bytes && p) return;
+    release();
+    size_t want = std::max<size_t>(n, 256);
+    cuda_check(cudaMalloc(&p, want), "cudaMalloc");
+    bytes = want;
+}
+
+void HostBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void HostBuf::ensure(size_t n) {
+    if (n <= bytes && p) return;
+    release();
+    size_t want = std::max<size_t>(n, 256);
+    cuda_check(cudaMallocHost(&p, want), "cudaMallocHost");
+    bytes = want;
+}
+
+int device_sm_count() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
+// ---------------------------------------------------------------- host geometry
+// Unique undirected edges in first-seen orientation (RTCD/Meshes/mesh.h:200-216).
+static std::vector<uint32_t> unique_edges(const uint32_t* tris, size_t n_tris) {
+    std::vector<uint32_t> out;
+    out.reserve(n_tris * 3);
+    std::unordered_set<uint64_t> seen;
+    seen.reserve(n_tris * 3);
+    for (size_t t = 0; t < n_tris; ++t)
+        for (int k = 0; k < 3; ++k) {
+            uint32_t a = tris[3 * t + k], b = tris[3 * t + (k + 1) % 3];
+            uint64_t key = ((uint64_t) std::min(a, b) << 32) | std::max(a, b);
+            if (seen.insert(key).second) {
+                out.push_back(a);
+                out.push_back(b);
+            }
+        }
+    return out;
+}
+
+// Symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations.
+static void jacobi3(double A[3][3], double V[3][3], double w[3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) V[i][j] = (i == j);
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        double off = std::fabs(A[0][1]) + std::fabs(A[0][2]) + std::fabs(A[1][2]);
+        if (off < 1e-300) break;
+        for (int p = 0; p < 2; ++p)
+            for (int q = p + 1; q < 3; ++q) {
+                if (std::fabs(A[p][q]) < 1e-300) continue;
+                double theta = (A[q][q] - A[p][p]) / (2 * A[p][q]);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                double c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int k = 0; k < 3; ++k) {
+                    double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - s * akq;
+                    A[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - s * aqk;
+                    A[q][k] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; ++k) {
+                    double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    for (int i = 0; i < 3; ++i) w[i] = A[i][i];
+}
+
+// PCA-fitted OBB of a point set (RTCD/Meshes/Obb.h:29-114): principal axes
+// by decreasing variance, right-handed, extents from the projections.  The
+// float result is then grown until it contains every input point and padded
+// by `pad`.  out: centre(3), half(3), axes x/y/z (9), bounding radius.
+static void fit_obb(const float* pts, const std::vector<uint32_t>& idx, float pad, float* out) {
+    std::memset(out, 0, 16 * sizeof(float));
+    out[6] = 1; out[10] = 1; out[14] = 1;
+    if (idx.empty()) return;
+    double mean[3] = {0, 0, 0};
+    for (uint32_t i : idx)
+        for (int k = 0; k < 3; ++k) mean[k] += pts[3 * i + k];
+    for (int k = 0; k < 3; ++k) mean[k] /= (double) idx.size();
+    double C[3][3] = {{0}};
+    for (uint32_t i : idx) {
+        double d[3] = {pts[3 * i] - mean[0], pts[3 * i + 1] - mean[1], pts[3 * i + 2] - mean[2]};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) C[a][b] += d[a] * d[b];
+    }
+    double V[3][3], w[3];
+    jacobi3(C, V, w);
+    int order[3] = {0, 1, 2};
+    std::sort(order, order + 3, [&](int a, int b) { return w[a] > w[b]; });
+    double ax[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < 3; ++k) ax[a][k] = V[k][order[a]];
+    double det = ax[0][0] * (ax[1][1] * ax[2][2] - ax[1][2] * ax[2][1]) -
+                 ax[0][1] * (ax[1][0] * ax[2][2] - ax[1][2] * ax[2][0]) +
+                 ax[0][2] * (ax[1][0] * ax[2][1] - ax[1][1] * ax[2][0]);
+    if (det < 0)
+        for (int k = 0; k < 3; ++k) ax[2][k] = -ax[2][k];
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (uint32_t i : idx)
+        for (int a = 0; a < 3; ++a) {
+            double v = ax[a][0] * pts[3 * i] + ax[a][1] * pts[3 * i + 1] + ax[a][2] * pts[3 * i + 2];
+            lo[a] = std::min(lo[a], v);
+            hi[a] = std::max(hi[a], v);
+        }
+    double c[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a)
+        for (int k = 0; k < 3; ++k) c[k] += ax[a][k] * 0.5 * (lo[a] + hi[a]);
+    float fc[3], fh[3], fa[9];
+    for (int k = 0; k < 3; ++k) fc[k] = (float) c[k];
+    for (int a = 0; a < 3; ++a) {
+        fh[a] = (float) (0.5 * (hi[a] - lo[a]));
+        for (int k = 0; k < 3; ++k) fa[3 * a + k] = (float) ax[a][k];
+    }
+    // grow the float box until it holds every point (checked in double on the float box)
+    for (uint32_t i : idx)
+        for (int a = 0; a < 3; ++a) {
+            double v = 0;
+            for (int k = 0; k < 3; ++k) v += (double) fa[3 * a + k] * ((double) pts[3 * i + k] - fc[k]);
+            double need = std::fabs(v) * (1 + 1e-6) + 1e-7;
+            if (need > fh[a]) fh[a] = (float) need;
+        }
+    for (int a = 0; a < 3; ++a) fh[a] += pad;
+    for (int k = 0; k < 3; ++k) out[k] = fc[k];
+    for (int a = 0; a < 3; ++a) out[3 + a] = fh[a];
+    for (int k = 0; k < 9; ++k) out[6 + k] = fa[k];
+    out[15] = std::sqrt(fh[0] * fh[0] + fh[1] * fh[1] + fh[2] * fh[2]);
+}
+
+// Device LBVH over triangles or edges, concatenated over several groups
+// (links); returns per-group roots.
+struct GroupedBvh {
+    DevBuf nodes, prims;
+    std::vector<uint32_t> roots;
+    uint32_t max_depth = 0;
+};
+
+static void build_grouped(bool tris, const float* d_verts, const std::vector<uint32_t>& vert_off, const uint32_t* d_idx,
+                          const std::vector<uint32_t>& prim_off, uint32_t* d_err, cudaStream_t s, GroupedBvh& out) {
+    size_t groups = prim_off.size() - 1;
+    uint32_t total = prim_off.back();
+    size_t total_nodes = 0;
+    for (size_t g = 0; g < groups; ++g) {
+        uint32_t n = prim_off[g + 1] - prim_off[g];
+        total_nodes += n > 1 ? n - 1 : 0;
+    }
+    out.nodes.ensure(64 * std::max<size_t>(total_nodes, 1));
+    out.prims.ensure((tris ? 48 : 32) * (size_t) std::max<uint32_t>(total, 1));
+    out.roots.assign(groups, kNone);
+    DevBuf lo, hi, perm;
+    lo.ensure(16ull * std::max<uint32_t>(total, 1));
+    hi.ensure(16ull * std::max<uint32_t>(total, 1));
+    perm.ensure(4ull * std::max<uint32_t>(total, 1));
+    uint32_t node_off = 0;
+    const int per = tris ? 3 : 2;
+    for (size_t g = 0; g < groups; ++g) {
+        uint32_t p0 = prim_off[g], n = prim_off[g + 1] - p0;
+        if (!n) continue;
+        const float* v = d_verts + 3ull * vert_off[g];
+        const uint32_t* ix = d_idx + (size_t) per * p0;
+        float4* l = lo.as<float4>() + p0;
+        float4* h = hi.as<float4>() + p0;
+        if (tris) tri_boxes(v, ix, n, l, h, s); else edge_boxes(v, ix, n, l, h, s);
+        LbvhResult r = build_lbvh(l, h, n, out.nodes.as<float4>() + 4ull * node_off, perm.as<uint32_t>() + p0, node_off,
+                                  p0, d_err, s);
+        out.roots[g] = r.root;
+        out.max_depth = std::max(out.max_depth, r.depth);
+        if (tris)
+            gather_tris(v, ix, perm.as<uint32_t>() + p0, n, p0, (uint32_t) g, out.prims.as<float4>() + 3ull * p0, s);
+        else
+            gather_edges(v, ix, perm.as<uint32_t>() + p0, n, p0, (uint32_t) g, out.prims.as<float4>() + 2ull * p0, s);
+        node_off += n > 1 ? n - 1 : 0;
+    }
+    cuda_check(cudaStreamSynchronize(s), "grouped bvh");
+}
+
+}  // namespace rtcd
+
+using namespace rtcd;
+
+struct rtcd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    DevBuf err;
+};
+
+struct rtcd_robot {
+    rtcd_ctx* ctx = nullptr;
+    RobotDev dev{};
+    GroupedBvh tri, edge;
+    DevBuf verts, tris, edges, spheres, sphere_link;
+    std::vector<uint32_t> edge_off;
+    uint32_t dof = 0;
+};
+
+struct rtcd_scene {
+    rtcd_ctx* ctx = nullptr;
+    SceneDev dev{};
+    GroupedBvh tri, edge;
+    DevBuf verts, tris, edges, obbs;
+    uint32_t n_tris = 0, n_edges = 0, n_obs = 0;
+};
+
+struct rtcd_detector {
+    rtcd_ctx* ctx = nullptr;
+    rtcd_detector_kind kind = RTCD_OBS_TO_ROBOT;
+    rtcd_robot* robot = nullptr;
+    rtcd_scene* scene = nullptr;
+    rtcd_config cfg{};
+    std::mutex mu;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t staged = nullptr;
+    uint32_t blocks = 0;
+    // discrete workspace
+    DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
+    ScanScratch scan;
+    // sweep workspace
+    DevBuf centers, ctrl, aux, piece_hit, W, W_off;
+    std::vector<float> W_host;
+    std::vector<uint32_t> W_off_host;
+    uint32_t W_max = 0;
+    HostBuf pin_in, pin_out, pin_aux;
+    uint64_t last_items = 0, last_culled = 0;
+};
+
+static rtcd_status finish(const std::exception_ptr& ep) {
+    try {
+        std::rethrow_exception(ep);
+    } catch (const Error& e) {
+        g_last_error = e.msg;
+        return (rtcd_status) e.status;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return RTCD_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return RTCD_ERR_INTERNAL;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return RTCD_ERR_INTERNAL;
+    }
+}
+
+template <class F>
+static rtcd_status guarded(F&& f) {
+    try {
+        g_last_error.clear();
+        f();
+        return RTCD_OK;
+    } catch (...) {
+        return finish(std::current_exception());
+    }
+}
+
+#define RTCD_REQUIRE(cond, msg) \
+    do {                        \
+        if (!(cond)) fail(RTCD_ERR_INVALID_ARGUMENT, msg); \
+    } while (0)
+
+struct DeviceScope {
+    int prev = 0;
+    explicit DeviceScope(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceScope() {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        if (cur != prev) cudaSetDevice(prev);
+    }
+};
+
+extern "C" {
+
+int rtcd_abi_version(void) { return RTCD_ABI_VERSION; }
+
+rtcd_status rtcd_last_error(char* buf, size_t n) {
+    if (buf && n) {
+        size_t k = std::min(n - 1, g_last_error.size());
+        std::memcpy(buf, g_last_error.data(), k);
+        buf[k] = 0;
+    }
+    return RTCD_OK;
+}
+
+rtcd_status rtcd_context_create(int device, rtcd_ctx** out) {
+    return guarded([&] {
+        RTCD_REQUIRE(out, "out is NULL");
+        *out = nullptr;
+        int n = 0;
+        cuda_check(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+        RTCD_REQUIRE(device >= 0 && device < n, "no such CUDA device");
+        DeviceScope ds(device);
+        auto* c = new rtcd_ctx();
+        c->device = device;
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            cuda_check(e, "cudaStreamCreate");
+        }
+        c->err.ensure(4);
+        cuda_check(cudaMemset(c->err.p, 0, 4), "memset");
+        *out = c;
+    });
+}
+
+rtcd_status rtcd_context_destroy(rtcd_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        DeviceScope ds(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+        ctx->err.release();
+        delete ctx;
+    });
+}
+
+rtcd_status rtcd_robot_create(rtcd_ctx* ctx, const rtcd_robot_desc* d, rtcd_robot** out) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && d && out, "NULL argument");
+        *out = nullptr;
+        RTCD_REQUIRE(d->dof >= 1 && d->dof <= (uint32_t) kMaxDof, "dof must be in [1, 15]");
+        RTCD_REQUIRE(d->base_tf && d->cos_mask && d->sin_mask && d->one_mask, "chain masks are required");
+        RTCD_REQUIRE(d->link_verts && d->link_vert_offsets && d->link_tris && d->link_tri_offsets,
+                     "link meshes are required");
+        DeviceScope ds(ctx->device);
+        const uint32_t L = d->dof + 1;
+        std::vector<uint32_t> voff(d->link_vert_offsets, d->link_vert_offsets + L + 1);
+        std::vector<uint32_t> toff(d->link_tri_offsets, d->link_tri_offsets + L + 1);
+        RTCD_REQUIRE(voff[0] == 0 && toff[0] == 0, "offsets must start at 0");
+        for (uint32_t l = 0; l < L; ++l)
+            RTCD_REQUIRE(voff[l + 1] >= voff[l] && toff[l + 1] >= toff[l], "offsets must be non-decreasing");
+        for (uint32_t l = 0; l < L; ++l)
+            for (uint32_t t = toff[l]; t < toff[l + 1]; ++t)
+                for (int k = 0; k < 3; ++k)
+                    RTCD_REQUIRE(d->link_tris[3ull * t + k] < voff[l + 1] - voff[l],
+                                 "link triangle index out of range");
+        std::unique_ptr<rtcd_robot> r(new rtcd_robot());
+        r->ctx = ctx;
+        r->dof = d->dof;
+        // edges
+        std::vector<uint32_t> edges, eoff(L + 1, 0);
+        if (d->link_edges) {
+            RTCD_REQUIRE(d->link_edge_offsets, "link_edge_offsets required with link_edges");
+            eoff.assign(d->link_edge_offsets, d->link_edge_offsets + L + 1);
+            RTCD_REQUIRE(eoff[0] == 0, "edge offsets must start at 0");
+            for (uint32_t l = 0; l < L; ++l) RTCD_REQUIRE(eoff[l + 1] >= eoff[l], "edge offsets must be non-decreasing");
+            edges.assign(d->link_edges, d->link_edges + 2ull * eoff[L]);
+            for (uint32_t l = 0; l < L; ++l)
+                for (uint32_t e = eoff[l]; e < eoff[l + 1]; ++e)
+                    RTCD_REQUIRE(edges[2 * e] < voff[l + 1] - voff[l] && edges[2 * e + 1] < voff[l + 1] - voff[l],
+                                 "link edge index out of range");
+        } else {
+            for (uint32_t l = 0; l < L; ++l) {
+                auto e = unique_edges(d->link_tris + 3ull * toff[l], toff[l + 1] - toff[l]);
+                edges.insert(edges.end(), e.begin(), e.end());
+                eoff[l + 1] = (uint32_t) (edges.size() / 2);
+            }
+        }
+        r->edge_off = eoff;
+        // chain
+        Chain& ch = r->dev.chain;
+        std::memset(&ch, 0, sizeof(ch));
+        ch.dof = (int) d->dof;
+        std::memcpy(ch.base, d->base_tf, 12 * sizeof(float));
+        std::memcpy(ch.cm, d->cos_mask, 12ull * d->dof * sizeof(float));
+        std::memcpy(ch.sm, d->sin_mask, 12ull * d->dof * sizeof(float));
+        std::memcpy(ch.om, d->one_mask, 12ull * d->dof * sizeof(float));
+        r->dev.n_links = L;
+        r->dev.first_link = d->skip_base ? 1 : 0;
+        // OBBs (link frames)
+        for (uint32_t l = 0; l < L; ++l) {
+            float* o = r->dev.obb[l];
+            if (d->link_obbs) {
+                std::memcpy(o, d->link_obbs + 15ull * l, 15 * sizeof(float));
+                o[3] += 1e-5f; o[4] += 1e-5f; o[5] += 1e-5f;
+                o[15] = std::sqrt(o[3] * o[3] + o[4] * o[4] + o[5] * o[5]);
+            } else {
+                std::vector<uint32_t> idx(voff[l + 1] - voff[l]);
+                for (size_t k = 0; k < idx.size(); ++k) idx[k] = voff[l] + (uint32_t) k;
+                fit_obb(d->link_verts, idx, 1e-5f, o);
+            }
+        }
+        cudaStream_t s = ctx->stream;
+        upload(r->verts, d->link_verts, 3ull * voff[L], s);
+        upload(r->tris, d->link_tris, 3ull * toff[L], s);
+        upload(r->edges, edges.data(), edges.size(), s);
+        build_grouped(true, r->verts.as<float>(), voff, r->tris.as<uint32_t>(), toff, ctx->err.as<uint32_t>(), s, r->tri);
+        build_grouped(false, r->verts.as<float>(), voff, r->edges.as<uint32_t>(), eoff, ctx->err.as<uint32_t>(), s,
+                      r->edge);
+        r->dev.tri_nodes = r->tri.nodes.as<float4>();
+        r->dev.tri_prims = r->tri.prims.as<float4>();
+        r->dev.edge_nodes = r->edge.nodes.as<float4>();
+        r->dev.edge_prims = r->edge.prims.as<float4>();
+        for (uint32_t l = 0; l < (uint32_t) kMaxLinks; ++l) {
+            r->dev.tri_root[l] = l < L ? r->tri.roots[l] : kNone;
+            r->dev.edge_root[l] = l < L ? r->edge.roots[l] : kNone;
+        }
+        r->dev.n_edges_total = eoff[L];
+        // spheres
+        r->dev.n_spheres = d->n_spheres;
+        if (d->n_spheres) {
+            RTCD_REQUIRE(d->sphere_centers && d->sphere_radii && d->sphere_links, "sphere arrays required");
+            std::vector<float4> sp(d->n_spheres);
+            for (uint32_t i = 0; i < d->n_spheres; ++i) {
+                RTCD_REQUIRE(d->sphere_links[i] < L, "sphere link out of range");
+                RTCD_REQUIRE(d->sphere_radii[i] >= 0, "negative sphere radius");
+                sp[i] = make_float4(d->sphere_centers[3 * i], d->sphere_centers[3 * i + 1], d->sphere_centers[3 * i + 2],
+                                    d->sphere_radii[i]);
+            }
+            upload(r->spheres, sp.data(), sp.size(), s);
+            upload(r->sphere_link, d->sphere_links, d->n_spheres, s);
+        } else {
+            r->spheres.ensure(16);
+            r->sphere_link.ensure(4);
+        }
+        r->dev.spheres = r->spheres.as<float4>();
+        r->dev.sphere_link = r->sphere_link.as<uint32_t>();
+        cuda_check(cudaStreamSynchronize(s), "robot upload");
+        *out = r.release();
+    });
+}
+
+rtcd_status rtcd_robot_destroy(rtcd_robot* r) {
+    return guarded([&] {
+        if (!r) return;
+        DeviceScope ds(r->ctx->device);
+        cudaStreamSynchronize(r->ctx->stream);
+        delete r;
+    });
+}
+
+rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_verts, const uint32_t* tris, uint32_t n_tris,
+                              const uint32_t* obstacle_tri_offsets, uint32_t n_obstacles, rtcd_scene** out) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && out, "NULL argument");
+        *out = nullptr;
+        RTCD_REQUIRE(n_tris == 0 || (verts && tris), "vertex and triangle arrays required");
+        for (size_t i = 0; i < 3ull * n_tris; ++i) RTCD_REQUIRE(tris[i] < n_verts, "triangle index out of range");
+        std::vector<uint32_t> off;
+        if (obstacle_tri_offsets && n_obstacles) {
+            off.assign(obstacle_tri_offsets, obstacle_tri_offsets + n_obstacles + 1);
+            RTCD_REQUIRE(off[0] == 0 && off.back() == n_tris, "obstacle offsets must span [0, n_tris]");
+            for (uint32_t i = 0; i < n_obstacles; ++i) RTCD_REQUIRE(off[i + 1] >= off[i], "obstacle offsets decrease");
+        } else {
+            off = {0, n_tris};
+        }
+        DeviceScope ds(ctx->device);
+        std::unique_ptr<rtcd_scene> sc(new rtcd_scene());
+        sc->ctx = ctx;
+        auto edges = unique_edges(tris, n_tris);
+        sc->n_tris = n_tris;
+        sc->n_edges = (uint32_t) (edges.size() / 2);
+        // obstacle OBBs
+        uint32_t nob = (uint32_t) off.size() - 1;
+        std::vector<float> obbs(16ull * nob);
+        for (uint32_t o = 0; o < nob; ++o) {
+            std::vector<uint32_t> idx;
+            idx.reserve(3ull * (off[o + 1] - off[o]));
+            for (uint32_t t = off[o]; t < off[o + 1]; ++t)
+                for (int k = 0; k < 3; ++k) idx.push_back(tris[3ull * t + k]);
+            std::sort(idx.begin(), idx.end());
+            idx.erase(std::unique(idx.begin(), idx.end()), idx.end());
+            fit_obb(verts, idx, 1e-5f, obbs.data() + 16ull * o);
+        }
+        sc->n_obs = nob;
+        cudaStream_t s = ctx->stream;
+        upload(sc->verts, verts, 3ull * n_verts, s);
+        upload(sc->tris, tris, 3ull * n_tris, s);
+        upload(sc->edges, edges.data(), edges.size(), s);
+        upload(sc->obbs, obbs.data(), obbs.size(), s);
+        std::vector<uint32_t> v0 = {0, 0};
+        std::vector<uint32_t> toff = {0, n_tris}, eoff = {0, sc->n_edges};
+        build_grouped(true, sc->verts.as<float>(), v0, sc->tris.as<uint32_t>(), toff, ctx->err.as<uint32_t>(), s, sc->tri);
+        build_grouped(false, sc->verts.as<float>(), v0, sc->edges.as<uint32_t>(), eoff, ctx->err.as<uint32_t>(), s,
+                      sc->edge);
+        SceneDev& dv = sc->dev;
+        dv.tri_nodes = sc->tri.nodes.as<float4>();
+        dv.tri_prims = sc->tri.prims.as<float4>();
+        dv.tri_root = sc->tri.roots[0];
+        dv.n_tris = n_tris;
+        dv.edge_nodes = sc->edge.nodes.as<float4>();
+        dv.edge_prims = sc->edge.prims.as<float4>();
+        dv.edge_root = sc->edge.roots[0];
+        dv.n_edges = sc->n_edges;
+        dv.obbs = sc->obbs.as<float>();
+        dv.n_obs = nob;
+        cuda_check(cudaStreamSynchronize(s), "scene upload");
+        *out = sc.release();
+    });
+}
+
+rtcd_status rtcd_scene_destroy(rtcd_scene* sc) {
+    return guarded([&] {
+        if (!sc) return;
+        DeviceScope ds(sc->ctx->device);
+        cudaStreamSynchronize(sc->ctx->stream);
+        delete sc;
+    });
+}
+
+rtcd_status rtcd_scene_info(const rtcd_scene* sc, uint32_t* n_tris, uint32_t* n_edges, uint32_t* n_obstacles) {
+    return guarded([&] {
+        RTCD_REQUIRE(sc, "NULL scene");
+        if (n_tris) *n_tris = sc->n_tris;
+        if (n_edges) *n_edges = sc->n_edges;
+        if (n_obstacles) *n_obstacles = sc->n_obs;
+    });
+}
+
+rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_robot* robot, rtcd_scene* scene,
+                                 const rtcd_config* config, rtcd_detector** out) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && robot && scene && out, "NULL argument");
+        *out = nullptr;
+        RTCD_REQUIRE(kind >= RTCD_OBS_TO_ROBOT && kind <= RTCD_QUAD_SWEEP, "unknown detector kind");
+        RTCD_REQUIRE(robot->ctx == ctx && scene->ctx == ctx, "robot and scene must belong to the context");
+        if (kind == RTCD_LINEAR_SWEEP || kind == RTCD_QUAD_SWEEP)
+            RTCD_REQUIRE(robot->dev.n_spheres > 0, "sweep detectors need a sphere model");
+        DeviceScope ds(ctx->device);
+        std::unique_ptr<rtcd_detector> d(new rtcd_detector());
+        d->ctx = ctx;
+        d->kind = kind;
+        d->robot = robot;
+        d->scene = scene;
+        if (config) d->cfg = *config;
+        if (!d->cfg.frame_size) d->cfg.frame_size = 64;
+        cuda_check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming), "cudaEventCreate");
+        if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS)
+            d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
+        else
+            d->blocks = sweep_persistent_blocks();
+        d->err.ensure(4);
+        d->stats.ensure(8 * 8);
+        d->work.ensure(4);
+        d->count.ensure(4);
+        cuda_check(cudaMemset(d->err.p, 0, 4), "memset");
+        cuda_check(cudaMemset(d->stats.p, 0, 64), "memset");
+        *out = d.release();
+    });
+}
+
+rtcd_status rtcd_detector_destroy(rtcd_detector* d) {
+    return guarded([&] {
+        if (!d) return;
+        DeviceScope ds(d->ctx->device);
+        cudaStreamSynchronize(d->stream);
+        cudaEventDestroy(d->staged);
+        cudaStreamDestroy(d->stream);
+        delete d;
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- query paths
+namespace {
+
+uint32_t quad_ctrl_count(uint32_t n_wp) { return std::max<uint32_t>(3, (n_wp + 1) / 2); }
+
+uint32_t pieces_of(rtcd_detector_kind kind, uint32_t n_wp, uint32_t flags) {
+    if (kind == RTCD_LINEAR_SWEEP) return n_wp > 0 ? n_wp - 1 : 0;
+    return quad_ctrl_count(n_wp) - 2 + ((flags & RTCD_CHECK_NO_ENDPOINTS) ? 0 : 2);
+}
+
+// Least-squares quadratic B-spline fit W = (B^T B)^{-1} B^T (nc x nt), with B
+// the uniform unclamped quadratic basis sampled at u = linspace(2, nc, nt);
+// the shipped weight tables (RTCD/data/weights/quad/normal/) are this matrix.
+std::vector<double> fit_weights(uint32_t nc, uint32_t nt) {
+    std::vector<double> B((size_t) nt * nc, 0.0), G((size_t) nc * nc, 0.0), W((size_t) nc * nt, 0.0);
+    for (uint32_t t = 0; t < nt; ++t) {
+        double x = nt > 1 ? 2.0 + (double) (nc - 2) * t / (nt - 1) : 2.0;
+        int seg = std::min<int>((int) std::floor(x) - 2, (int) nc - 3);
+        seg = std::max(seg, 0);
+        double s = x - (seg + 2);
+        B[(size_t) t * nc + seg] += 0.5 * (1 - s) * (1 - s);
+        B[(size_t) t * nc + seg + 1] += 0.5 + s - s * s;
+        B[(size_t) t * nc + seg + 2] += 0.5 * s * s;
+    }
+    for (uint32_t i = 0; i < nc; ++i)
+        for (uint32_t j = 0; j < nc; ++j) {
+            double acc = 0;
+            for (uint32_t t = 0; t < nt; ++t) acc += B[(size_t) t * nc + i] * B[(size_t) t * nc + j];
+            G[(size_t) i * nc + j] = acc;
+        }
+    // Cholesky G = L L^T (in place, lower)
+    for (uint32_t j = 0; j < nc; ++j) {
+        double dg = G[(size_t) j * nc + j];
+        for (uint32_t k = 0; k < j; ++k) dg -= G[(size_t) j * nc + k] * G[(size_t) j * nc + k];
+        if (dg <= 0) fail(RTCD_ERR_INVALID_ARGUMENT, "spline fit is singular");
+        dg = std::sqrt(dg);
+        G[(size_t) j * nc + j] = dg;
+        for (uint32_t i = j + 1; i < nc; ++i) {
+            double v = G[(size_t) i * nc + j];
+            for (uint32_t k = 0; k < j; ++k) v -= G[(size_t) i * nc + k] * G[(size_t) j * nc + k];
+            G[(size_t) i * nc + j] = v / dg;
+        }
+    }
+    std::vector<double> y(nc);
+    for (uint32_t t = 0; t < nt; ++t) {
+        for (uint32_t i = 0; i < nc; ++i) {
+            double v = B[(size_t) t * nc + i];
+            for (uint32_t k = 0; k < i; ++k) v -= G[(size_t) i * nc + k] * y[k];
+            y[i] = v / G[(size_t) i * nc + i];
+        }
+        for (int i = (int) nc - 1; i >= 0; --i) {
+            double v = y[i];
+            for (uint32_t k = i + 1; k < nc; ++k) v -= G[(size_t) k * nc + i] * y[k];
+            y[i] = v / G[(size_t) i * nc + i];
+        }
+        for (uint32_t i = 0; i < nc; ++i) W[(size_t) i * nt + t] = y[i];
+    }
+    return W;
+}
+
+void ensure_weights(rtcd_detector* d, uint32_t max_wp) {
+    if (max_wp <= d->W_max) return;
+    if (d->W_off_host.empty()) d->W_off_host.assign(1, 0);
+    d->W_off_host.resize(max_wp + 2, 0);
+    for (uint32_t n = d->W_max + 1; n <= max_wp; ++n) {
+        d->W_off_host[n] = (uint32_t) d->W_host.size();
+        if (n >= 3) {
+            auto W = fit_weights(quad_ctrl_count(n), n);
+            for (double v : W) d->W_host.push_back((float) v);
+        }
+    }
+    d->W_max = max_wp;
+    cuda_check(cudaStreamSynchronize(d->stream), "weights sync");
+    upload(d->W, d->W_host.data(), std::max<size_t>(d->W_host.size(), 1), d->stream);
+    upload(d->W_off, d->W_off_host.data(), d->W_off_host.size(), d->stream);
+    cuda_check(cudaStreamSynchronize(d->stream), "weights upload");
+}
+
+void check_device_errors(rtcd_detector* d, cudaStream_t s) {
+    uint32_t e = 0;
+    cuda_check(cudaMemcpyAsync(&e, d->err.p, 4, cudaMemcpyDeviceToHost, s), "error readback");
+    cuda_check(cudaStreamSynchronize(s), "sync");
+    if (e) {
+        cudaMemsetAsync(d->err.p, 0, 4, s);
+        cudaStreamSynchronize(s);
+        if (e & kErrLookback) fail(RTCD_ERR_DEVICE_TIMEOUT, "device look-back wait ran out");
+        if (e & kErrStack) fail(RTCD_ERR_CAPACITY, "traversal stack overflow");
+        fail(RTCD_ERR_INTERNAL, "device range check failed");
+    }
+}
+
+// One discrete pass over poses [0, n) of d_q.  When `plain`, the item count
+// is read back and the traversal grid sized to it (the upstream shape).
+void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_hit, uint32_t* d_counts,
+                   uint32_t* d_bits, uint32_t flags, bool plain, cudaStream_t s) {
+    RobotDev& R = d->robot->dev;
+    const uint32_t L = R.n_links;
+    const bool r2o = d->kind == RTCD_ROBOT_TO_OBS;
+    const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
+    d->T.ensure(48ull * n * L);
+    d->mask.ensure((size_t) n * L);
+    d->items.ensure(4ull * n * L);
+    launch_fk_poses(R.chain, d_q, n, d->T.as<float4>(), s);
+    if (flags & RTCD_CHECK_NO_CULL) {
+        launch_all_items(R, n, d->items.as<uint32_t>(), d->count.as<uint32_t>(), s);
+    } else {
+        launch_cull(R, d->scene->dev, d->T.as<float4>(), n, d->mask.as<uint8_t>(), s);
+        select_u8(d->mask.as<uint8_t>(), n * L, d->items.as<uint32_t>(), d->count.as<uint32_t>(), d->scan,
+                  d->err.as<uint32_t>(), s);
+    }
+    uint32_t blocks = d->blocks;
+    if (plain) {
+        uint32_t cnt = 0;
+        cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, s), "count readback");
+        cuda_check(cudaStreamSynchronize(s), "frame sync");
+        d->last_items += cnt;
+        if (!cnt) return;
+        blocks = (cnt + kTravThreads - 1) / kTravThreads;
+    }
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 4, s), "memset");
+    DiscreteArgs A{};
+    A.T = d->T.as<float4>();
+    A.items = d->items.as<uint32_t>();
+    A.n_items = d->count.as<uint32_t>();
+    A.n_poses = n;
+    A.pose_hit = d_hit;
+    A.counts = (counts && !r2o) ? d_counts : nullptr;
+    A.edge_bits = (counts && r2o) ? d_bits : nullptr;
+    A.edge_words = (R.n_edges_total + 31) / 32;
+    A.work_counter = d->work.as<uint32_t>();
+    A.err = d->err.as<uint32_t>();
+    A.stats = d->stats.as<unsigned long long>();
+    A.want_counts = counts ? 1 : 0;
+    launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+    if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);
+}
+
+void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags_out, uint32_t* counts_out,
+                    uint32_t flags, cudaStream_t s) {
+    const bool host = (flags & RTCD_CHECK_HOST_BUFFERS) != 0;
+    const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
+    const uint32_t dof = d->robot->dof;
+    RobotDev& R = d->robot->dev;
+    const float* d_q = q;
+    if (host) {
+        d->q.ensure(4ull * n * dof);
+        d->pin_in.ensure(4ull * n * dof);
+        std::memcpy(d->pin_in.p, q, 4ull * n * dof);
+        cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * n * dof, cudaMemcpyHostToDevice, s), "q upload");
+        d_q = d->q.as<float>();
+    }
+    d->pose_hit.ensure(4ull * n);
+    cuda_check(cudaMemsetAsync(d->pose_hit.p, 0, 4ull * n, s), "memset");
+    uint32_t* d_counts = nullptr;
+    uint32_t* d_bits = nullptr;
+    uint32_t words = (R.n_edges_total + 31) / 32;
+    if (counts) {
+        if (host || !counts_out) {
+            d->counts.ensure(4ull * n);
+            d_counts = d->counts.as<uint32_t>();
+        } else {
+            d_counts = counts_out;
+        }
+        cuda_check(cudaMemsetAsync(d_counts, 0, 4ull * n, s), "memset");
+        if (d->kind == RTCD_ROBOT_TO_OBS) {
+            d->edge_bits.ensure(4ull * n * words);
+            d_bits = d->edge_bits.as<uint32_t>();
+            cuda_check(cudaMemsetAsync(d_bits, 0, 4ull * n * words, s), "memset");
+        }
+    }
+    d->last_items = 0;
+    if (flags & RTCD_CHECK_PLAIN) {
+        uint32_t fs = d->cfg.frame_size;
+        for (uint32_t start = 0; start < n; start += fs) {
+            uint32_t m = std::min(fs, n - start);
+            discrete_pass(d, d_q + (size_t) start * dof, m, d->pose_hit.as<uint32_t>() + start,
+                          d_counts ? d_counts + start : nullptr, d_bits ? d_bits + (size_t) start * words : nullptr,
+                          flags, true, s);
+        }
+    } else {
+        discrete_pass(d, d_q, n, d->pose_hit.as<uint32_t>(), d_counts, d_bits, flags, false, s);
+    }
+    uint8_t* d_flags = flags_out;
+    if (host || !flags_out) {
+        d->flags.ensure(n);
+        d_flags = d->flags.as<uint8_t>();
+    }
+    launch_flags(d->pose_hit.as<uint32_t>(), n, d_flags, s);
+    if (host) {
+        d->pin_out.ensure(5ull * n + 16);
+        uint8_t* pf = d->pin_out.as<uint8_t>();
+        uint32_t* pc = reinterpret_cast<uint32_t*>(pf + ((n + 15) & ~15u));
+        cuda_check(cudaMemcpyAsync(pf, d_flags, n, cudaMemcpyDeviceToHost, s), "flags download");
+        if (counts && counts_out)
+            cuda_check(cudaMemcpyAsync(pc, d_counts, 4ull * n, cudaMemcpyDeviceToHost, s), "counts download");
+        cuda_check(cudaStreamSynchronize(s), "check sync");
+        if (flags_out) std::memcpy(flags_out, pf, n);
+        if (counts && counts_out) std::memcpy(counts_out, pc, 4ull * n);
+    } else if (counts && counts_out && d_counts != counts_out) {
+        cuda_check(cudaMemcpyAsync(counts_out, d_counts, 4ull * n, cudaMemcpyDeviceToDevice, s), "counts copy");
+    }
+}
+
+void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uint32_t n, uint8_t* flags_out,
+                 uint8_t* seg_out, uint32_t* counts_out, uint32_t flags, cudaStream_t s) {
+    RTCD_REQUIRE(traj_off, "traj_offsets required for sweep detectors");
+    const bool host = (flags & RTCD_CHECK_HOST_BUFFERS) != 0;
+    const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
+    const bool quad = d->kind == RTCD_QUAD_SWEEP;
+    const bool want_pieces = seg_out != nullptr;
+    RobotDev& R = d->robot->dev;
+    const uint32_t dof = d->robot->dof, ns = R.n_spheres;
+    RTCD_REQUIRE(traj_off[0] == 0, "traj_offsets must start at 0");
+    uint32_t max_wp = 0;
+    uint64_t pieces = 0, ctrl_total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        RTCD_REQUIRE(traj_off[i + 1] >= traj_off[i], "traj_offsets must be non-decreasing");
+        uint32_t w = traj_off[i + 1] - traj_off[i];
+        RTCD_REQUIRE(w >= (quad ? 3u : 2u), quad ? "quadratic trajectories need >= 3 waypoints"
+                                                : "linear trajectories need >= 2 waypoints");
+        max_wp = std::max(max_wp, w);
+        pieces += pieces_of(d->kind, w, flags);
+        if (quad) ctrl_total += quad_ctrl_count(w);
+    }
+    RTCD_REQUIRE(pieces * ns < (1ull << 32), "too many sweep units in one call");
+    const uint32_t total_wp = traj_off[n];
+    if (quad) ensure_weights(d, max_wp);
+    // auxiliary tables: wp_off | piece_off | ctrl_off | piece_traj
+    const size_t aux_words = 3ull * (n + 1) + pieces;
+    cuda_check(cudaEventSynchronize(d->staged), "staging reuse");
+    d->pin_aux.ensure(4 * aux_words);
+    uint32_t* a = d->pin_aux.as<uint32_t>();
+    uint32_t* wp_off = a;
+    uint32_t* piece_off = a + (n + 1);
+    uint32_t* ctrl_off = a + 2 * (n + 1);
+    uint32_t* piece_traj = a + 3 * (n + 1);
+    wp_off[0] = piece_off[0] = ctrl_off[0] = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t w = traj_off[i + 1] - traj_off[i];
+        uint32_t p = pieces_of(d->kind, w, flags);
+        wp_off[i + 1] = traj_off[i + 1];
+        piece_off[i + 1] = piece_off[i] + p;
+        ctrl_off[i + 1] = ctrl_off[i] + (quad ? quad_ctrl_count(w) : 0);
+        for (uint32_t k = 0; k < p; ++k) piece_traj[piece_off[i] + k] = i;
+    }
+    d->aux.ensure(4 * aux_words);
+    cuda_check(cudaMemcpyAsync(d->aux.p, a, 4 * aux_words, cudaMemcpyHostToDevice, s), "aux upload");
+    const float* d_q = q;
+    if (host) {
+        d->q.ensure(4ull * total_wp * dof);
+        d->pin_in.ensure(4ull * total_wp * dof);
+        std::memcpy(d->pin_in.p, q, 4ull * total_wp * dof);
+        cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
+        d_q = d->q.as<float>();
+    }
+    cuda_check(cudaEventRecord(d->staged, s), "event");
+    const uint32_t* dwp = d->aux.as<uint32_t>();
+    const uint32_t* dpo = dwp + (n + 1);
+    const uint32_t* dco = dwp + 2 * (n + 1);
+    const uint32_t* dpt = dwp + 3 * (n + 1);
+    d->centers.ensure(16ull * total_wp * ns);
+    launch_fk_spheres(R, d_q, total_wp, d->centers.as<float4>(), s);
+    if (quad) {
+        d->ctrl.ensure(16ull * ctrl_total * ns);
+        launch_fit(d->centers.as<float4>(), dwp, dco, d->W.as<float>(), d->W_off.as<uint32_t>(), n, ns,
+                   d->ctrl.as<float4>(), s);
+    }
+    d->pose_hit.ensure(4ull * n);
+    cuda_check(cudaMemsetAsync(d->pose_hit.p, 0, 4ull * n, s), "memset");
+    if (want_pieces) {
+        d->piece_hit.ensure(4ull * pieces);
+        cuda_check(cudaMemsetAsync(d->piece_hit.p, 0, 4ull * pieces, s), "memset");
+    }
+    uint32_t* d_counts = nullptr;
+    if (counts) {
+        d->counts.ensure(4ull * n);
+        d_counts = d->counts.as<uint32_t>();
+        cuda_check(cudaMemsetAsync(d_counts, 0, 4ull * n, s), "memset");
+    }
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 4, s), "memset");
+    SweepArgs A{};
+    A.centers = d->centers.as<float4>();
+    A.ctrl = quad ? d->ctrl.as<float4>() : nullptr;
+    A.traj_piece_off = dpo;
+    A.traj_wp_off = dwp;
+    A.traj_ctrl_off = dco;
+    A.piece_traj = dpt;
+    A.n_traj = n;
+    A.n_spheres = ns;
+    A.total_units = (uint32_t) (pieces * ns);
+    A.quad = quad;
+    A.endpoints = !(flags & RTCD_CHECK_NO_ENDPOINTS);
+    A.traj_hit = d->pose_hit.as<uint32_t>();
+    A.piece_hit = want_pieces ? d->piece_hit.as<uint32_t>() : nullptr;
+    A.counts = d_counts;
+    A.work_counter = d->work.as<uint32_t>();
+    A.err = d->err.as<uint32_t>();
+    A.stats = d->stats.as<unsigned long long>();
+    A.want_counts = counts;
+    A.want_pieces = want_pieces;
+    d->last_items = A.total_units;
+    if (A.total_units) launch_sweep(d->scene->dev, A, d->blocks, s);
+    // outputs
+    uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
+    launch_flags(d->pose_hit.as<uint32_t>(), n, d_flags, s);
+    uint8_t* d_seg = nullptr;
+    if (want_pieces) {
+        d_seg = host ? (d->seg_flags.ensure(pieces), d->seg_flags.as<uint8_t>()) : seg_out;
+        launch_flags(d->piece_hit.as<uint32_t>(), (uint32_t) pieces, d_seg, s);
+    }
+    if (host) {
+        size_t fpad = (n + 15) & ~15ull, ppad = (pieces + 15) & ~15ull;
+        d->pin_out.ensure(fpad + ppad + 4ull * n + 16);
+        uint8_t* pf = d->pin_out.as<uint8_t>();
+        uint8_t* pp = pf + fpad;
+        uint32_t* pc = reinterpret_cast<uint32_t*>(pp + ppad);
+        cuda_check(cudaMemcpyAsync(pf, d_flags, n, cudaMemcpyDeviceToHost, s), "flags download");
+        if (want_pieces) cuda_check(cudaMemcpyAsync(pp, d_seg, pieces, cudaMemcpyDeviceToHost, s), "seg download");
+        if (counts && counts_out)
+            cuda_check(cudaMemcpyAsync(pc, d_counts, 4ull * n, cudaMemcpyDeviceToHost, s), "counts download");
+        cuda_check(cudaStreamSynchronize(s), "check sync");
+        if (flags_out) std::memcpy(flags_out, pf, n);
+        if (want_pieces) std::memcpy(seg_out, pp, pieces);
+        if (counts && counts_out) std::memcpy(counts_out, pc, 4ull * n);
+    } else if (counts && counts_out) {
+        cuda_check(cudaMemcpyAsync(counts_out, d_counts, 4ull * n, cudaMemcpyDeviceToDevice, s), "counts copy");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_offsets, uint32_t n, uint8_t* flags_out,
+                       uint8_t* seg_flags_out, uint32_t* counts_out, uint32_t flags, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(d, "NULL detector");
+        RTCD_REQUIRE(n == 0 || q, "q is NULL");
+        std::lock_guard<std::mutex> lock(d->mu);
+        DeviceScope ds(d->ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
+        if (n == 0) return;
+        if (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) {
+            RTCD_REQUIRE(!seg_flags_out, "segment flags exist only for sweep detectors");
+            check_discrete(d, q, n, flags_out, counts_out, flags, s);
+        } else {
+            RTCD_REQUIRE(!(flags & RTCD_CHECK_PLAIN), "the plain frame path is for the discrete detectors");
+            check_sweep(d, q, traj_offsets, n, flags_out, seg_flags_out, counts_out, flags, s);
+        }
+        if (flags & RTCD_CHECK_HOST_BUFFERS) check_device_errors(d, s);
+    });
+}
+
+rtcd_status rtcd_sync(rtcd_detector* d, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(d, "NULL detector");
+        std::lock_guard<std::mutex> lock(d->mu);
+        DeviceScope ds(d->ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
+        check_device_errors(d, s);
+    });
+}
+
+rtcd_status rtcd_segment_offsets(rtcd_detector_kind kind, const uint32_t* traj_offsets, uint32_t n, uint32_t flags,
+                                 uint32_t* offsets_out) {
+    return guarded([&] {
+        RTCD_REQUIRE(kind == RTCD_LINEAR_SWEEP || kind == RTCD_QUAD_SWEEP, "segments exist only for sweep kinds");
+        RTCD_REQUIRE(traj_offsets && offsets_out, "NULL argument");
+        offsets_out[0] = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            RTCD_REQUIRE(traj_offsets[i + 1] >= traj_offsets[i], "traj_offsets must be non-decreasing");
+            offsets_out[i + 1] = offsets_out[i] + pieces_of(kind, traj_offsets[i + 1] - traj_offsets[i], flags);
+        }
+    });
+}
+
+rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
+    return guarded([&] {
+        RTCD_REQUIRE(d && out, "NULL argument");
+        std::lock_guard<std::mutex> lock(d->mu);
+        DeviceScope ds(d->ctx->device);
+        std::memset(out, 0, sizeof(*out));
+        unsigned long long st[8] = {0};
+        uint32_t cnt = 0;
+        cuda_check(cudaMemcpyAsync(st, d->stats.p, sizeof(st), cudaMemcpyDeviceToHost, d->stream), "stats");
+        cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, d->stream), "stats");
+        cuda_check(cudaStreamSynchronize(d->stream), "stats sync");
+        out->fp64_retests = st[0];
+        out->work_items = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) && !d->last_items ? cnt
+                                                                                                          : d->last_items;
+    });
+}
+
+rtcd_status rtcd_robot_fk(rtcd_robot* r, const float* q_dev, uint32_t n, float* T_dev, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(r && (n == 0 || (q_dev && T_dev)), "NULL argument");
+        DeviceScope ds(r->ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : r->ctx->stream;
+        launch_fk_poses(r->dev.chain, q_dev, n, reinterpret_cast<float4*>(T_dev), s);
+    });
+}
+
+rtcd_status rtcd_exclusive_scan_u32(rtcd_ctx* ctx, const uint32_t* in_dev, uint32_t* out_dev, uint32_t n,
+                                    uint32_t* total_dev, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && (n == 0 || (in_dev && out_dev)), "NULL argument");
+        RTCD_REQUIRE(in_dev != out_dev, "in and out must differ");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : ctx->stream;
+        ScanScratch sc;
+        scan_u32(in_dev, out_dev, n, total_dev, sc, ctx->err.as<uint32_t>(), s);
+        cuda_check(cudaStreamSynchronize(s), "scan");  // the scratch is released on return
+    });
+}
+
+rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
+                                 uint32_t* count_dev, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && count_dev && (n == 0 || (mask_dev && idx_dev)), "NULL argument");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : ctx->stream;
+        ScanScratch sc;
+        select_u8(mask_dev, n, idx_dev, count_dev, sc, ctx->err.as<uint32_t>(), s);
+        cuda_check(cudaStreamSynchronize(s), "select");
+    });
+}
+
+rtcd_status rtcd_lbvh_build(rtcd_ctx* ctx, const float* lo, const float* hi, uint32_t n, uint32_t* codes_out,
+                            uint32_t* perm_out, uint32_t* child_out, float* node_lo, float* node_hi,
+                            uint32_t* depth_out) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && (n == 0 || (lo && hi)), "NULL argument");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = ctx->stream;
+        std::vector<float4> hl(n), hh(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            hl[i] = make_float4(lo[3 * i], lo[3 * i + 1], lo[3 * i + 2], 0.f);
+            hh[i] = make_float4(hi[3 * i], hi[3 * i + 1], hi[3 * i + 2], 0.f);
+        }
+        DevBuf dl, dh, nodes, perm;
+        upload(dl, hl.data(), n, s);
+        upload(dh, hh.data(), n, s);
+        nodes.ensure(64ull * std::max<uint32_t>(n, 2));
+        perm.ensure(4ull * std::max<uint32_t>(n, 1));
+        std::vector<uint32_t> codes, child;
+        LbvhResult res = build_lbvh(dl.as<float4>(), dh.as<float4>(), n, nodes.as<float4>(), perm.as<uint32_t>(), 0, 0,
+                                    ctx->err.as<uint32_t>(), s, &codes, &child);
+        if (depth_out) *depth_out = res.depth;
+        if (codes_out && n) std::memcpy(codes_out, codes.data(), 4ull * n);
+        if (perm_out && n) cuda_check(cudaMemcpy(perm_out, perm.p, 4ull * n, cudaMemcpyDeviceToHost), "perm");
+        if (child_out && n > 1) std::memcpy(child_out, child.data(), 8ull * (n - 1));
+        if ((node_lo || node_hi) && n > 1) {
+            std::vector<float4> pk(4ull * (n - 1));
+            cuda_check(cudaMemcpy(pk.data(), nodes.p, 64ull * (n - 1), cudaMemcpyDeviceToHost), "nodes");
+            // a node's own box is the union of the two child boxes packed in it
+            for (uint32_t i = 0; i < n - 1; ++i) {
+                const float4* p = &pk[4ull * i];
+                float l[3] = {std::min(p[0].x, p[1].z), std::min(p[0].y, p[1].w), std::min(p[0].z, p[2].x)};
+                float h[3] = {std::max(p[0].w, p[2].y), std::max(p[1].x, p[2].z), std::max(p[1].y, p[2].w)};
+                for (int k = 0; k < 3; ++k) {
+                    if (node_lo) node_lo[3ull * i + k] = l[k];
+                    if (node_hi) node_hi[3ull * i + k] = h[k];
+                }
+            }
+        }
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// kernels.h - device-side views and launchers of the query kernels.
+#pragma once
+#include "engine.h"
+
+namespace rtcd {
+
+// Robot resident on the device (passed by value to the kernels).
+struct RobotDev {
+    Chain chain;
+    uint32_t n_links;
+    uint32_t first_link;            // 1 when the base link is skipped
+    float obb[kMaxLinks][16];       // local OBB: centre(3), half(3), axes x/y/z (9), pad
+    const float4* tri_nodes;        // link triangle LBVHs (link frames)
+    const float4* tri_prims;        // 3 float4 per triangle
+    uint32_t tri_root[kMaxLinks];
+    const float4* edge_nodes;       // link edge LBVHs (link frames)
+    const float4* edge_prims;       // 2 float4 per edge; w of the first = global edge id
+    uint32_t edge_root[kMaxLinks];
+    uint32_t n_edges_total;
+    const float4* spheres;          // local centre xyz, radius w
+    const uint32_t* sphere_link;
+    uint32_t n_spheres;
+};
+
+// Scene resident on the device.
+struct SceneDev {
+    const float4* tri_nodes;
+    const float4* tri_prims;
+    uint32_t tri_root;
+    uint32_t n_tris;
+    const float4* edge_nodes;
+    const float4* edge_prims;
+    uint32_t edge_root;
+    uint32_t n_edges;
+    const float* obbs;  // 16 floats per obstacle: centre(3), half(3), axes(9), bounding radius
+    uint32_t n_obs;
+};
+
+struct DiscreteArgs {
+    const float4* T;           // [pose][link][3] link transforms
+    const uint32_t* items;     // compacted (pose * n_links + link); NULL = all links >= first_link
+    const uint32_t* n_items;   // device count of items
+    uint32_t n_poses;
+    uint32_t* pose_hit;        // [pose] nonzero when colliding
+    uint32_t* counts;          // [pose] upstream counts (ObsToRobot) or NULL
+    uint32_t* edge_bits;       // [pose][edge_words] RobotToObs hit-edge bitset or NULL
+    uint32_t edge_words;
+    uint32_t* work_counter;    // zeroed before launch
+    uint32_t* err;
+    unsigned long long* stats; // [0] fp64 re-tests
+    int want_counts;
+};
+
+constexpr int kFkThreads = 128;
+constexpr int kTravThreads = 128;
+
+void launch_fk_poses(const Chain& ch, const float* d_q, uint32_t n, float4* d_T, cudaStream_t s);
+void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, cudaStream_t s);
+void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t* d_count, cudaStream_t s);
+void launch_discrete(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t blocks,
+                     cudaStream_t s);
+void launch_popcount_rows(const uint32_t* d_bits, uint32_t words, uint32_t rows, uint32_t* d_out, cudaStream_t s);
+void launch_flags(const uint32_t* d_hit, uint32_t n, uint8_t* d_flags, cudaStream_t s);
+uint32_t discrete_persistent_blocks(bool robot_to_obs);
+
+// ---- sweeps
+struct SweepArgs {
+    const float4* centers;     // [waypoint][sphere] world centre xyz, radius w
+    const float4* ctrl;        // [control point][sphere] (quadratic) or NULL
+    const uint32_t* traj_piece_off;  // [n_traj + 1] prefix of pieces
+    const uint32_t* traj_wp_off;     // [n_traj + 1] waypoint offsets
+    const uint32_t* traj_ctrl_off;   // [n_traj + 1] control point offsets (quadratic)
+    const uint32_t* piece_traj;      // [pieces] owning trajectory of each piece
+    uint32_t n_traj;
+    uint32_t n_spheres;
+    uint32_t total_units;      // pieces * spheres
+    int quad;
+    int endpoints;
+    uint32_t* traj_hit;        // [n_traj]
+    uint32_t* piece_hit;       // [pieces] or NULL
+    uint32_t* counts;          // [n_traj] or NULL
+    uint32_t* work_counter;
+    uint32_t* err;
+    unsigned long long* stats;
+    int want_counts;
+    int want_pieces;
+};
+
+void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s);
+void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_t* d_ctrl_off, const float* d_W,
+                const uint32_t* d_W_off, uint32_t n_traj, uint32_t n_spheres, float4* d_ctrl, cudaStream_t s);
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, cudaStream_t s);
+uint32_t sweep_persistent_blocks();
+
+}  // namespace rtcd

@@ -1,0 +1,436 @@
+// lbvh.cu - device LBVH builder and the shared scan/select launchers.
+//
+// Replaces the OptiX GAS/IAS builds of the upstream path (optixAccelBuild in
+// RTCD/Meshes/mesh.h:725-740, :798-815, RTCD/CollisionScenes/scene.h:138-145).
+// The tree is the canonical one: 30-bit Morton codes of the float centroids
+// normalised by the centroid bounds, a stable sort by (code, index), the
+// Karras 2012 hierarchy ("Maximizing Parallelism in the Construction of BVHs,
+// Octrees, and k-d Trees") with index tie-breaks for equal codes, one
+// primitive per leaf and an atomic bottom-up box fit.  Every float step uses
+// explicitly rounded intrinsics so the tree is bit-identical to the CPU
+// restatement in the oracle.
+#include <algorithm>
+
+#include "engine.h"
+#include "scan.cuh"
+
+namespace rtcd {
+
+// ---------------------------------------------------------------- scan glue
+void ScanScratch::prepare(uint32_t n_items, cudaStream_t s) {
+    uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n_items));
+    status.ensure(sizeof(unsigned long long) * tiles);
+    counter.ensure(sizeof(uint32_t));
+    cuda_check(cudaMemsetAsync(status.p, 0, sizeof(unsigned long long) * tiles, s), "scan status memset");
+    cuda_check(cudaMemsetAsync(counter.p, 0, sizeof(uint32_t), s), "scan counter memset");
+}
+
+void scan_u32(const uint32_t* d_in, uint32_t* d_out, uint32_t n, uint32_t* d_total, ScanScratch& sc, uint32_t* d_err,
+              cudaStream_t s) {
+    sc.prepare(n, s);
+    uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
+    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err};
+    k_scan_u32<<<tiles, kScanThreads, 0, s>>>(d_in, d_out, n, st, d_total);
+    cuda_check(cudaGetLastError(), "k_scan_u32");
+}
+
+void select_u8(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_count, ScanScratch& sc, uint32_t* d_err,
+               cudaStream_t s) {
+    sc.prepare(n, s);
+    uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
+    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err};
+    k_select_u8<<<tiles, kScanThreads, 0, s>>>(d_mask, n, d_out, d_count, st);
+    cuda_check(cudaGetLastError(), "k_select_u8");
+}
+
+// ---------------------------------------------------------------- prim boxes
+__global__ void k_tri_boxes(const float* __restrict__ v, const uint32_t* __restrict__ t, uint32_t n, float4* lo,
+                            float4* hi) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* a = v + 3ull * t[3ull * i];
+    const float* b = v + 3ull * t[3ull * i + 1];
+    const float* c = v + 3ull * t[3ull * i + 2];
+    lo[i] = make_float4(fminf(a[0], fminf(b[0], c[0])), fminf(a[1], fminf(b[1], c[1])), fminf(a[2], fminf(b[2], c[2])), 0.f);
+    hi[i] = make_float4(fmaxf(a[0], fmaxf(b[0], c[0])), fmaxf(a[1], fmaxf(b[1], c[1])), fmaxf(a[2], fmaxf(b[2], c[2])), 0.f);
+}
+
+__global__ void k_edge_boxes(const float* __restrict__ v, const uint32_t* __restrict__ e, uint32_t n, float4* lo,
+                             float4* hi) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* a = v + 3ull * e[2ull * i];
+    const float* b = v + 3ull * e[2ull * i + 1];
+    lo[i] = make_float4(fminf(a[0], b[0]), fminf(a[1], b[1]), fminf(a[2], b[2]), 0.f);
+    hi[i] = make_float4(fmaxf(a[0], b[0]), fmaxf(a[1], b[1]), fmaxf(a[2], b[2]), 0.f);
+}
+
+void tri_boxes(const float* d_verts, const uint32_t* d_tris, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s) {
+    if (!n) return;
+    k_tri_boxes<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_tris, n, d_lo, d_hi);
+    cuda_check(cudaGetLastError(), "k_tri_boxes");
+}
+
+void edge_boxes(const float* d_verts, const uint32_t* d_edges, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s) {
+    if (!n) return;
+    k_edge_boxes<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_edges, n, d_lo, d_hi);
+    cuda_check(cudaGetLastError(), "k_edge_boxes");
+}
+
+__global__ void k_gather_tris(const float* __restrict__ v, const uint32_t* __restrict__ t,
+                              const uint32_t* __restrict__ perm, uint32_t n, uint32_t id_base, uint32_t group,
+                              float4* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t p = perm[i];
+    const float* a = v + 3ull * t[3ull * p];
+    const float* b = v + 3ull * t[3ull * p + 1];
+    const float* c = v + 3ull * t[3ull * p + 2];
+    out[3ull * i] = make_float4(a[0], a[1], a[2], __uint_as_float(id_base + p));
+    out[3ull * i + 1] = make_float4(b[0], b[1], b[2], __uint_as_float(group));
+    out[3ull * i + 2] = make_float4(c[0], c[1], c[2], 0.f);
+}
+
+__global__ void k_gather_edges(const float* __restrict__ v, const uint32_t* __restrict__ e,
+                               const uint32_t* __restrict__ perm, uint32_t n, uint32_t id_base, uint32_t group,
+                               float4* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t p = perm[i];
+    const float* a = v + 3ull * e[2ull * p];
+    const float* b = v + 3ull * e[2ull * p + 1];
+    out[2ull * i] = make_float4(a[0], a[1], a[2], __uint_as_float(id_base + p));
+    out[2ull * i + 1] = make_float4(b[0], b[1], b[2], __uint_as_float(group));
+}
+
+void gather_tris(const float* d_verts, const uint32_t* d_tris, const uint32_t* d_perm, uint32_t n, uint32_t id_base,
+                 uint32_t group, float4* d_out, cudaStream_t s) {
+    if (!n) return;
+    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_tris, d_perm, n, id_base, group, d_out);
+    cuda_check(cudaGetLastError(), "k_gather_tris");
+}
+
+void gather_edges(const float* d_verts, const uint32_t* d_edges, const uint32_t* d_perm, uint32_t n, uint32_t id_base,
+                  uint32_t group, float4* d_out, cudaStream_t s) {
+    if (!n) return;
+    k_gather_edges<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_edges, d_perm, n, id_base, group, d_out);
+    cuda_check(cudaGetLastError(), "k_gather_edges");
+}
+
+// ---------------------------------------------------------------- Morton codes
+__device__ __forceinline__ uint32_t fenc(float f) {
+    uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float fdec(uint32_t e) {
+    uint32_t b = (e & 0x80000000u) ? (e & 0x7fffffffu) : ~e;
+    return __uint_as_float(b);
+}
+
+__device__ __forceinline__ float centroid(float lo, float hi) { return __fmul_rn(0.5f, __fadd_rn(lo, hi)); }
+
+// bounds[0..2] = encoded min, bounds[3..5] = encoded max of the centroids
+__global__ void k_centroid_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi, uint32_t n,
+                                  uint32_t* bounds) {
+    uint32_t mn[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, mx[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 a = lo[i], b = hi[i];
+        uint32_t c[3] = {fenc(centroid(a.x, b.x)), fenc(centroid(a.y, b.y)), fenc(centroid(a.z, b.z))};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = min(mn[k], c[k]);
+            mx[k] = max(mx[k], c[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = min(mn[k], __shfl_xor_sync(0xffffffffu, mn[k], o));
+            mx[k] = max(mx[k], __shfl_xor_sync(0xffffffffu, mx[k], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(bounds + k, mn[k]);
+            atomicMax(bounds + 3 + k, mx[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t quantize(float c, float lo, float ext) {
+    float t = ext > 0.0f ? __fdiv_rn(__fsub_rn(c, lo), ext) : 0.0f;
+    float v = __fmul_rn(t, 1024.0f);
+    if (!(v >= 0.0f)) v = 0.0f;
+    uint32_t q = (uint32_t) floorf(v);
+    return q > 1023u ? 1023u : q;
+}
+
+__global__ void k_morton(const float4* __restrict__ lo, const float4* __restrict__ hi, uint32_t n,
+                         const uint32_t* __restrict__ bounds, uint32_t* codes, uint32_t* idx) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float clo[3], ext[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        clo[k] = fdec(bounds[k]);
+        ext[k] = __fsub_rn(fdec(bounds[3 + k]), clo[k]);
+    }
+    float4 a = lo[i], b = hi[i];
+    uint32_t qx = quantize(centroid(a.x, b.x), clo[0], ext[0]);
+    uint32_t qy = quantize(centroid(a.y, b.y), clo[1], ext[1]);
+    uint32_t qz = quantize(centroid(a.z, b.z), clo[2], ext[2]);
+    codes[i] = (expand_bits(qx) << 2) | (expand_bits(qy) << 1) | expand_bits(qz);
+    idx[i] = i;
+}
+
+// ---------------------------------------------------------------- radix sort
+// Stable LSD radix sort of (code, index) pairs, 8-bit digits.  Per digit pass:
+// a per-tile histogram, a decoupled look-back scan of the digit-major
+// histogram, and a scatter that ranks keys stably inside the tile with warp
+// match masks.
+constexpr int kRsThreads = 256;
+constexpr int kRsRounds = 8;
+constexpr int kRsTile = kRsThreads * kRsRounds;
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
+                                                       uint32_t n_tiles, uint32_t* hist) {
+    __shared__ uint32_t cnt[256];
+    cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const size_t base = (size_t) blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsRounds; ++r) {
+        size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
+        if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[(size_t) threadIdx.x * n_tiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t* __restrict__ kin,
+                                                          const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+                                                          uint32_t* __restrict__ vout, uint32_t n, int shift,
+                                                          uint32_t n_tiles, const uint32_t* __restrict__ offsets) {
+    constexpr int W = kRsThreads / 32;
+    __shared__ uint32_t run[256];
+    __shared__ uint32_t wcnt[W][256];
+    __shared__ uint32_t goff[256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    run[threadIdx.x] = 0;
+    goff[threadIdx.x] = offsets[(size_t) threadIdx.x * n_tiles + blockIdx.x];
+    const size_t base = (size_t) blockIdx.x * kRsTile;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (int r = 0; r < kRsRounds; ++r) {
+#pragma unroll
+        for (int w = 0; w < W; ++w) wcnt[w][threadIdx.x] = 0;
+        __syncthreads();
+        size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
+        bool valid = i < n;
+        uint32_t key = valid ? kin[i] : 0u, val = valid ? vin[i] : 0u;
+        uint32_t d = valid ? ((key >> shift) & 255u) : 256u;
+        uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t rank = __popc(peers & lt);
+        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
+        __syncthreads();
+        {
+            uint32_t dd = threadIdx.x, acc = run[dd];
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                uint32_t t = wcnt[w][dd];
+                wcnt[w][dd] = acc;
+                acc += t;
+            }
+            run[dd] = acc;
+        }
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = goff[d] + wcnt[warp][d] + rank;
+            kout[pos] = key;
+            vout[pos] = val;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- hierarchy
+__device__ __forceinline__ int kdelta(const uint32_t* codes, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t x = codes[i] ^ codes[j];
+    if (x) return __clz(x);
+    return 32 + __clz((uint32_t) i ^ (uint32_t) j);
+}
+
+// child refs: internal node index, or kLeaf | sorted position; parent[n-1+s] for leaves.
+__global__ void k_karras(const uint32_t* __restrict__ codes, int n, uint32_t* child, uint32_t* parent) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (kdelta(codes, n, i, i + 1) - kdelta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = kdelta(codes, n, i, i - d);
+    int lmax = 2;
+    while (kdelta(codes, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (kdelta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = kdelta(codes, n, i, j);
+    int s = 0;
+    for (int div = 2;; div *= 2) {
+        int t = (l + div - 1) / div;
+        if (kdelta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t <= 1) break;
+    }
+    int g = i + s * d + (d < 0 ? -1 : 0);
+    int lo = min(i, j), hi = max(i, j);
+    uint32_t left = (lo == g) ? (kLeaf | (uint32_t) g) : (uint32_t) g;
+    uint32_t right = (hi == g + 1) ? (kLeaf | (uint32_t) (g + 1)) : (uint32_t) (g + 1);
+    child[2 * i] = left;
+    child[2 * i + 1] = right;
+    parent[(left & kLeaf) ? (n - 1 + (left & ~kLeaf)) : left] = (uint32_t) i;
+    parent[(right & kLeaf) ? (n - 1 + (right & ~kLeaf)) : right] = (uint32_t) i;
+}
+
+__device__ __forceinline__ void child_box(uint32_t ref, const uint32_t* perm, const float4* plo, const float4* phi,
+                                          const float4* nlo, const float4* nhi, float4& lo, float4& hi) {
+    if (ref & kLeaf) {
+        uint32_t p = perm[ref & ~kLeaf];
+        lo = plo[p];
+        hi = phi[p];
+    } else {
+        lo = __ldcg(nlo + ref);
+        hi = __ldcg(nhi + ref);
+    }
+}
+
+// Bottom-up fit: the second thread to reach a node computes its box.
+__global__ void k_fit(const uint32_t* __restrict__ child, const uint32_t* __restrict__ parent,
+                      const uint32_t* __restrict__ perm, const float4* __restrict__ plo, const float4* __restrict__ phi,
+                      int n, float4* nlo, float4* nhi, uint32_t* visits) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t node = parent[n - 1 + s];
+    for (int guard = 0; guard < 2 * n + 2; ++guard) {
+        __threadfence();
+        if (atomicAdd(visits + node, 1u) == 0) return;
+        float4 al, ah, bl, bh;
+        child_box(child[2 * node], perm, plo, phi, nlo, nhi, al, ah);
+        child_box(child[2 * node + 1], perm, plo, phi, nlo, nhi, bl, bh);
+        float4 lo = make_float4(fminf(al.x, bl.x), fminf(al.y, bl.y), fminf(al.z, bl.z), 0.f);
+        float4 hi = make_float4(fmaxf(ah.x, bh.x), fmaxf(ah.y, bh.y), fmaxf(ah.z, bh.z), 0.f);
+        __stcg(nlo + node, lo);
+        __stcg(nhi + node, hi);
+        if (node == 0) return;
+        node = parent[node];
+    }
+}
+
+__global__ void k_leaf_depth(const uint32_t* __restrict__ parent, int n, uint32_t* max_depth) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t node = parent[n - 1 + s], d = 1;
+    while (node != 0 && d < 4096u) {
+        node = parent[node];
+        ++d;
+    }
+    atomicMax(max_depth, d);
+}
+
+__global__ void k_pack(const uint32_t* __restrict__ child, const uint32_t* __restrict__ perm,
+                       const float4* __restrict__ plo, const float4* __restrict__ phi, const float4* __restrict__ nlo,
+                       const float4* __restrict__ nhi, int n, uint32_t node_offset, uint32_t prim_offset,
+                       float4* nodes) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    uint32_t cl = child[2 * i], cr = child[2 * i + 1];
+    float4 al, ah, bl, bh;
+    child_box(cl, perm, plo, phi, nlo, nhi, al, ah);
+    child_box(cr, perm, plo, phi, nlo, nhi, bl, bh);
+    uint32_t rl = (cl & kLeaf) ? (kLeaf | (prim_offset + (cl & ~kLeaf))) : (node_offset + cl);
+    uint32_t rr = (cr & kLeaf) ? (kLeaf | (prim_offset + (cr & ~kLeaf))) : (node_offset + cr);
+    float4* o = nodes + 4ull * i;
+    o[0] = make_float4(al.x, al.y, al.z, ah.x);
+    o[1] = make_float4(ah.y, ah.z, bl.x, bl.y);
+    o[2] = make_float4(bl.z, bh.x, bh.y, bh.z);
+    o[3] = make_float4(__uint_as_float(rl), __uint_as_float(rr), 0.f, 0.f);
+}
+
+LbvhResult build_lbvh(const float4* d_lo, const float4* d_hi, uint32_t n, float4* d_nodes, uint32_t* d_perm,
+                      uint32_t node_offset, uint32_t prim_offset, uint32_t* d_err, cudaStream_t s,
+                      std::vector<uint32_t>* codes_out, std::vector<uint32_t>* child_out) {
+    LbvhResult r;
+    if (n == 0) return r;
+    if (n >= (1u << 30)) fail(5, "LBVH: too many primitives");
+    DevBuf bounds, codes_a, codes_b, idx_a, idx_b, hist, offs, child, parent, nlo, nhi, visits, depth;
+    ScanScratch sc;
+    bounds.ensure(6 * sizeof(uint32_t));
+    uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    cuda_check(cudaMemcpyAsync(bounds.p, init, sizeof(init), cudaMemcpyHostToDevice, s), "bounds init");
+    int sms = device_sm_count();
+    k_centroid_bounds<<<std::max(1, std::min<int>((n + 255) / 256, sms * 4)), 256, 0, s>>>(d_lo, d_hi, n,
+                                                                                           bounds.as<uint32_t>());
+    codes_a.ensure(4ull * n); codes_b.ensure(4ull * n); idx_a.ensure(4ull * n); idx_b.ensure(4ull * n);
+    k_morton<<<(n + 255) / 256, 256, 0, s>>>(d_lo, d_hi, n, bounds.as<uint32_t>(), codes_a.as<uint32_t>(),
+                                             idx_a.as<uint32_t>());
+    cuda_check(cudaGetLastError(), "k_morton");
+    uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+    hist.ensure(4ull * 256 * tiles);
+    offs.ensure(4ull * 256 * tiles);
+    uint32_t *ka = codes_a.as<uint32_t>(), *kb = codes_b.as<uint32_t>(), *va = idx_a.as<uint32_t>(),
+             *vb = idx_b.as<uint32_t>();
+    for (int shift = 0; shift < 30; shift += 8) {
+        k_rs_hist<<<tiles, kRsThreads, 0, s>>>(ka, n, shift, tiles, hist.as<uint32_t>());
+        scan_u32(hist.as<uint32_t>(), offs.as<uint32_t>(), 256 * tiles, nullptr, sc, d_err, s);
+        k_rs_scatter<<<tiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, tiles, offs.as<uint32_t>());
+        cuda_check(cudaGetLastError(), "radix pass");
+        std::swap(ka, kb);
+        std::swap(va, vb);
+    }
+    cuda_check(cudaMemcpyAsync(d_perm, va, 4ull * n, cudaMemcpyDeviceToDevice, s), "perm copy");
+    if (codes_out) {
+        codes_out->resize(n);
+        cuda_check(cudaMemcpyAsync(codes_out->data(), ka, 4ull * n, cudaMemcpyDeviceToHost, s), "codes download");
+    }
+    if (n == 1) {
+        cuda_check(cudaStreamSynchronize(s), "lbvh sync");
+        r.root = kLeaf | prim_offset;
+        r.depth = 0;
+        return r;
+    }
+    child.ensure(8ull * (n - 1));
+    parent.ensure(4ull * (2 * n - 1));
+    nlo.ensure(16ull * (n - 1));
+    nhi.ensure(16ull * (n - 1));
+    visits.ensure(4ull * (n - 1));
+    depth.ensure(4);
+    cuda_check(cudaMemsetAsync(visits.p, 0, 4ull * (n - 1), s), "visits memset");
+    cuda_check(cudaMemsetAsync(depth.p, 0, 4, s), "depth memset");
+    k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(ka, (int) n, child.as<uint32_t>(), parent.as<uint32_t>());
+    k_fit<<<(n + 255) / 256, 256, 0, s>>>(child.as<uint32_t>(), parent.as<uint32_t>(), d_perm, d_lo, d_hi, (int) n,
+                                          nlo.as<float4>(), nhi.as<float4>(), visits.as<uint32_t>());
+    k_leaf_depth<<<(n + 255) / 256, 256, 0, s>>>(parent.as<uint32_t>(), (int) n, depth.as<uint32_t>());
+    k_pack<<<(n - 1 + 255) / 256, 256, 0, s>>>(child.as<uint32_t>(), d_perm, d_lo, d_hi, nlo.as<float4>(),
+                                               nhi.as<float4>(), (int) n, node_offset, prim_offset, d_nodes);
+    cuda_check(cudaGetLastError(), "lbvh hierarchy");
+    if (child_out) {
+        child_out->resize(2ull * (n - 1));
+        cuda_check(cudaMemcpyAsync(child_out->data(), child.p, 8ull * (n - 1), cudaMemcpyDeviceToHost, s),
+                   "child download");
+    }
+    uint32_t dep = 0;
+    cuda_check(cudaMemcpyAsync(&dep, depth.p, 4, cudaMemcpyDeviceToHost, s), "depth download");
+    cuda_check(cudaStreamSynchronize(s), "lbvh sync");
+    r.root = node_offset;
+    r.depth = dep;
+    if (dep > (uint32_t) kMaxTreeDepth) fail(5, "LBVH deeper than the traversal stack (" + std::to_string(dep) + ")");
+    return r;
+}
+
+}  // namespace rtcd

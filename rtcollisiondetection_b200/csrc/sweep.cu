@@ -1,0 +1,402 @@
+// sweep.cu - continuous detectors: piecewise-linear (capsule) and quadratic
+// B-spline swept spheres.
+//
+// Upstream (RTCD/Robot/batchCurveRobot.h:341-403, RTCD/Robot/sweptVolume.cu:
+// 22-96, RTCD/CollisionDetector/CCCuda.cu:37-41): FK per waypoint, sphere
+// centres per waypoint, (quadratic) control points C = W P, a full OptiX curve
+// GAS rebuild per batch, then one RT-core ray per obstacle loop edge against
+// the built-in ROUND_LINEAR / ROUND_QUADRATIC_BSPLINE intersectors.
+//
+// Here nothing is rebuilt per batch: the obstacle edges sit in a resident
+// LBVH and each swept primitive (one sphere over one trajectory piece)
+// queries it with its bounding box - the primitive-side traversal of the same
+// predicate "some obstacle edge comes within r of the sphere path".  A unit is
+// (piece, sphere); lanes pull units from a device counter, units of uneven
+// trajectories share one launch, and a piece (or a trajectory) stops once it
+// is flagged.  The exact tests run in FP32 and fall back to FP64 inside a
+// narrow band around the radius: for the quadratic piece the FP64 step is a
+// safeguarded Newton polish of the stationary points of the squared distance.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace cg = cooperative_groups;
+
+namespace rtcd {
+
+// ---------------------------------------------------------------- FK + sphere centres
+constexpr int kWpPerBlock = 32;
+
+__global__ void __launch_bounds__(kWpPerBlock) k_fk_spheres(const RobotDev R, const float* __restrict__ q, uint32_t n_wp,
+                                                           float4* __restrict__ centers) {
+    __shared__ float sT[kWpPerBlock][kMaxLinks][12];
+    uint32_t w = blockIdx.x * kWpPerBlock + threadIdx.x;
+    if (w < n_wp) {
+        float qq[kMaxDof];
+        for (int k = 0; k < R.chain.dof; ++k) qq[k] = q[(size_t) w * R.chain.dof + k];
+        fk_chain(R.chain, qq, sT[threadIdx.x]);
+    }
+    __syncthreads();
+    uint32_t nw = min((uint32_t) kWpPerBlock, n_wp - blockIdx.x * kWpPerBlock);
+    for (uint32_t idx = threadIdx.x; idx < nw * R.n_spheres; idx += kWpPerBlock) {
+        uint32_t wl = idx / R.n_spheres, s = idx % R.n_spheres;
+        const float* T = sT[wl][R.sphere_link[s]];
+        float4 p = R.spheres[s];
+        centers[((size_t) blockIdx.x * kWpPerBlock + wl) * R.n_spheres + s] =
+            make_float4(T[0] * p.x + T[1] * p.y + T[2] * p.z + T[3], T[4] * p.x + T[5] * p.y + T[6] * p.z + T[7],
+                        T[8] * p.x + T[9] * p.y + T[10] * p.z + T[11], p.w);
+    }
+}
+
+void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s) {
+    if (!n_wp) return;
+    k_fk_spheres<<<(n_wp + kWpPerBlock - 1) / kWpPerBlock, kWpPerBlock, 0, s>>>(R, d_q, n_wp, d_centers);
+    cuda_check(cudaGetLastError(), "k_fk_spheres");
+}
+
+// ---------------------------------------------------------------- quadratic fit
+// One block per trajectory: C[k][s] = sum_t W_n[k][t] P[t][s]
+// (upstream genCtrlPtsKern, RTCD/Robot/sweptVolume.cu:22-83).  W_n, the
+// least-squares fit for n waypoints, comes from a table indexed by n.
+__global__ void __launch_bounds__(256) k_fit(const float4* __restrict__ centers, const uint32_t* __restrict__ wp_off,
+                                            const uint32_t* __restrict__ ctrl_off, const float* __restrict__ W,
+                                            const uint32_t* __restrict__ W_off, uint32_t ns, float4* __restrict__ ctrl) {
+    uint32_t tr = blockIdx.x;
+    uint32_t w0 = wp_off[tr], nwp = wp_off[tr + 1] - w0;
+    uint32_t c0 = ctrl_off[tr], nc = ctrl_off[tr + 1] - c0;
+    const float* Wn = W + W_off[nwp];
+    for (uint32_t idx = threadIdx.x; idx < nc * ns; idx += blockDim.x) {
+        uint32_t k = idx / ns, s = idx % ns;
+        float x = 0.f, y = 0.f, z = 0.f;
+        const float* wr = Wn + (size_t) k * nwp;
+        for (uint32_t t = 0; t < nwp; ++t) {
+            float wt = __ldg(wr + t);
+            float4 p = __ldg(centers + (size_t) (w0 + t) * ns + s);
+            x = fmaf(wt, p.x, x);
+            y = fmaf(wt, p.y, y);
+            z = fmaf(wt, p.z, z);
+        }
+        float r = __ldg(centers + (size_t) w0 * ns + s).w;
+        ctrl[(size_t) (c0 + k) * ns + s] = make_float4(x, y, z, r);
+    }
+}
+
+void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_t* d_ctrl_off, const float* d_W,
+                const uint32_t* d_W_off, uint32_t n_traj, uint32_t n_spheres, float4* d_ctrl, cudaStream_t s) {
+    if (!n_traj) return;
+    k_fit<<<n_traj, 256, 0, s>>>(d_centers, d_wp_off, d_ctrl_off, d_W, d_W_off, n_spheres, d_ctrl);
+    cuda_check(cudaGetLastError(), "k_fit");
+}
+
+// ---------------------------------------------------------------- exact distances
+template <class T>
+struct V3 {
+    T x, y, z;
+};
+template <class T>
+__device__ __forceinline__ V3<T> vm(T x, T y, T z) { return V3<T>{x, y, z}; }
+template <class T>
+__device__ __forceinline__ V3<T> vsub(V3<T> a, V3<T> b) { return vm<T>(a.x - b.x, a.y - b.y, a.z - b.z); }
+template <class T>
+__device__ __forceinline__ V3<T> vadd(V3<T> a, V3<T> b) { return vm<T>(a.x + b.x, a.y + b.y, a.z + b.z); }
+template <class T>
+__device__ __forceinline__ V3<T> vscale(V3<T> a, T s) { return vm<T>(a.x * s, a.y * s, a.z * s); }
+template <class T>
+__device__ __forceinline__ T vdot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class T>
+__device__ __forceinline__ T clamp01(T v) { return v < T(0) ? T(0) : (v > T(1) ? T(1) : v); }
+
+template <class T>
+__device__ __forceinline__ V3<T> v3cast(float4 v) { return vm<T>((T) v.x, (T) v.y, (T) v.z); }
+
+// Squared distance between segments p1q1 and p2q2 (Ericson, Real-Time
+// Collision Detection, 5.1.9).
+template <class T>
+__device__ T seg_seg2(V3<T> p1, V3<T> q1, V3<T> p2, V3<T> q2) {
+    V3<T> d1 = vsub(q1, p1), d2 = vsub(q2, p2), r = vsub(p1, p2);
+    T a = vdot(d1, d1), e = vdot(d2, d2), f = vdot(d2, r);
+    T s, t;
+    if (a <= T(0) && e <= T(0)) return vdot(r, r);
+    if (a <= T(0)) {
+        s = T(0);
+        t = clamp01(f / e);
+    } else {
+        T c = vdot(d1, r);
+        if (e <= T(0)) {
+            t = T(0);
+            s = clamp01(-c / a);
+        } else {
+            T b = vdot(d1, d2), den = a * e - b * b;
+            s = den > T(0) ? clamp01((b * f - c * e) / den) : T(0);
+            t = (b * s + f) / e;
+            if (t < T(0)) {
+                t = T(0);
+                s = clamp01(-c / a);
+            } else if (t > T(1)) {
+                t = T(1);
+                s = clamp01((b - c) / a);
+            }
+        }
+    }
+    V3<T> dd = vsub(vadd(p1, vscale(d1, s)), vadd(p2, vscale(d2, t)));
+    return vdot(dd, dd);
+}
+
+// Real roots of a u^2 + b u + c (numerically stable form); returns the count.
+template <class T>
+__device__ __forceinline__ int quad_roots(T a, T b, T c, T* r) {
+    if (a == T(0)) {
+        if (b == T(0)) return 0;
+        r[0] = -c / b;
+        return 1;
+    }
+    T disc = b * b - T(4) * a * c;
+    if (disc < T(0)) return 0;
+    T sq = sqrt(disc);
+    T qq = T(-0.5) * (b + (b >= T(0) ? sq : -sq));
+    int n = 0;
+    r[n++] = qq / a;
+    if (qq != T(0)) r[n++] = c / qq;
+    return n;
+}
+
+template <class T>
+__device__ __forceinline__ T poly3(const T* c, T u) { return ((c[3] * u + c[2]) * u + c[1]) * u + c[0]; }
+
+// Roots in [0, 1] of the cubic c[3] u^3 + ... + c[0]: the derivative's roots
+// split [0, 1] into monotone brackets, each bracket with a sign change is
+// solved by safeguarded Newton (falls back to bisection when a step leaves the
+// bracket).  `iters` Newton steps per bracket.
+template <class T>
+__device__ int cubic_roots01(const T* c, T* out, int iters) {
+    T br[4];
+    int nb = 0;
+    br[nb++] = T(0);
+    T cr[2];
+    int ncr = quad_roots(T(3) * c[3], T(2) * c[2], c[1], cr);
+    if (ncr == 2 && cr[0] > cr[1]) {
+        T t = cr[0];
+        cr[0] = cr[1];
+        cr[1] = t;
+    }
+    for (int k = 0; k < ncr; ++k)
+        if (cr[k] > T(0) && cr[k] < T(1)) br[nb++] = cr[k];
+    br[nb++] = T(1);
+    int n = 0;
+    for (int k = 0; k + 1 < nb; ++k) {
+        T lo = br[k], hi = br[k + 1];
+        T flo = poly3(c, lo), fhi = poly3(c, hi);
+        if (flo == T(0)) {
+            out[n++] = lo;
+            continue;
+        }
+        if ((flo > T(0)) == (fhi > T(0))) continue;
+        T u = T(0.5) * (lo + hi);
+        for (int it = 0; it < iters; ++it) {
+            T f = poly3(c, u);
+            if ((f > T(0)) == (flo > T(0))) lo = u; else hi = u;
+            T df = (T(3) * c[3] * u + T(2) * c[2]) * u + c[1];
+            T nu = df != T(0) ? u - f / df : T(0.5) * (lo + hi);
+            if (!(nu > lo && nu < hi)) nu = T(0.5) * (lo + hi);
+            u = nu;
+        }
+        out[n++] = u;
+    }
+    return n;
+}
+
+// Squared distance from the quadratic Bezier C(u) = A2 u^2 + A1 u + A0
+// (coordinates relative to the segment start) to the segment [0, d].
+template <class T>
+__device__ __forceinline__ T g_at(V3<T> A2, V3<T> A1, V3<T> A0, V3<T> d, T dd, T u) {
+    V3<T> w = vadd(vadd(vscale(A2, u * u), vscale(A1, u)), A0);
+    T s = dd > T(0) ? clamp01(vdot(w, d) / dd) : T(0);
+    V3<T> e = vsub(w, vscale(d, s));
+    return vdot(e, e);
+}
+
+// Minimum over u in [0, 1] of the squared distance from the Bezier piece
+// (B0, B1, B2) to the segment pq.  The distance is a piecewise quartic in u
+// whose pieces switch where the closest segment point reaches an end (s = 0
+// or 1); its minimum lies at u = 0, u = 1, a switch point (root of a
+// quadratic) or a stationary point of one of the three quartics (root of a
+// cubic).  All candidates are evaluated on the exact piecewise function.
+template <class T>
+__device__ T seg_quad2(V3<T> p, V3<T> q, V3<T> B0, V3<T> B1, V3<T> B2, int iters) {
+    V3<T> A0 = vsub(B0, p);
+    V3<T> A1 = vscale(vsub(B1, B0), T(2));
+    V3<T> A2 = vadd(vsub(B0, vscale(B1, T(2))), B2);
+    V3<T> d = vsub(q, p);
+    T dd = vdot(d, d);
+    T best = g_at(A2, A1, A0, d, dd, T(0));
+    T g1 = g_at(A2, A1, A0, d, dd, T(1));
+    if (g1 < best) best = g1;
+    T cand[4];
+    if (dd > T(0)) {
+        T pa = vdot(A2, d), pb = vdot(A1, d), pc = vdot(A0, d);
+        for (int k = 0; k < 2; ++k) {
+            int n = quad_roots(pa, pb, pc - (k ? dd : T(0)), cand);
+            for (int j = 0; j < n; ++j)
+                if (cand[j] > T(0) && cand[j] < T(1)) {
+                    T g = g_at(A2, A1, A0, d, dd, cand[j]);
+                    if (g < best) best = g;
+                }
+        }
+    }
+    // stationary points: w.w' for the ends, w.w' - (w.d)(w'.d)/|d|^2 for the line
+    T aa = vdot(A2, A2), ab = vdot(A2, A1), bb = vdot(A1, A1);
+    for (int piece = 0; piece < 3; ++piece) {
+        V3<T> C0 = piece == 1 ? vsub(A0, d) : A0;
+        T c[4] = {vdot(A1, C0), bb + T(2) * vdot(A2, C0), T(3) * ab, T(2) * aa};
+        if (piece == 2) {
+            if (!(dd > T(0))) continue;
+            T pa = vdot(A2, d), pb = vdot(A1, d), pc = vdot(A0, d);
+            T inv = T(1) / dd;
+            c[3] -= T(2) * pa * pa * inv;
+            c[2] -= T(3) * pa * pb * inv;
+            c[1] -= (pb * pb + T(2) * pa * pc) * inv;
+            c[0] -= pb * pc * inv;
+        }
+        T roots[3];
+        int n = cubic_roots01(c, roots, iters);
+        for (int j = 0; j < n; ++j) {
+            T g = g_at(A2, A1, A0, d, dd, roots[j]);
+            if (g < best) best = g;
+        }
+    }
+    return best;
+}
+
+// ---------------------------------------------------------------- traversal
+__device__ __forceinline__ uint32_t ldflag(const uint32_t* p) { return __ldcg(p); }
+
+__global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const SweepArgs A) {
+    const uint32_t* __restrict__ piece_traj = A.piece_traj;
+    constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
+    const float4* __restrict__ en = S.edge_nodes;
+    const float4* __restrict__ ep = S.edge_prims;
+    uint32_t st[kStack];
+    int sp = 0;
+    bool busy = false;
+    uint32_t traj = 0, piece_g = 0;
+    float4 P0 = make_float4(0, 0, 0, 0), P1 = P0, P2 = P0;  // linear: P0-P1 axis; quadratic: Bezier B0,B1,B2
+    float r = 0.f;
+    float blo[3], bhi[3];
+
+    while (true) {
+        if (!busy) {
+            cg::coalesced_group g = cg::coalesced_threads();
+            uint32_t base = 0;
+            if (g.thread_rank() == 0) base = atomicAdd(A.work_counter, g.size());
+            base = g.shfl(base, 0);
+            uint32_t u = base + g.thread_rank();
+            if (u >= A.total_units) break;
+            piece_g = u / A.n_spheres;
+            uint32_t s = u - piece_g * A.n_spheres;
+            traj = piece_traj[piece_g];
+            if (traj >= A.n_traj) {
+                atomicOr(A.err, kErrRange);
+                continue;
+            }
+            if (A.want_pieces ? ldflag(A.piece_hit + piece_g) && !A.want_counts
+                              : (!A.want_counts && ldflag(A.traj_hit + traj)))
+                continue;
+            uint32_t piece = piece_g - A.traj_piece_off[traj];
+            uint32_t w0 = A.traj_wp_off[traj], nwp = A.traj_wp_off[traj + 1] - w0;
+            if (!A.quad) {
+                P0 = A.centers[(size_t) (w0 + piece) * A.n_spheres + s];
+                P1 = A.centers[(size_t) (w0 + piece + 1) * A.n_spheres + s];
+                P2 = P1;
+            } else {
+                uint32_t c0 = A.traj_ctrl_off[traj], nc = A.traj_ctrl_off[traj + 1] - c0;
+                if (piece + 2 < nc) {
+                    float4 a = A.ctrl[(size_t) (c0 + piece) * A.n_spheres + s];
+                    float4 b = A.ctrl[(size_t) (c0 + piece + 1) * A.n_spheres + s];
+                    float4 c = A.ctrl[(size_t) (c0 + piece + 2) * A.n_spheres + s];
+                    P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), a.w);
+                    P1 = b;
+                    P2 = make_float4(0.5f * (b.x + c.x), 0.5f * (b.y + c.y), 0.5f * (b.z + c.z), a.w);
+                } else {
+                    uint32_t w = (piece + 2 == nc) ? w0 : w0 + nwp - 1;
+                    P0 = A.centers[(size_t) w * A.n_spheres + s];
+                    P1 = P0;
+                    P2 = P0;
+                }
+            }
+            r = P0.w;
+            float pad = r + 2e-5f;
+            blo[0] = fminf(P0.x, fminf(P1.x, P2.x)) - pad; bhi[0] = fmaxf(P0.x, fmaxf(P1.x, P2.x)) + pad;
+            blo[1] = fminf(P0.y, fminf(P1.y, P2.y)) - pad; bhi[1] = fmaxf(P0.y, fmaxf(P1.y, P2.y)) + pad;
+            blo[2] = fminf(P0.z, fminf(P1.z, P2.z)) - pad; bhi[2] = fmaxf(P0.z, fmaxf(P1.z, P2.z)) + pad;
+            if (S.edge_root == kNone) continue;
+            st[0] = S.edge_root;
+            sp = 1;
+            busy = true;
+            continue;
+        }
+        if (sp == 0) {
+            busy = false;
+            continue;
+        }
+        uint32_t ref = st[--sp];
+        if (ref & kLeaf) {
+            const float4* e = ep + 2ull * (ref & ~kLeaf);
+            float4 ea = __ldg(e), eb = __ldg(e + 1);
+            V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
+            float d2;
+            if (!A.quad)
+                d2 = seg_seg2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1));
+            else
+                d2 = seg_quad2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1), v3cast<float>(P2), 12);
+            float dist = sqrtf(fmaxf(d2, 0.f));
+            bool hit = dist <= r;
+            if (fabsf(dist - r) <= kBand + 1e-6f * r) {
+                atomicAdd(A.stats, 1ull);
+                double dd2;
+                if (!A.quad)
+                    dd2 = seg_seg2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0),
+                                           v3cast<double>(P1));
+                else
+                    dd2 = seg_quad2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0),
+                                            v3cast<double>(P1), v3cast<double>(P2), 48);
+                hit = dd2 <= (double) r * (double) r;
+            }
+            if (hit) {
+                if (A.want_pieces) atomicExch(A.piece_hit + piece_g, 1u);
+                if (A.want_counts) {
+                    A.traj_hit[traj] = 1u;
+                    atomicAdd(A.counts + traj, 1u);
+                } else {
+                    atomicExch(A.traj_hit + traj, 1u);
+                    busy = false;
+                }
+            }
+            continue;
+        }
+        Box bl, br;
+        uint32_t rl, rr;
+        load_node(en, ref, bl, br, rl, rr);
+        bool hr = box_overlap(br, blo, bhi), hl = box_overlap(bl, blo, bhi);
+        if (sp + 2 > kStack) {
+            atomicOr(A.err, kErrStack);
+            hr = hl = false;
+        }
+        if (hr) st[sp++] = rr;
+        if (hl) st[sp++] = rl;
+    }
+}
+
+uint32_t sweep_persistent_blocks() {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep, kTravThreads, 0);
+    return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
+}
+
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, cudaStream_t s) {
+    k_sweep<<<blocks, kTravThreads, 0, s>>>(S, A);
+    cuda_check(cudaGetLastError(), "k_sweep");
+}
+
+}  // namespace rtcd

@@ -1,0 +1,374 @@
+"""ctypes binding of ``librtcd_b200.so`` (include/rtcd.h) and a Python mirror
+of the upstream detector interface.
+
+The upstream API is ``RTCD::CollisionDetector<NSTREAM, LinkType>``
+(RTCD/CollisionDetector/CollisionDetector.h:18-157) driven as
+``setupScene -> setupOptix -> setupRobot -> buildSBT`` then per query
+``robot->prepareUpdateData(poses, n); setNCheck(n); check(); downloadResult(v)``.
+:class:`CollisionDetector` keeps those method names; :class:`Context`,
+:class:`Robot`, :class:`Scene` and :class:`Detector` are the thin handle
+wrappers.  There is no CPU fallback: a missing library raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'librtcd_b200.so')
+
+OBS_TO_ROBOT, ROBOT_TO_OBS, LINEAR_SWEEP, QUAD_SWEEP = 0, 1, 2, 3
+KIND_NAMES = {'ObsToRobot': OBS_TO_ROBOT, 'RobotToObs': ROBOT_TO_OBS, 'Linear': LINEAR_SWEEP, 'Quadratic': QUAD_SWEEP}
+
+CHECK_COUNTS = 1 << 0
+CHECK_HOST_BUFFERS = 1 << 1
+CHECK_NO_CULL = 1 << 2
+CHECK_PLAIN = 1 << 3
+CHECK_NO_ENDPOINTS = 1 << 4
+
+STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
+          4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}
+
+EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_context_destroy', 'rtcd_robot_create',
+           'rtcd_robot_destroy', 'rtcd_scene_create', 'rtcd_scene_destroy', 'rtcd_scene_info', 'rtcd_detector_create',
+           'rtcd_detector_destroy', 'rtcd_check', 'rtcd_sync', 'rtcd_segment_offsets', 'rtcd_last_stats',
+           'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build']
+
+
+class RTCDError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__('%s: %s' % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+F, U, VP = C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_void_p
+
+
+class RobotDesc(C.Structure):
+    _fields_ = [('dof', C.c_uint32), ('base_tf', F), ('cos_mask', F), ('sin_mask', F), ('one_mask', F),
+                ('link_verts', F), ('link_vert_offsets', U), ('link_tris', U), ('link_tri_offsets', U),
+                ('link_edges', U), ('link_edge_offsets', U), ('link_obbs', F), ('n_spheres', C.c_uint32),
+                ('sphere_centers', F), ('sphere_radii', F), ('sphere_links', U), ('skip_base', C.c_int32)]
+
+
+class Config(C.Structure):
+    _fields_ = [('frame_size', C.c_uint32), ('reserved', C.c_uint32 * 7)]
+
+
+class Stats(C.Structure):
+    _fields_ = [('work_items', C.c_uint64), ('culled_items', C.c_uint64), ('fp64_retests', C.c_uint64),
+                ('reserved', C.c_uint64 * 5)]
+
+
+_lib = None
+
+
+def lib():
+    """Load the engine.  Raises when the library has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError('librtcd_b200.so is missing: run `python -m rtcollisiondetection_b200.build` '
+                               '(or __graft_entry__.build()) first')
+        l = C.CDLL(LIB_PATH)
+        for name in EXPORTS:
+            getattr(l, name).restype = C.c_int
+        _lib = l
+    return _lib
+
+
+def last_error():
+    buf = C.create_string_buffer(1024)
+    lib().rtcd_last_error(buf, C.c_size_t(1024))
+    return buf.value.decode(errors='replace')
+
+
+def _ok(status):
+    if status != 0:
+        raise RTCDError(status, last_error())
+
+
+def _arr(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+def _ptr(a, ct):
+    if a is None:
+        return None
+    if hasattr(a, 'data_ptr'):            # torch tensor (device or host)
+        return C.cast(C.c_void_p(a.data_ptr()), C.POINTER(ct))
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def lbvh_build(ctx, lo, hi):
+    """Canonical LBVH over boxes: dict(codes, perm, child[n-1, 2], node_lo, node_hi, depth)."""
+    lo, hi = _arr(lo, np.float32).reshape(-1, 3), _arr(hi, np.float32).reshape(-1, 3)
+    n = len(lo)
+    m = max(n - 1, 1)
+    out = {'codes': np.zeros(max(n, 1), np.uint32), 'perm': np.zeros(max(n, 1), np.uint32),
+           'child': np.zeros((m, 2), np.uint32), 'node_lo': np.zeros((m, 3), np.float32),
+           'node_hi': np.zeros((m, 3), np.float32)}
+    depth = C.c_uint32()
+    _ok(lib().rtcd_lbvh_build(ctx.h, _ptr(lo, C.c_float), _ptr(hi, C.c_float), C.c_uint32(n),
+                              _ptr(out['codes'], C.c_uint32), _ptr(out['perm'], C.c_uint32),
+                              _ptr(out['child'], C.c_uint32), _ptr(out['node_lo'], C.c_float),
+                              _ptr(out['node_hi'], C.c_float), C.byref(depth)))
+    for k in ('codes', 'perm'):
+        out[k] = out[k][:n]
+    for k in ('child', 'node_lo', 'node_hi'):
+        out[k] = out[k][:max(n - 1, 0)]
+    out['depth'] = depth.value
+    return out
+
+
+def exclusive_scan_u32(ctx, in_dev, out_dev, n, total_dev=None, stream=None):
+    _ok(lib().rtcd_exclusive_scan_u32(ctx.h, _ptr(in_dev, C.c_uint32), _ptr(out_dev, C.c_uint32), C.c_uint32(n),
+                                      _ptr(total_dev, C.c_uint32), C.c_void_p(stream) if stream else None))
+
+
+def select_flags_u8(ctx, mask_dev, n, idx_dev, count_dev, stream=None):
+    _ok(lib().rtcd_select_flags_u8(ctx.h, _ptr(mask_dev, C.c_uint8), C.c_uint32(n), _ptr(idx_dev, C.c_uint32),
+                                   _ptr(count_dev, C.c_uint32), C.c_void_p(stream) if stream else None))
+
+
+def robot_fk(robot, q_dev, n, T_dev, stream=None):
+    _ok(lib().rtcd_robot_fk(robot.h, _ptr(q_dev, C.c_float), C.c_uint32(n), _ptr(T_dev, C.c_float),
+                            C.c_void_p(stream) if stream else None))
+
+
+class Context:
+    def __init__(self, device=0):
+        self.h = VP()
+        _ok(lib().rtcd_context_create(C.c_int(device), C.byref(self.h)))
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().rtcd_context_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Robot:
+    """Serial-chain robot: chain masks, link meshes, optional spheres."""
+
+    def __init__(self, ctx, model, spheres=None, skip_base=True, edges=True):
+        self.ctx = ctx
+        m = model
+        self._keep = {
+            'base': _arr(m['base_tf'], np.float32), 'cos': _arr(m['cos_mask'], np.float32),
+            'sin': _arr(m['sin_mask'], np.float32), 'one': _arr(m['one_mask'], np.float32),
+            'lv': _arr(m['link_verts'], np.float32), 'lvo': _arr(m['link_vert_off'], np.uint32),
+            'lt': _arr(m['link_tris'], np.uint32), 'lto': _arr(m['link_tri_off'], np.uint32),
+            'le': _arr(m['link_edges'], np.uint32) if edges and 'link_edges' in m else None,
+            'leo': _arr(m['link_edge_off'], np.uint32) if edges and 'link_edges' in m else None,
+        }
+        if spheres is None and 'sphere_centers' in m:
+            spheres = (m['sphere_centers'], m['sphere_radii'], m['sphere_links'])
+        if spheres is not None:
+            self._keep['sc'] = _arr(spheres[0], np.float32)
+            self._keep['sr'] = _arr(spheres[1], np.float32)
+            self._keep['sl'] = _arr(spheres[2], np.uint32)
+        k = self._keep
+        self.dof = len(k['cos']) if k['cos'].ndim == 2 else len(k['cos']) // 12
+        d = RobotDesc()
+        d.dof = self.dof
+        d.base_tf, d.cos_mask, d.sin_mask, d.one_mask = (_ptr(k[x], C.c_float) for x in ('base', 'cos', 'sin', 'one'))
+        d.link_verts = _ptr(k['lv'], C.c_float)
+        d.link_vert_offsets = _ptr(k['lvo'], C.c_uint32)
+        d.link_tris = _ptr(k['lt'], C.c_uint32)
+        d.link_tri_offsets = _ptr(k['lto'], C.c_uint32)
+        d.link_edges = _ptr(k['le'], C.c_uint32)
+        d.link_edge_offsets = _ptr(k['leo'], C.c_uint32)
+        d.link_obbs = None
+        if spheres is not None:
+            d.n_spheres = len(k['sr'])
+            d.sphere_centers = _ptr(k['sc'], C.c_float)
+            d.sphere_radii = _ptr(k['sr'], C.c_float)
+            d.sphere_links = _ptr(k['sl'], C.c_uint32)
+        d.skip_base = 1 if skip_base else 0
+        self.h = VP()
+        _ok(lib().rtcd_robot_create(ctx.h, C.byref(d), C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().rtcd_robot_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """Resident obstacle scene (triangle soup with obstacle ranges)."""
+
+    def __init__(self, ctx, verts, tris, obstacle_tri_off=None):
+        self.ctx = ctx
+        v = _arr(verts, np.float32).reshape(-1, 3)
+        t = _arr(tris, np.uint32).reshape(-1, 3)
+        o = _arr(obstacle_tri_off, np.uint32)
+        self.h = VP()
+        _ok(lib().rtcd_scene_create(ctx.h, _ptr(v, C.c_float), C.c_uint32(len(v)), _ptr(t, C.c_uint32),
+                                    C.c_uint32(len(t)), _ptr(o, C.c_uint32),
+                                    C.c_uint32(0 if o is None else len(o) - 1), C.byref(self.h)))
+        nt, ne, no = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _ok(lib().rtcd_scene_info(self.h, C.byref(nt), C.byref(ne), C.byref(no)))
+        self.n_tris, self.n_edges, self.n_obstacles = nt.value, ne.value, no.value
+
+    @classmethod
+    def from_mesh(cls, ctx, mesh):
+        return cls(ctx, mesh.verts, mesh.tris, mesh.obstacle_tri_off)
+
+    def close(self):
+        if self.h:
+            lib().rtcd_scene_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def segment_offsets(kind, traj_off, flags=0):
+    traj_off = _arr(traj_off, np.uint32)
+    out = np.zeros(len(traj_off), np.uint32)
+    _ok(lib().rtcd_segment_offsets(C.c_int(kind), _ptr(traj_off, C.c_uint32), C.c_uint32(len(traj_off) - 1),
+                                   C.c_uint32(flags), _ptr(out, C.c_uint32)))
+    return out
+
+
+class Detector:
+    """One detector of one kind over a robot and a scene."""
+
+    def __init__(self, ctx, kind, robot, scene, frame_size=0):
+        if isinstance(kind, str):
+            kind = KIND_NAMES[kind]
+        self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
+        cfg = Config()
+        cfg.frame_size = frame_size
+        self.h = VP()
+        _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
+
+    @property
+    def sweep(self):
+        return self.kind in (LINEAR_SWEEP, QUAD_SWEEP)
+
+    def check(self, q, traj_off=None, counts=False, segments=False, flags=0):
+        """Host-buffer call: q is a numpy array; returns dict of numpy outputs."""
+        q = _arr(q, np.float32)
+        flags |= CHECK_HOST_BUFFERS | (CHECK_COUNTS if counts else 0)
+        if self.sweep:
+            traj_off = _arr(traj_off, np.uint32)
+            n = len(traj_off) - 1
+        else:
+            n = len(q)
+        out = {'flags': np.zeros(n, np.uint8)}
+        if counts:
+            out['counts'] = np.zeros(n, np.uint32)
+        seg = None
+        if segments:
+            seg_off = segment_offsets(self.kind, traj_off, flags)
+            seg = np.zeros(max(1, int(seg_off[-1])), np.uint8)
+            out['seg_off'] = seg_off
+        _ok(lib().rtcd_check(self.h, _ptr(q, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
+                             _ptr(out['flags'], C.c_uint8), _ptr(seg, C.c_uint8),
+                             _ptr(out.get('counts'), C.c_uint32), C.c_uint32(flags), None))
+        if segments:
+            out['seg_flags'] = seg[:int(out['seg_off'][-1])]
+        return out
+
+    def check_device(self, q_dev, n, flags_dev, traj_off=None, counts_dev=None, seg_dev=None, flags=0, stream=None):
+        """Device-buffer call (torch CUDA tensors or raw pointers); asynchronous."""
+        traj_off = _arr(traj_off, np.uint32)
+        if counts_dev is not None:
+            flags |= CHECK_COUNTS
+        _ok(lib().rtcd_check(self.h, _ptr(q_dev, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
+                             _ptr(flags_dev, C.c_uint8), _ptr(seg_dev, C.c_uint8), _ptr(counts_dev, C.c_uint32),
+                             C.c_uint32(flags), C.c_void_p(stream) if stream else None))
+
+    def sync(self, stream=None):
+        _ok(lib().rtcd_sync(self.h, C.c_void_p(stream) if stream else None))
+
+    def stats(self):
+        s = Stats()
+        _ok(lib().rtcd_last_stats(self.h, C.byref(s)))
+        return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests}
+
+    def close(self):
+        if self.h:
+            lib().rtcd_detector_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CollisionDetector:
+    """Mirror of the upstream ``RTCD::CollisionDetector`` call sequence.
+
+    ``setupScene(scene)``, ``setupRobot(robot)``, ``setupOptix()`` and
+    ``buildSBT()`` are accepted for drop-in call order (the last two have
+    nothing to do here); ``prepareUpdateData(poses, n)`` stages host poses
+    (``CCRobotWrapper.h:39-46``), ``setNCheck(n)`` sets the query size
+    (``CollisionDetector.h:354``), ``check()`` runs it and ``downloadResult``
+    returns the per-pose (per-trajectory) upstream hit counts, nonzero = hit
+    (``CollisionDetector.h:62``).
+    """
+
+    def __init__(self, ctx, kind, robot=None, scene=None):
+        self.ctx, self.kind = ctx, KIND_NAMES.get(kind, kind)
+        self.robot, self.scene, self.det = robot, scene, None
+        self.poses, self.traj_off, self.n = None, None, 0
+        self.result = None
+
+    def setupScene(self, scene):
+        self.scene = scene
+        self.det = None
+
+    def setupRobot(self, robot):
+        self.robot = robot
+        self.det = None
+
+    def setupOptix(self):
+        pass
+
+    def buildSBT(self):
+        if self.det is None:
+            self.det = Detector(self.ctx, self.kind, self.robot, self.scene)
+
+    def prepareUpdateData(self, poses, n, traj_off=None):
+        self.poses, self.traj_off = np.ascontiguousarray(poses, np.float32), traj_off
+        self.n = n
+
+    def setNCheck(self, n):
+        self.n = n
+
+    def check(self):
+        self.buildSBT()
+        if self.det.sweep:
+            traj = np.asarray(self.traj_off[:self.n + 1], np.uint32)
+            self.result = self.det.check(self.poses, traj, counts=True)
+        else:
+            self.result = self.det.check(self.poses[:self.n], counts=True)
+
+    def downloadResult(self):
+        return self.result['counts'].copy()
+
+    def flags(self):
+        return self.result['flags'].copy()
+
+    def clearResult(self):
+        self.result = None

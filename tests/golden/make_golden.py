@@ -1,0 +1,72 @@
+"""Regenerate the golden fixtures in this folder from the upstream repository.
+
+Run where the upstream RTCollisionDetection checkout is available:
+    python tests/golden/make_golden.py <upstream root>
+
+Writes
+* ``panda_header.json`` - the cos/sin/one masks, base transform and joint
+  limits as literal numbers from ``RTCD/Robot/models/panda.h:7-44``; the test
+  suite checks that masks derived from the URDF reproduce them.
+* ``quad_weights.npz``  - the shipped least-squares quadratic B-spline fit
+  matrices ``RTCD/data/weights/quad/normal/{nC}_{nT}.txt`` (row-major nC x nT),
+  the known answers for the on-device fit weights.
+* ``panda_mesh_stats.json`` - per-link vertex/triangle/unique-edge counts of
+  the merged visual meshes, counted here with a direct text scan of the OBJ
+  files (independent of the package loader).
+"""
+import json
+import os
+import re
+import sys
+import glob
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def header_arrays(path):
+    src = open(path).read()
+    out = {}
+    for name in ('baseT', 'lowerBound', 'upperBound', 'sinMask', 'cosMask', 'oneMask'):
+        m = re.search(name + r'[^{;]*\{([^}]*)\}', src)
+        nums = re.findall(r'-?\d+\.?\d*(?:e-?\d+)?', m.group(1))
+        out[name] = [float(x) for x in nums]
+    return out
+
+
+def mesh_stats(root):
+    stats = []
+    for li in range(8):
+        p = os.path.join(root, 'models/franka_description/merged_meshes/panda_link%d_visual.obj' % li)
+        pos, faces = [], []
+        for line in open(p):
+            if line.startswith('v '):
+                pos.append(tuple(np.float32(float(x)) for x in line.split()[1:4]))
+            elif line.startswith('f '):
+                faces.append([int(t.split('/')[0]) - 1 for t in line.split()[1:]])
+        uniq = {}
+        for v in pos:
+            uniq.setdefault(v, len(uniq))
+        edges = set()
+        for f in faces:
+            g = [uniq[pos[i]] for i in f]
+            for a, b in ((g[0], g[1]), (g[1], g[2]), (g[2], g[0])):
+                edges.add((min(a, b), max(a, b)))
+        stats.append({'verts': len(uniq), 'tris': len(faces), 'edges': len(edges)})
+    return stats
+
+
+def main(root):
+    hdr = header_arrays(os.path.join(root, 'RTCD/Robot/models/panda.h'))
+    json.dump(hdr, open(os.path.join(HERE, 'panda_header.json'), 'w'), indent=1)
+    w = {}
+    for f in sorted(glob.glob(os.path.join(root, 'RTCD/data/weights/quad/normal/*.txt'))):
+        key = os.path.basename(f)[:-4]
+        nc, nt = map(int, key.split('_'))
+        w['w_' + key] = np.loadtxt(f, dtype=np.float32).reshape(nc, nt)
+    np.savez_compressed(os.path.join(HERE, 'quad_weights.npz'), **w)
+    json.dump(mesh_stats(root), open(os.path.join(HERE, 'panda_mesh_stats.json'), 'w'), indent=1)
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')

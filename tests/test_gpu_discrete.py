@@ -1,0 +1,115 @@
+"""Discrete detectors (ObsToRobot, RobotToObs) against the FP64 oracle.
+
+Flags must agree on every pose outside the 1e-5 m band; the upstream hit
+counts must agree on every pose with no marginal primitive pair."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rtcollisiondetection_b200 import rtcd, scenes
+
+pytestmark = pytest.mark.gpu
+KINDS = [('ObsToRobot', O.OBS_TO_ROBOT), ('RobotToObs', O.ROBOT_TO_OBS)]
+
+
+@pytest.fixture(scope='module')
+def setup(ctx, panda, small_scene):
+    robot = rtcd.Robot(ctx, panda)
+    scene = rtcd.Scene.from_mesh(ctx, small_scene)
+    orc = (O.Robot(panda), O.Scene(small_scene))
+    return robot, scene, orc
+
+
+def _compare(out, ref, counts=True):
+    band = ref['band'].astype(bool)
+    mism = (out['flags'] != ref['hit']) & ~band
+    assert mism.sum() == 0, 'flag mismatches outside the band at poses %s' % np.nonzero(mism)[0][:20]
+    if counts:
+        safe = ~ref['marg'].astype(bool)
+        cm = (out['counts'] != ref['count']) & safe
+        assert cm.sum() == 0, 'count mismatches at %s' % np.nonzero(cm)[0][:20]
+        assert np.array_equal(out['counts'] > 0, out['flags'] > 0)
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_small_scene_parity(setup, panda, name, okind):
+    robot, scene, (orob, oscene) = setup
+    q = scenes.uniform_poses(panda, 1024, seed=0)
+    ref = O.discrete(okind, orob, oscene, q)
+    det = rtcd.Detector(robot.ctx, name, robot, scene)
+    flags_only = det.check(q)
+    with_counts = det.check(q, counts=True)
+    _compare(with_counts, ref)
+    assert np.array_equal(flags_only['flags'], with_counts['flags'])
+    assert 0.2 < ref['hit'].mean() < 0.9  # the workload is not trivial
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_cull_plain_and_device_paths_agree(setup, panda, name, okind):
+    import torch
+    robot, scene, _ = setup
+    q = scenes.uniform_poses(panda, 777, seed=11)
+    det = rtcd.Detector(robot.ctx, name, robot, scene, frame_size=64)
+    a = det.check(q, counts=True)
+    b = det.check(q, counts=True, flags=rtcd.CHECK_NO_CULL)
+    c = det.check(q, counts=True, flags=rtcd.CHECK_PLAIN)
+    assert np.array_equal(a['flags'], b['flags']) and np.array_equal(a['counts'], b['counts'])
+    assert np.array_equal(a['flags'], c['flags']) and np.array_equal(a['counts'], c['counts'])
+    qd = torch.from_numpy(q).cuda()
+    fd = torch.zeros(len(q), dtype=torch.uint8, device='cuda')
+    cd = torch.zeros(len(q), dtype=torch.int32, device='cuda')
+    det.check_device(qd, len(q), fd, counts_dev=cd, stream=torch.cuda.current_stream().cuda_stream)
+    det.sync(torch.cuda.current_stream().cuda_stream)
+    assert np.array_equal(fd.cpu().numpy(), a['flags'])
+    assert np.array_equal(cd.cpu().numpy().astype(np.uint32), a['counts'])
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_edge_cases(setup, panda, name, okind):
+    robot, scene, (orob, oscene) = setup
+    det = rtcd.Detector(robot.ctx, name, robot, scene)
+    # single pose, the joint limits, repeated poses
+    q = np.stack([panda['lower'], panda['upper'], 0.5 * (panda['lower'] + panda['upper'])]).astype(np.float32)
+    q = np.concatenate([q, q[:1].repeat(5, 0)])
+    ref = O.discrete(okind, orob, oscene, q)
+    _compare(det.check(q, counts=True), ref)
+    one = det.check(q[:1])
+    assert one['flags'][0] == det.check(q)['flags'][0]
+
+
+def test_empty_scene_and_far_scene(ctx, panda):
+    robot = rtcd.Robot(ctx, panda)
+    far = scenes.random_scene(3, 3, 1, seed=5)
+    far.verts[:] += np.float32(50.0)
+    for mesh in (far,):
+        sc = rtcd.Scene.from_mesh(ctx, mesh)
+        for name in ('ObsToRobot', 'RobotToObs'):
+            det = rtcd.Detector(ctx, name, robot, sc)
+            out = det.check(scenes.uniform_poses(panda, 100), counts=True)
+            assert out['flags'].sum() == 0 and out['counts'].sum() == 0
+
+
+def test_single_triangle_scene(ctx, panda):
+    """A single large triangle through the robot's reach; brute-force oracle."""
+    robot = rtcd.Robot(ctx, panda)
+    v = np.array([[-1, -1, 0.5], [2, -1, 0.5], [-1, 2, 0.5]], np.float32)
+    t = np.array([[0, 1, 2]], np.uint32)
+    mesh = scenes.Mesh(v, t, np.array([0, 1], np.uint32))
+    sc = rtcd.Scene.from_mesh(ctx, mesh)
+    q = scenes.uniform_poses(panda, 256, seed=9)
+    orob, osc = O.Robot(panda), O.Scene(mesh)
+    for name, okind in KINDS:
+        det = rtcd.Detector(ctx, name, robot, sc)
+        _compare(det.check(q, counts=True), O.discrete(okind, orob, osc, q))
+
+
+def test_invalid_arguments(ctx, panda, small_scene):
+    robot = rtcd.Robot(ctx, panda)
+    with pytest.raises(rtcd.RTCDError):
+        rtcd.Scene(ctx, small_scene.verts, np.array([[0, 1, 10 ** 7]], np.uint32))
+    sc = rtcd.Scene.from_mesh(ctx, small_scene)
+    with pytest.raises(rtcd.RTCDError):
+        rtcd.Detector(ctx, 7, robot, sc)
+    det = rtcd.Detector(ctx, 'RobotToObs', robot, sc)
+    with pytest.raises(rtcd.RTCDError):
+        det.check(np.zeros((4, 7), np.float32), segments=True, traj_off=np.array([0, 4], np.uint32))
