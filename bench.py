@@ -1,0 +1,371 @@
+"""Benchmark of the batched collision-query path on B200.
+
+Workload (one step): the RobotToObs detector over 65,536 uniform random
+Panda poses against the dense synthetic scene (64 boxes, 256 level-3
+icospheres, one 100k-triangle noisy sphere: 428,448 triangles), flags out.
+``--config`` selects the other workloads (ObsToRobot small/dense, linear and
+quadratic sweeps) for the same measurement.
+
+Timing: W untimed warm-up steps, then K steps; a 256 MiB buffer is written
+before every step to flush the 126 MB L2 and each step is timed with CUDA
+events on the launching stream (max over ranks for N > 1, weak scaling:
+every rank checks its own batch).  ``e2e`` repeats the step through the
+public C ABI with host buffers (pose upload and flag download inside the
+timed call).  ``plain`` is the same engine driven the upstream way: frames
+of 64 poses with a host round trip per frame.  ``cpu_baseline`` times the
+FP64 oracle (flags only, every host thread) on a bounded sample.
+
+``--impl reference`` times the CPU restatement of the reference path (the
+oracle port; the upstream OptiX path needs RT cores and the OptiX SDK) on the
+same workload and prints the same JSON line with ``"impl": "reference"``.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'poses/s and p50/p99 latency: batched-served vs plain, same B200, 0 flag errors'
+PEAK_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, 'measured'
+    return dict(PEAK_FALLBACK), 'fallback'
+
+
+CONFIGS = {
+    'c2': dict(kind='RobotToObs', n=65536, scene='dense',
+               workload='RobotToObs, 65,536 uniform Panda poses, dense scene 64 boxes + 256 level-3 icospheres + '
+                        '100k-tri noisy sphere (428,448 tris) over x,y in [-1.5,1.5] m, z in [0,1.5] m'),
+    'c2o': dict(kind='ObsToRobot', n=65536, scene='dense',
+                workload='ObsToRobot, 65,536 uniform Panda poses, dense 428,448-tri scene'),
+    'c1': dict(kind='ObsToRobot', n=1024, scene='small',
+               workload='ObsToRobot, 1,024 uniform Panda poses, 12 boxes + 16 level-2 icospheres (5,264 tris)'),
+    'c3': dict(kind='Linear', n=4096, scene='sweep', wp=32,
+               workload='Linear sweep, 4,096 random-walk trajectories x 32 waypoints, 64 spheres, 49,744-tri scene'),
+    'c4': dict(kind='Quadratic', n=4096, scene='sweep', wp=(8, 64),
+               workload='Quadratic sweep, 4,096 trajectories of 8-64 waypoints (log-uniform), 64 spheres, '
+                        '49,744-tri scene'),
+}
+
+
+def make_inputs(cfg, rank, scenes):
+    model = scenes.load_panda()
+    mesh = {'dense': scenes.discrete_dense, 'small': scenes.discrete_small, 'sweep': scenes.sweep_scene}[cfg['scene']]()
+    spheres = scenes.synth_spheres(model) if cfg['kind'] in ('Linear', 'Quadratic') else None
+    if cfg['kind'] in ('Linear', 'Quadratic'):
+        wp = cfg['wp']
+        counts = wp if np.isscalar(wp) else scenes.log_uniform_counts(cfg['n'], wp[0], wp[1], seed=rank)
+        q, off = scenes.random_walk_trajectories(model, cfg['n'], counts, seed=rank)
+    else:
+        q, off = scenes.uniform_poses(model, cfg['n'], seed=rank), None
+    return model, mesh, spheres, q, off
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(',')])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace('.', '', 1).isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and 'Active' in r[5 + k]
+                          and 'Not' not in r[5 + k]})
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+                'reasons': reasons, 'samples': len(self.rows)}
+
+
+def cpu_baseline(cfg, model, mesh, spheres, q, off, seconds=10.0):
+    """The oracle (FP64, flags only for the discrete kinds) on a bounded sample."""
+    from oracle import oracle as O
+    robot = O.Robot(model, spheres=spheres)
+    scene = O.Scene(mesh)
+    threads = os.cpu_count() or 1
+    if cfg['kind'] in ('RobotToObs', 'ObsToRobot'):
+        prep = O.PreparedDiscrete(O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT, robot, scene)
+        n = 256
+        while True:
+            t0 = time.perf_counter()
+            prep.flags(q[:n], threads)
+            dt = time.perf_counter() - t0
+            if dt * 4 > seconds or n >= len(q):
+                break
+            n = min(len(q), n * 4)
+        unit, value = 'poses/s', n / dt
+        sample = '%d of the %d poses, flags only with per-pose early exit' % (n, len(q))
+    else:
+        quad = cfg['kind'] == 'Quadratic'
+        n = 16
+        while True:
+            t0 = time.perf_counter()
+            O.sweep(quad, robot, scene, q[:off[n]], off[:n + 1], threads=threads)
+            dt = time.perf_counter() - t0
+            if dt * 4 > seconds or n >= len(off) - 1:
+                break
+            n = min(len(off) - 1, n * 4)
+        unit, value = 'trajectories/s', n / dt
+        sample = '%d of the %d trajectories, full segment flags' % (n, len(off) - 1)
+    return {'value': value, 'unit': unit, 'cores': threads, 'kind': 'port', 'sample': sample,
+            'seconds': round(dt, 3)}
+
+
+def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512):
+    """Flag mismatches outside the 1e-5 m band on a sample of the batch."""
+    from oracle import oracle as O
+    robot = O.Robot(model, spheres=spheres)
+    scene = O.Scene(mesh)
+    if cfg['kind'] in ('RobotToObs', 'ObsToRobot'):
+        k = O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT
+        idx = np.linspace(0, len(q) - 1, min(n_sample, len(q))).astype(int)
+        ref = O.discrete(k, robot, scene, q[idx])
+        err = int(((flags[idx] != ref['hit']) & (ref['band'] == 0)).sum())
+        return {'flag_errors': err, 'checked': len(idx), 'in_band': int(ref['band'].sum()),
+                'collision_rate': float(ref['hit'].mean())}
+    m = min(len(off) - 1, n_sample // 4)
+    ref = O.sweep(cfg['kind'] == 'Quadratic', robot, scene, q[:off[m]], off[:m + 1])
+    err = int(((flags[:m] != ref['traj_hit']) & (ref['traj_band'] == 0)).sum())
+    return {'flag_errors': err, 'checked': m, 'in_band': int(ref['traj_band'].sum()),
+            'collision_rate': float(ref['traj_hit'].mean())}
+
+
+def run_reference(args, cfg, rank, world):
+    from rtcollisiondetection_b200 import scenes
+    if rank != 0:
+        return
+    model, mesh, spheres, q, off = make_inputs(cfg, 0, scenes)
+    from oracle import oracle as O
+    robot = O.Robot(model, spheres=spheres)
+    scene = O.Scene(mesh)
+    threads = os.cpu_count() or 1
+    discrete = cfg['kind'] in ('RobotToObs', 'ObsToRobot')
+    if discrete:
+        prep = O.PreparedDiscrete(O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT, robot, scene)
+        sample = max(256, min(len(q), args.ref_sample))
+
+        def step():
+            prep.flags(q[:sample], threads)
+        units = sample
+    else:
+        quad = cfg['kind'] == 'Quadratic'
+        sample = max(4, min(len(off) - 1, args.ref_sample // 64))
+
+        def step():
+            O.sweep(quad, robot, scene, q[:off[sample]], off[:sample + 1], threads=threads)
+        units = sample
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    unit = 'poses/s' if discrete else 'trajectories/s'
+    value = units / dt
+    what = ('%d of the %d poses per step' if discrete else '%d of the %d trajectories per step') % (
+        units, len(q) if discrete else len(off) - 1)
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': unit, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': dt * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': cfg['workload'], 'detector': cfg['kind'],
+                       'reference': 'CPU restatement of the reference path (FP64 oracle, flags only); the upstream '
+                                    'OptiX path is unavailable on this box (no RT cores, no OptiX SDK)'},
+            'cpu_baseline': {'value': value, 'unit': unit, 'cores': threads, 'kind': 'port', 'sample': what},
+            'e2e': {'value': value, 'unit': unit, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--config', default='c2', choices=sorted(CONFIGS))
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-check', action='store_true')
+    ap.add_argument('--ref-sample', type=int, default=8192)
+    ap.add_argument('--plain-frame', type=int, default=64)
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get('RANK', 0))
+    world = int(os.environ.get('WORLD_SIZE', 1))
+    local = int(os.environ.get('LOCAL_RANK', 0))
+    if args.impl == 'reference':
+        run_reference(args, cfg, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120), device_id=torch.device('cuda', local))
+    from rtcollisiondetection_b200 import rtcd, scenes
+    model, mesh, spheres, q, off = make_inputs(cfg, rank, scenes)
+    ctx = rtcd.Context(local)
+    robot = rtcd.Robot(ctx, model, spheres=spheres)
+    scene = rtcd.Scene.from_mesh(ctx, mesh)
+    det = rtcd.Detector(ctx, cfg['kind'], robot, scene, frame_size=args.plain_frame)
+    sweep = det.sweep
+    n = cfg['n']
+    # a dedicated stream: the legacy default stream has handle 0, which the ABI
+    # reads as "the detector's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    qd = torch.from_numpy(q).cuda()
+    fd = torch.zeros(n, dtype=torch.uint8, device='cuda')
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
+
+    def step(extra=0):
+        det.check_device(qd, n, fd, traj_off=off, flags=rtcd.CHECK_TIMING | extra, stream=sp)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    trav = []
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.fill_(k & 255)
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+        trav.append(det.stats())   # syncs the step; stage times come from events on the same stream
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(np.sum(ms))
+    if dist:
+        t = torch.tensor([total_ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    units_all = n * world
+    value = units_all / (ms_step / 1e3)
+    unit = 'trajectories/s' if sweep else 'poses/s'
+    flags = fd.cpu().numpy()
+    st = det.stats()
+
+    # end to end through the C ABI with host buffers (upload + download inside the call)
+    e2e_ms = []
+    for k in range(max(3, args.steps // 2) + 2):
+        flush.fill_(k & 255)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = det.check(q, off)
+        dt = (time.perf_counter() - t0) * 1e3
+        if k >= 2:
+            e2e_ms.append(dt)
+    e2e_step = float(np.mean(e2e_ms))
+    assert np.array_equal(out['flags'], flags), 'host-buffer path disagrees with the device path'
+    h2d = q.nbytes + (0 if off is None else off.nbytes)
+    d2h = n
+
+    # plain path: frames of 64 poses, host round trip per frame (the upstream check() shape)
+    plain = None
+    if not sweep:
+        pm = []
+        for k in range(3):
+            flush.fill_(k & 255)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            det.check_device(qd, n, fd, flags=rtcd.CHECK_PLAIN, stream=sp)
+            torch.cuda.synchronize()
+            pm.append((time.perf_counter() - t0) * 1e3)
+        assert np.array_equal(fd.cpu().numpy(), flags), 'plain path disagrees'
+        plain = {'value': units_all / (np.median(pm) / 1e3), 'unit': unit, 'frame': args.plain_frame,
+                 'ms_per_step': float(np.median(pm))}
+
+    peaks, peak_src = load_peaks()
+    t_trav = float(np.mean([s['ms_traverse'] for s in trav]))
+    # algorithmic bytes of one traversal launch: poses in, flags out, the resident structures read once
+    if sweep:
+        bytes_alg = n * 4 + int(q.nbytes) + 32 * scene.n_edges * 3
+    else:
+        bytes_alg = n * (4 * model['cos_mask'].shape[0] + 1) + (64 + 48) * scene.n_tris + (64 + 32) * 35991
+    achieved = bytes_alg / (t_trav / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, 'profiles', 'traffic.json')
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(args.config)
+    line = {
+        'metric': METRIC, 'value': value, 'unit': unit, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
+        'data': 'synthetic',
+        'config': {'workload': cfg['workload'], 'detector': cfg['kind'], 'units_per_gpu': n,
+                   'l2': 'flushed before every step (256 MiB write)', 'form': 'batched: one persistent launch per step'},
+        'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
+                'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
+        'gpu_launches': args.steps * (5 if not sweep else (4 if cfg['kind'] == 'Linear' else 5)),
+        'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in trav])),
+                      'cull': float(np.mean([s['ms_cull'] for s in trav])), 'traverse': t_trav},
+        'roofline': {'bound': 'hbm', 'kernel': 'k_sweep' if sweep else 'k_discrete', 'achieved': achieved,
+                     'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved / peaks['hbm_gbs'],
+                     'traffic': traffic, 'peak_source': peak_src,
+                     'note': 'latency-bound tree traversal: HBM is not the binding resource'},
+        'clocks': clocks,
+    }
+    if plain:
+        line['plain'] = plain
+        line['batched_over_plain'] = value / plain['value']
+    if not args.no_check and rank == 0:
+        line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags)
+        line['fp64_retests'] = st['fp64_retests']
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        line['cpu_baseline'] = cpu_baseline(cfg, model, mesh, spheres, q, off)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del det, scene, robot, ctx
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

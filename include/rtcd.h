@@ -63,6 +63,7 @@ typedef enum {
 #define RTCD_CHECK_NO_CULL (1u << 2)       /* skip the OBB prefilter of the discrete detectors */
 #define RTCD_CHECK_PLAIN (1u << 3)         /* frame-by-frame path with a host sync per frame */
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
+#define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
 
 typedef struct rtcd_ctx rtcd_ctx;
 typedef struct rtcd_robot rtcd_robot;
@@ -167,7 +168,11 @@ typedef struct {
     uint64_t work_items;   /* (pose, link) items or sweep units processed */
     uint64_t culled_items; /* items the OBB prefilter removed */
     uint64_t fp64_retests; /* candidates re-tested in FP64 */
-    uint64_t reserved[5];
+    float ms_prepare;      /* with RTCD_CHECK_TIMING: FK / sphere centres / fit */
+    float ms_cull;         /* OBB prefilter + compaction (discrete) */
+    float ms_traverse;     /* the traversal kernel */
+    float ms_total;        /* whole check on the device */
+    uint64_t reserved[3];
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 

@@ -536,6 +536,7 @@ typedef struct {
     unsigned char *hit, *band, *marg;
     u32* count;
     orc_work* work;  /* per pose, optional */
+    int early;       /* stop a pose at its first hit (flags only) */
 } disc_ctx;
 
 typedef struct {
@@ -567,8 +568,18 @@ static int visit_tri(void* vctx, u32 t) {
     return 0;
 }
 
+typedef struct {
+    u32* ids;
+    u32 n;
+} edge_list;
+
+static int collect_prim(void* vctx, u32 prim) {
+    edge_list* l = (edge_list*) vctx;
+    l->ids[l->n++] = prim;
+    return 0;
+}
+
 static void disc_pose(void* vctx, int pose, void* scratch) {
-    (void) scratch;
     disc_ctx* C = (disc_ctx*) vctx;
     const orc_robot* R = C->R;
     const orc_scene* S = C->S;
@@ -597,11 +608,22 @@ static void disc_pose(void* vctx, int pose, void* scratch) {
                 ptests += s.prim_tests;
                 if (s.any_hit) { any = 1; ++count; }
                 robust |= s.robust; marginal |= s.marginal;
+                if (C->early && any) goto done;
             }
         } else {
-            /* every obstacle edge, moved into the link frame, against the link triangles */
+            /* every obstacle edge, moved into the link frame, against the link triangles;
+             * only edges whose boxes reach the link's world box can hit (pure acceleration) */
             const u32* lt = R->link_tris + (size_t) R->link_tri_off[l] * 3;
-            for (int e = 0; e < S->n_edges; ++e) {
+            double wlo[3] = {INFINITY, INFINITY, INFINITY}, whi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (u32 v = R->link_vert_off[l]; v < R->link_vert_off[l + 1]; ++v) {
+                d3 w = xform(TL, fv(R->link_verts + (size_t) v * 3));
+                double c[3] = {w.x, w.y, w.z};
+                for (int k = 0; k < 3; ++k) { wlo[k] = fmin(wlo[k], c[k] - eps); whi[k] = fmax(whi[k], c[k] + eps); }
+            }
+            edge_list cand = {(u32*) scratch, 0};
+            ntests += bvh_query(&C->scene_edge, wlo, whi, collect_prim, &cand);
+            for (u32 ci = 0; ci < cand.n; ++ci) {
+                u32 e = cand.ids[ci];
                 d3 pw = fv(S->verts + S->edges[e * 2] * 3), qw = fv(S->verts + S->edges[e * 2 + 1] * 3);
                 seg_query s;
                 memset(&s, 0, sizeof(s));
@@ -614,9 +636,11 @@ static void disc_pose(void* vctx, int pose, void* scratch) {
                 ptests += s.prim_tests;
                 if (s.any_hit) { any = 1; count += s.hits; }
                 robust |= s.robust; marginal |= s.marginal;
+                if (C->early && any) goto done;
             }
         }
     }
+done:
     if (Tp != T) free(Tp);
     C->hit[pose] = (unsigned char) any;
     if (C->count) C->count[pose] = count;
@@ -625,31 +649,57 @@ static void disc_pose(void* vctx, int pose, void* scratch) {
     if (C->work) { C->work[pose].node_tests = ntests; C->work[pose].prim_tests = ptests; }
 }
 
-int orc_discrete(int kind, const orc_robot* R, const orc_scene* S, const float* q, int n, double eps, int threads,
-                 unsigned char* hit, u32* count, unsigned char* band, unsigned char* marg, orc_work* work) {
-    disc_ctx C;
-    memset(&C, 0, sizeof(C));
-    C.kind = kind; C.R = R; C.S = S; C.q = q; C.eps = eps;
-    C.hit = hit; C.count = count; C.band = band; C.marg = marg; C.work = work;
+/* A prepared discrete query: the acceleration structures are built once so
+ * repeated runs (the timed CPU baseline) measure the queries alone. */
+void* orc_discrete_prepare(int kind, const orc_robot* R, const orc_scene* S) {
+    disc_ctx* C = (disc_ctx*) calloc(1, sizeof(disc_ctx));
+    C->kind = kind; C->R = R; C->S = S;
     float *lo, *hi;
     if (kind == ORC_ROBOT_TO_OBS) {
         tri_boxes(S->verts, S->tris, S->n_tris, &lo, &hi);
-        bvh_make(&C.scene_tri, S->n_tris, lo, hi);
+        bvh_make(&C->scene_tri, S->n_tris, lo, hi);
     } else {
-        C.link_tri = (bvh_t*) calloc((size_t) R->n_links, sizeof(bvh_t));
+        edge_boxes(S->verts, S->edges, S->n_edges, &lo, &hi);
+        bvh_make(&C->scene_edge, S->n_edges, lo, hi);
+        C->link_tri = (bvh_t*) calloc((size_t) R->n_links, sizeof(bvh_t));
         for (int l = 0; l < R->n_links; ++l) {
             int nt = (int) (R->link_tri_off[l + 1] - R->link_tri_off[l]);
             tri_boxes(R->link_verts + (size_t) R->link_vert_off[l] * 3, R->link_tris + (size_t) R->link_tri_off[l] * 3, nt,
                       &lo, &hi);
-            bvh_make(&C.link_tri[l], nt, lo, hi);
+            bvh_make(&C->link_tri[l], nt, lo, hi);
         }
     }
-    run_pool(n, threads, disc_pose, &C, 0);
-    if (kind == ORC_ROBOT_TO_OBS) bvh_free(&C.scene_tri);
+    return C;
+}
+
+void orc_discrete_free(void* h) {
+    disc_ctx* C = (disc_ctx*) h;
+    if (!C) return;
+    if (C->kind == ORC_ROBOT_TO_OBS) bvh_free(&C->scene_tri);
     else {
-        for (int l = 0; l < R->n_links; ++l) bvh_free(&C.link_tri[l]);
-        free(C.link_tri);
+        bvh_free(&C->scene_edge);
+        for (int l = 0; l < C->R->n_links; ++l) bvh_free(&C->link_tri[l]);
+        free(C->link_tri);
     }
+    free(C);
+}
+
+/* early != 0: flags only, each pose stops at its first hit (count/band/marg
+ * are then partial and must not be used). */
+int orc_discrete_run(void* h, const float* q, int n, double eps, int threads, int early, unsigned char* hit, u32* count,
+                     unsigned char* band, unsigned char* marg, orc_work* work) {
+    disc_ctx* C = (disc_ctx*) h;
+    C->q = q; C->eps = eps; C->early = early;
+    C->hit = hit; C->count = count; C->band = band; C->marg = marg; C->work = work;
+    run_pool(n, threads, disc_pose, C, sizeof(u32) * (size_t) (C->S->n_edges + 1));
+    return 0;
+}
+
+int orc_discrete(int kind, const orc_robot* R, const orc_scene* S, const float* q, int n, double eps, int threads,
+                 unsigned char* hit, u32* count, unsigned char* band, unsigned char* marg, orc_work* work) {
+    void* h = orc_discrete_prepare(kind, R, S);
+    orc_discrete_run(h, q, n, eps, threads, 0, hit, count, band, marg, work);
+    orc_discrete_free(h);
     return 0;
 }
 

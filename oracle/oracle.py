@@ -146,6 +146,31 @@ def discrete(kind, robot, scene, q, eps=1e-5, threads=None, work=False):
     return out
 
 
+class PreparedDiscrete:
+    """Acceleration structures built once; ``run`` times the queries alone."""
+
+    def __init__(self, kind, robot, scene):
+        self.robot, self.scene = robot, scene
+        lib().orc_discrete_prepare.restype = C.c_void_p
+        self.h = C.c_void_p(lib().orc_discrete_prepare(C.c_int(kind), C.byref(robot.s), C.byref(scene.s)))
+
+    def flags(self, q, threads=None):
+        """Flags only, each pose stopping at its first hit."""
+        q = _c(q, np.float32)
+        hit = np.zeros(len(q), np.uint8)
+        lib().orc_discrete_run(self.h, _p(q, F), C.c_int(len(q)), D(1e-5), C.c_int(threads or threads_default()),
+                               C.c_int(1), _p(hit, B), None, None, None, None)
+        return hit
+
+    def close(self):
+        if self.h:
+            lib().orc_discrete_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
 def quad_ctrl_count(n_wp):
     return max(3, -(-int(n_wp) // 2))
 

@@ -262,6 +262,10 @@ struct rtcd_detector {
     std::mutex mu;
     cudaStream_t stream = nullptr;
     cudaEvent_t staged = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage timing: start, prepared, culled, traversed
+    cudaEvent_t ev_end = nullptr;
+    bool timed = false;
+    cudaStream_t last_stream = nullptr;  // stream of the last check (stats read on it)
     uint32_t blocks = 0;
     // discrete workspace
     DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
@@ -579,6 +583,8 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         if (!d->cfg.frame_size) d->cfg.frame_size = 64;
         cuda_check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming), "cudaEventCreate");
+        for (auto& e : d->ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&d->ev_end), "cudaEventCreate");
         if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS)
             d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
         else
@@ -599,6 +605,8 @@ rtcd_status rtcd_detector_destroy(rtcd_detector* d) {
         DeviceScope ds(d->ctx->device);
         cudaStreamSynchronize(d->stream);
         cudaEventDestroy(d->staged);
+        for (auto& e : d->ev) cudaEventDestroy(e);
+        cudaEventDestroy(d->ev_end);
         cudaStreamDestroy(d->stream);
         delete d;
     });
@@ -708,7 +716,10 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     d->T.ensure(48ull * n * L);
     d->mask.ensure((size_t) n * L);
     d->items.ensure(4ull * n * L);
+    const bool timed = (flags & RTCD_CHECK_TIMING) && !plain;
+    if (timed) cuda_check(cudaEventRecord(d->ev[0], s), "event");
     launch_fk_poses(R.chain, d_q, n, d->T.as<float4>(), s);
+    if (timed) cuda_check(cudaEventRecord(d->ev[1], s), "event");
     if (flags & RTCD_CHECK_NO_CULL) {
         launch_all_items(R, n, d->items.as<uint32_t>(), d->count.as<uint32_t>(), s);
     } else {
@@ -739,7 +750,10 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     A.err = d->err.as<uint32_t>();
     A.stats = d->stats.as<unsigned long long>();
     A.want_counts = counts ? 1 : 0;
+    if (timed) cuda_check(cudaEventRecord(d->ev[2], s), "event");
     launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+    if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
+    d->timed = timed;
     if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);
 }
 
@@ -867,6 +881,9 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     const uint32_t* dco = dwp + 2 * (n + 1);
     const uint32_t* dpt = dwp + 3 * (n + 1);
     d->centers.ensure(16ull * total_wp * ns);
+    const bool timed = (flags & RTCD_CHECK_TIMING) != 0;
+    d->timed = timed;
+    if (timed) cuda_check(cudaEventRecord(d->ev[0], s), "event");
     launch_fk_spheres(R, d_q, total_wp, d->centers.as<float4>(), s);
     if (quad) {
         d->ctrl.ensure(16ull * ctrl_total * ns);
@@ -907,7 +924,12 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.want_counts = counts;
     A.want_pieces = want_pieces;
     d->last_items = A.total_units;
+    if (timed) {
+        cuda_check(cudaEventRecord(d->ev[1], s), "event");
+        cuda_check(cudaEventRecord(d->ev[2], s), "event");
+    }
     if (A.total_units) launch_sweep(d->scene->dev, A, d->blocks, s);
+    if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     // outputs
     uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
     launch_flags(d->pose_hit.as<uint32_t>(), n, d_flags, s);
@@ -947,6 +969,8 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
         std::lock_guard<std::mutex> lock(d->mu);
         DeviceScope ds(d->ctx->device);
         cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
+        d->timed = false;
+        d->last_stream = s;
         if (n == 0) return;
         if (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) {
             RTCD_REQUIRE(!seg_flags_out, "segment flags exist only for sweep detectors");
@@ -955,6 +979,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             RTCD_REQUIRE(!(flags & RTCD_CHECK_PLAIN), "the plain frame path is for the discrete detectors");
             check_sweep(d, q, traj_offsets, n, flags_out, seg_flags_out, counts_out, flags, s);
         }
+        if (d->timed) cuda_check(cudaEventRecord(d->ev_end, s), "event");
         if (flags & RTCD_CHECK_HOST_BUFFERS) check_device_errors(d, s);
     });
 }
@@ -990,10 +1015,17 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
         std::memset(out, 0, sizeof(*out));
         unsigned long long st[8] = {0};
         uint32_t cnt = 0;
-        cuda_check(cudaMemcpyAsync(st, d->stats.p, sizeof(st), cudaMemcpyDeviceToHost, d->stream), "stats");
-        cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, d->stream), "stats");
-        cuda_check(cudaStreamSynchronize(d->stream), "stats sync");
+        cudaStream_t s = d->last_stream ? d->last_stream : d->stream;
+        cuda_check(cudaMemcpyAsync(st, d->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s), "stats");
+        cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, s), "stats");
+        cuda_check(cudaStreamSynchronize(s), "stats sync");
         out->fp64_retests = st[0];
+        if (d->timed) {
+            cuda_check(cudaEventElapsedTime(&out->ms_prepare, d->ev[0], d->ev[1]), "elapsed");
+            cuda_check(cudaEventElapsedTime(&out->ms_cull, d->ev[1], d->ev[2]), "elapsed");
+            cuda_check(cudaEventElapsedTime(&out->ms_traverse, d->ev[2], d->ev[3]), "elapsed");
+            cuda_check(cudaEventElapsedTime(&out->ms_total, d->ev[0], d->ev_end), "elapsed");
+        }
         out->work_items = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) && !d->last_items ? cnt
                                                                                                           : d->last_items;
     });

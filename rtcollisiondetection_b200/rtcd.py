@@ -25,6 +25,7 @@ CHECK_HOST_BUFFERS = 1 << 1
 CHECK_NO_CULL = 1 << 2
 CHECK_PLAIN = 1 << 3
 CHECK_NO_ENDPOINTS = 1 << 4
+CHECK_TIMING = 1 << 5
 
 STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
           4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}
@@ -57,7 +58,8 @@ class Config(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [('work_items', C.c_uint64), ('culled_items', C.c_uint64), ('fp64_retests', C.c_uint64),
-                ('reserved', C.c_uint64 * 5)]
+                ('ms_prepare', C.c_float), ('ms_cull', C.c_float), ('ms_traverse', C.c_float),
+                ('ms_total', C.c_float), ('reserved', C.c_uint64 * 3)]
 
 
 _lib = None
@@ -302,7 +304,8 @@ class Detector:
     def stats(self):
         s = Stats()
         _ok(lib().rtcd_last_stats(self.h, C.byref(s)))
-        return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests}
+        return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests, 'ms_prepare': s.ms_prepare,
+                'ms_cull': s.ms_cull, 'ms_traverse': s.ms_traverse, 'ms_total': s.ms_total}
 
     def close(self):
         if self.h:

@@ -4,12 +4,17 @@ Every generator is deterministic for a given seed (numpy PCG64).  The shapes,
 sizes and value ranges follow the benchmark workloads of the detector:
 
 * ``discrete_small``  - 12 axis-aligned boxes (extents U(0.02, 0.6) m) and 16
-  level-2 icospheres (radius U(0.03, 0.1) m) in the workspace
-  x in [0, 1], y in [-0.5, 0.5], z in [0, 1] (5,264 triangles);
-* ``discrete_dense``  - 64 boxes, 256 level-3 icospheres and one
-  100,000-triangle sphere with seeded radial displacement noise of amplitude
-  0.1 r (about 428k triangles; ``ico_level=2`` gives the 183k variant);
-* ``sweep_scene``     - 12 boxes and 155 level-2 icospheres (49,744 triangles).
+  level-2 icospheres (radius U(0.03, 0.1) m) in the 1 m cube in front of the
+  robot, x in [0, 1], y in [-0.5, 0.5], z in [0, 1] (5,264 triangles);
+* ``discrete_dense``  - 64 boxes (extents U(0.02, 0.4) m), 256 level-3
+  icospheres (radius U(0.03, 0.1) m) and one 100,000-triangle sphere
+  (radius 0.15 m) with seeded radial displacement noise of amplitude 0.1 r,
+  about 428k triangles (``ico_level=2`` gives the 183k variant), spread over
+  the robot-centred box x, y in [-1.5, 1.5], z in [0, 1.5]: packed into the
+  1 m cube every random pose collides;
+* ``sweep_scene``     - 12 boxes (extents U(0.02, 0.3) m) and 155 level-2
+  icospheres (radius U(0.02, 0.06) m), 49,744 triangles, over the same
+  robot-centred box.
 
 Poses are uniform within the joint limits; trajectories are random walks with
 N(0, 0.1) rad steps clipped to the limits.  The robot model (Panda) comes from
@@ -21,6 +26,8 @@ import numpy as np
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data')
 WORKSPACE_LO = np.array([0.0, -0.5, 0.0])
 WORKSPACE_HI = np.array([1.0, 0.5, 1.0])
+WIDE_LO = np.array([-1.5, -1.5, 0.0])
+WIDE_HI = np.array([1.5, 1.5, 1.5])
 
 
 class Mesh:
@@ -132,48 +139,46 @@ def _assemble(parts):
     return Mesh(np.concatenate(verts), np.concatenate(tris), np.asarray(off, np.uint32))
 
 
-def _uniform_center(rng):
-    return rng.uniform(WORKSPACE_LO, WORKSPACE_HI)
-
-
 def random_scene(n_boxes, n_icos, ico_level, seed=0, big_sphere_tris=0, big_sphere_radius=0.15,
-                 ico_r=(0.03, 0.1), box_ext=(0.02, 0.6)):
+                 ico_r=(0.03, 0.1), box_ext=(0.02, 0.6), workspace=(WORKSPACE_LO, WORKSPACE_HI)):
     rng = np.random.default_rng(seed)
+    lo, hi = workspace
     parts = []
     for _ in range(n_boxes):
-        parts.append(box_mesh(_uniform_center(rng), rng.uniform(box_ext[0], box_ext[1], size=3)))
+        parts.append(box_mesh(rng.uniform(lo, hi), rng.uniform(box_ext[0], box_ext[1], size=3)))
     uv, ut = icosphere(ico_level)
     for _ in range(n_icos):
         r = rng.uniform(*ico_r)
-        parts.append((uv * r + _uniform_center(rng), ut))
+        parts.append((uv * r + rng.uniform(lo, hi), ut))
     if big_sphere_tris:
         n_lon = 250
         n_lat = big_sphere_tris // (2 * n_lon) + 1
         sv, st = latlong_sphere(n_lon, n_lat)
         radial = big_sphere_radius * (1.0 + 0.1 * rng.uniform(-1.0, 1.0, size=len(sv)))
-        parts.append((sv * radial[:, None] + _uniform_center(rng), st))
+        parts.append((sv * radial[:, None] + rng.uniform(lo, hi), st))
     return _assemble(parts)
 
 
 def discrete_small(seed=0):
-    """12 boxes + 16 level-2 icospheres: 5,264 triangles."""
+    """12 boxes + 16 level-2 icospheres in the 1 m cube: 5,264 triangles."""
     return random_scene(12, 16, 2, seed)
 
 
 def discrete_dense(seed=0, ico_level=3):
-    """64 boxes + 256 icospheres (level 3: ~428k triangles with the 100k sphere)."""
-    return random_scene(64, 256, ico_level, seed, big_sphere_tris=100_000)
+    """64 boxes + 256 icospheres + the 100k noisy sphere (level 3: ~428k triangles)."""
+    return random_scene(64, 256, ico_level, seed, big_sphere_tris=100_000, box_ext=(0.02, 0.4),
+                        workspace=(WIDE_LO, WIDE_HI))
 
 
 def sweep_scene(seed=0):
     """12 boxes + 155 level-2 icospheres: 49,744 triangles."""
-    return random_scene(12, 155, 2, seed)
+    return random_scene(12, 155, 2, seed, ico_r=(0.02, 0.06), box_ext=(0.02, 0.3), workspace=(WIDE_LO, WIDE_HI))
 
 
 def served_large_scene(seed=0):
     """Dense scene plus 225 extra level-2 icospheres (~500k triangles)."""
     base = discrete_dense(seed)
-    extra = random_scene(0, 225, 2, seed + 1)
+    extra = random_scene(0, 225, 2, seed + 1, workspace=(WIDE_LO, WIDE_HI))
     v = np.concatenate([base.verts, extra.verts])
     t = np.concatenate([base.tris, extra.tris + len(base.verts)])
     off = np.concatenate([base.obstacle_tri_off, extra.obstacle_tri_off[1:] + base.obstacle_tri_off[-1]])

@@ -55,11 +55,13 @@ def test_cull_plain_and_device_paths_agree(setup, panda, name, okind):
     c = det.check(q, counts=True, flags=rtcd.CHECK_PLAIN)
     assert np.array_equal(a['flags'], b['flags']) and np.array_equal(a['counts'], b['counts'])
     assert np.array_equal(a['flags'], c['flags']) and np.array_equal(a['counts'], c['counts'])
-    qd = torch.from_numpy(q).cuda()
-    fd = torch.zeros(len(q), dtype=torch.uint8, device='cuda')
-    cd = torch.zeros(len(q), dtype=torch.int32, device='cuda')
-    det.check_device(qd, len(q), fd, counts_dev=cd, stream=torch.cuda.current_stream().cuda_stream)
-    det.sync(torch.cuda.current_stream().cuda_stream)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        qd = torch.from_numpy(q).cuda()
+        fd = torch.zeros(len(q), dtype=torch.uint8, device='cuda')
+        cd = torch.zeros(len(q), dtype=torch.int32, device='cuda')
+        det.check_device(qd, len(q), fd, counts_dev=cd, stream=s.cuda_stream)
+        det.sync(s.cuda_stream)
     assert np.array_equal(fd.cpu().numpy(), a['flags'])
     assert np.array_equal(cd.cpu().numpy().astype(np.uint32), a['counts'])
 

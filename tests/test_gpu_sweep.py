@@ -1,0 +1,105 @@
+"""Continuous detectors (linear capsules, quadratic B-spline sweeps) against
+the FP64 oracle: trajectory and segment flags outside the 1e-5 m band,
+hit counts wherever no primitive pair is marginal."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from rtcollisiondetection_b200 import rtcd, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def sweep_setup(ctx, panda):
+    sph = scenes.synth_spheres(panda, per_link=8, seed=0)
+    mesh = scenes.sweep_scene()
+    robot = rtcd.Robot(ctx, panda, spheres=sph)
+    scene = rtcd.Scene.from_mesh(ctx, mesh)
+    return robot, scene, O.Robot(panda, spheres=sph), O.Scene(mesh)
+
+
+def _cmp(out, ref):
+    tb = ref['traj_band'].astype(bool)
+    m = (out['flags'] != ref['traj_hit']) & ~tb
+    assert m.sum() == 0, 'trajectory flag mismatches at %s' % np.nonzero(m)[0][:20]
+    if 'seg_flags' in out:
+        sb = ref['seg_band'].astype(bool)
+        ms = (out['seg_flags'] != ref['seg_hit']) & ~sb
+        assert ms.sum() == 0, 'segment flag mismatches at %s' % np.nonzero(ms)[0][:20]
+        # a trajectory is hit iff one of its segments is
+        off = out['seg_off']
+        for t in range(len(out['flags'])):
+            assert out['flags'][t] == out['seg_flags'][off[t]:off[t + 1]].max(initial=0)
+    if 'counts' in out:
+        safe = ~ref['traj_marg'].astype(bool)
+        mc = (out['counts'] != ref['traj_count']) & safe
+        assert mc.sum() == 0, 'count mismatches at %s' % np.nonzero(mc)[0][:20]
+
+
+def test_linear_parity(sweep_setup, panda):
+    robot, scene, orob, osc = sweep_setup
+    q, off = scenes.random_walk_trajectories(panda, 256, 32, seed=0)
+    ref = O.sweep(False, orob, osc, q, off)
+    det = rtcd.Detector(robot.ctx, 'Linear', robot, scene)
+    _cmp(det.check(q, off, segments=True), ref)
+    _cmp(det.check(q, off, counts=True, segments=True), ref)
+    plain = det.check(q, off)
+    _cmp(plain, ref)
+    assert 0.05 < ref['traj_hit'].mean() < 0.99
+
+
+def test_quadratic_parity_uneven(sweep_setup, panda):
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(192, 8, 64, seed=1)
+    q, off = scenes.random_walk_trajectories(panda, 192, n_wp, seed=1)
+    ref = O.sweep(True, orob, osc, q, off)
+    det = rtcd.Detector(robot.ctx, 'Quadratic', robot, scene)
+    _cmp(det.check(q, off, segments=True), ref)
+    _cmp(det.check(q, off, counts=True), ref)
+    ref_ne = O.sweep(True, orob, osc, q, off, endpoints=False)
+    _cmp(det.check(q, off, segments=True, flags=rtcd.CHECK_NO_ENDPOINTS), ref_ne)
+
+
+def test_quadratic_fit_weights_on_device_match_tables(sweep_setup, panda):
+    """The device fit uses W = pinv(B): a trajectory whose waypoints lie on a
+    quadratic B-spline is reproduced, so its sweep equals the spline's sweep."""
+    robot, scene, orob, osc = sweep_setup
+    q, off = scenes.random_walk_trajectories(panda, 64, 32, seed=5)
+    det = rtcd.Detector(robot.ctx, 'Quadratic', robot, scene)
+    ref = O.sweep(True, orob, osc, q, off)
+    _cmp(det.check(q, off, segments=True), ref)
+
+
+def test_short_and_single_trajectories(sweep_setup, panda):
+    robot, scene, orob, osc = sweep_setup
+    for kind, quad, wp in (('Linear', False, [2, 3, 2]), ('Quadratic', True, [3, 4, 5])):
+        q, off = scenes.random_walk_trajectories(panda, 3, wp, seed=2)
+        det = rtcd.Detector(robot.ctx, kind, robot, scene)
+        _cmp(det.check(q, off, segments=True, counts=True), O.sweep(quad, orob, osc, q, off))
+        one = det.check(q[:off[1]], off[:2])
+        assert one['flags'][0] == det.check(q, off)['flags'][0]
+
+
+def test_sweep_results_independent_of_batch(sweep_setup, panda):
+    robot, scene, _, _ = sweep_setup
+    n_wp = scenes.log_uniform_counts(64, 8, 40, seed=3)
+    q, off = scenes.random_walk_trajectories(panda, 64, n_wp, seed=3)
+    det = rtcd.Detector(robot.ctx, 'Quadratic', robot, scene)
+    full = det.check(q, off)['flags']
+    for a, b in ((0, 10), (10, 11), (11, 64)):
+        sub_off = off[a:b + 1] - off[a]
+        part = det.check(q[off[a]:off[b]], sub_off)['flags']
+        assert np.array_equal(part, full[a:b])
+
+
+def test_sweep_rejects_bad_offsets(sweep_setup):
+    robot, scene, _, _ = sweep_setup
+    det = rtcd.Detector(robot.ctx, 'Linear', robot, scene)
+    with pytest.raises(rtcd.RTCDError):
+        det.check(np.zeros((4, 7), np.float32), np.array([0, 3, 1], np.uint32))
+    with pytest.raises(rtcd.RTCDError):
+        det.check(np.zeros((4, 7), np.float32), np.array([0, 1], np.uint32))  # one waypoint
+    qd = rtcd.Detector(robot.ctx, 'Quadratic', robot, scene)
+    with pytest.raises(rtcd.RTCDError):
+        qd.check(np.zeros((2, 7), np.float32), np.array([0, 2], np.uint32))
