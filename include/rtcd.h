@@ -196,6 +196,25 @@ RTCD_API rtcd_status rtcd_exclusive_scan_u32(rtcd_ctx* ctx, const uint32_t* in_d
 RTCD_API rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
                                           uint32_t* count_dev, void* stream);
 
+/* rtcd_select_flags_u8 for callers that cannot allocate device memory when
+ * they query: a control loop with a hard deadline cannot afford cudaMalloc /
+ * cudaFree (they may synchronise the device and take unbounded time), and a
+ * process whose device memory belongs to another owner may not allocate at
+ * all.  No counterpart in the reference.  The look-back scratch lives in a
+ * fixed 131 KB device array inside this library, so the call allocates
+ * nothing; that array is held on every GPU that loads the library until the
+ * process exits.  Limit: n <= 33,554,432 flags (RTCD_ERR_CAPACITY beyond).
+ * The first call on a device, made with that device current, looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  All calls share the one array, and it keeps the
+ * previous call's contents (each call first clears the words it uses); two
+ * calls that overlap on the GPU would race on it, so the library serialises
+ * them: each call takes a process-wide lock and returns only after its work
+ * has finished.  `stream` is a cudaStream_t (NULL = the legacy default
+ * stream); on return idx_dev / count_dev hold the result. */
+RTCD_API rtcd_status rtcd_select_flags_u8_noalloc(const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
+                                                  uint32_t* count_dev, void* stream);
+
 /* Canonical LBVH over n boxes (replaces optixAccelBuild, RTCD/Meshes/mesh.h:725-740).
  * Host arrays: lo/hi float[n][3] in; codes_out[n] (sorted Morton codes),
  * perm_out[n] (sorted position -> box), child_out[2(n-1)] (bit 31 set = leaf

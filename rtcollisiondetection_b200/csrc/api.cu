@@ -24,6 +24,8 @@ static thread_local std::string g_last_error;
 
 void fail(int status, const std::string& msg) { throw Error{status, msg}; }
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 void cuda_check(cudaError_t e, const char* what) {
     if (e == cudaSuccess) return;
     cudaGetLastError();

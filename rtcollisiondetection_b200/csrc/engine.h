@@ -17,6 +17,7 @@ struct Error {
 };
 
 [[noreturn]] void fail(int status, const std::string& msg);
+void set_last_error(const std::string& msg);  // the message rtcd_last_error returns on this thread
 void cuda_check(cudaError_t e, const char* what);
 
 // Grow-only device allocation.
@@ -65,6 +66,12 @@ void scan_u32(const uint32_t* d_in, uint32_t* d_out, uint32_t n, uint32_t* d_tot
 // Stable compaction of the indices of nonzero mask bytes.
 void select_u8(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_count, ScanScratch& sc, uint32_t* d_err,
                cudaStream_t s);
+
+// The same compaction with caller-provided look-back scratch: d_status needs
+// one zeroed word per 2048 flags (at least one), d_counter and d_err zeroed.
+void select_u8_raw(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_count,
+                   unsigned long long* d_status, uint32_t* d_counter, uint32_t* d_err, cudaStream_t s);
+constexpr uint32_t kSelectTileFlags = 2048;  // flags per look-back tile of the compaction kernel
 
 // A packed LBVH over one primitive set.
 struct LbvhResult {

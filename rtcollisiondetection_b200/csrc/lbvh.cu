@@ -43,6 +43,14 @@ void select_u8(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_c
     cuda_check(cudaGetLastError(), "k_select_u8");
 }
 
+void select_u8_raw(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_count,
+                   unsigned long long* d_status, uint32_t* d_counter, uint32_t* d_err, cudaStream_t s) {
+    uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
+    ScanState st{d_status, d_counter, d_err};
+    k_select_u8<<<tiles, kScanThreads, 0, s>>>(d_mask, n, d_out, d_count, st);
+    cuda_check(cudaGetLastError(), "k_select_u8");
+}
+
 // ---------------------------------------------------------------- prim boxes
 __global__ void k_tri_boxes(const float* __restrict__ v, const uint32_t* __restrict__ t, uint32_t n, float4* lo,
                             float4* hi) {
