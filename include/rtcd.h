@@ -64,6 +64,7 @@ typedef enum {
 #define RTCD_CHECK_PLAIN (1u << 3)         /* frame-by-frame path with a host sync per frame */
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
 #define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
+#define RTCD_CHECK_FUSED (1u << 6)         /* discrete: one fused traversal kernel instead of the two-stage wavefront */
 
 typedef struct rtcd_ctx rtcd_ctx;
 typedef struct rtcd_robot rtcd_robot;
@@ -175,6 +176,55 @@ typedef struct {
     uint64_t reserved[3];
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
+
+/* ---- serving: continuous batching over resident scenes ----
+ *
+ * The upstream detector serves one caller at a time: check() splits a query
+ * into frames of BATCHSIZE over NSTREAM streams with a thread pool
+ * (CollisionDetector.h:354-471, threadPool.h:10-92).  A server instead takes
+ * requests of any size from any thread as they arrive, merges queued requests
+ * for the same detector into one launch, runs up to `slots` launches
+ * concurrently (one stream and one workspace each), and admits a launch only
+ * while the bytes of the launches in flight stay within a memory budget.
+ * Each request's result equals what rtcd_check returns for it alone. */
+typedef struct rtcd_server rtcd_server;
+
+typedef struct {
+    uint32_t slots;           /* launches in flight at once; 0 = 4 */
+    uint32_t max_batch_units; /* poses / trajectory waypoints merged into one launch; 0 = 65536 */
+    uint64_t memory_budget;   /* bytes the in-flight launches may hold; 0 = half the free device memory */
+    uint32_t reserved[4];
+} rtcd_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint64_t units_completed;   /* poses + trajectories */
+    uint64_t batches;           /* launches */
+    uint64_t inflight_bytes_peak;
+    uint32_t queue_depth;       /* requests waiting for a slot */
+    uint32_t reserved0;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result ready, over completed requests */
+    uint64_t reserved[4];
+} rtcd_server_stats;
+
+#define RTCD_WAIT_FOREVER (-1)
+
+RTCD_API rtcd_status rtcd_server_create(rtcd_ctx* ctx, const rtcd_server_config* config, rtcd_server** out);
+/* Finishes every accepted request, then stops the workers. */
+RTCD_API rtcd_status rtcd_server_destroy(rtcd_server* server);
+/* Copies the inputs (host memory, as rtcd_check with RTCD_CHECK_HOST_BUFFERS)
+ * and returns a ticket at once.  `flags` may carry RTCD_CHECK_COUNTS and
+ * RTCD_CHECK_NO_ENDPOINTS. */
+RTCD_API rtcd_status rtcd_server_submit(rtcd_server* server, rtcd_detector* det, const float* q,
+                                        const uint32_t* traj_offsets, uint32_t n, uint32_t flags, uint64_t* ticket);
+/* Waits up to timeout_ms (RTCD_WAIT_FOREVER: no limit) for the ticket; on
+ * completion copies the outputs (any may be NULL), releases the ticket and
+ * reports the request's latency.  RTCD_ERR_DEVICE_TIMEOUT when the wait ran
+ * out (the ticket stays valid). */
+RTCD_API rtcd_status rtcd_server_wait(rtcd_server* server, uint64_t ticket, int32_t timeout_ms, uint8_t* flags_out,
+                                      uint8_t* seg_flags_out, uint32_t* counts_out, double* latency_ms);
+RTCD_API rtcd_status rtcd_server_get_stats(rtcd_server* server, rtcd_server_stats* out);
+RTCD_API rtcd_status rtcd_server_reset_stats(rtcd_server* server);
 
 /* ---- building blocks, exposed for callers that compose their own pipelines ---- */
 

@@ -271,6 +271,8 @@ struct rtcd_detector {
     uint32_t blocks = 0;
     // discrete workspace
     DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
+    DevBuf cand, item_overflow, overflow_items, wave_counts;  // wavefront traversal
+    uint32_t blocks_a = 0, blocks_b = 0;
     ScanScratch scan;
     // sweep workspace
     DevBuf centers, ctrl, aux, piece_hit, W, W_off;
@@ -587,10 +589,13 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         cuda_check(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming), "cudaEventCreate");
         for (auto& e : d->ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         cuda_check(cudaEventCreate(&d->ev_end), "cudaEventCreate");
-        if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS)
+        if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS) {
             d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
-        else
-            d->blocks = sweep_persistent_blocks();
+            d->blocks_a = stage_a_blocks(kind == RTCD_ROBOT_TO_OBS);
+            d->blocks_b = stage_b_blocks(kind == RTCD_ROBOT_TO_OBS);
+        } else {
+            d->blocks = sweep_persistent_blocks(kind == RTCD_QUAD_SWEEP);
+        }
         d->err.ensure(4);
         d->stats.ensure(8 * 8);
         d->work.ensure(4);
@@ -600,6 +605,24 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         *out = d.release();
     });
 }
+
+}  // extern "C"
+
+namespace rtcd {
+void detector_info(rtcd_detector* d, rtcd_ctx** ctx, int* kind, rtcd_robot** robot, rtcd_scene** scene,
+                   rtcd_config* cfg, uint32_t* n_links, uint32_t* n_spheres, uint32_t* dof) {
+    *ctx = d->ctx;
+    *kind = (int) d->kind;
+    *robot = d->robot;
+    *scene = d->scene;
+    *cfg = d->cfg;
+    *n_links = d->robot->dev.n_links;
+    *n_spheres = d->robot->dev.n_spheres;
+    *dof = d->robot->dof;
+}
+}  // namespace rtcd
+
+extern "C" {
 
 rtcd_status rtcd_detector_destroy(rtcd_detector* d) {
     return guarded([&] {
@@ -739,6 +762,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         blocks = (cnt + kTravThreads - 1) / kTravThreads;
     }
     cuda_check(cudaMemsetAsync(d->work.p, 0, 4, s), "memset");
+    const bool fused = (flags & RTCD_CHECK_FUSED) != 0;
     DiscreteArgs A{};
     A.T = d->T.as<float4>();
     A.items = d->items.as<uint32_t>();
@@ -753,7 +777,36 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     A.stats = d->stats.as<unsigned long long>();
     A.want_counts = counts ? 1 : 0;
     if (timed) cuda_check(cudaEventRecord(d->ev[2], s), "event");
-    launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+    if (fused) {
+        launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+    } else {
+        // stage A -> stage B -> the fused kernel over items whose candidates overflowed
+        const size_t items_max = (size_t) n * L;
+        const uint32_t cap = (uint32_t) std::min<size_t>(std::max<size_t>(items_max * 128, 1u << 16), 1u << 26);
+        d->cand.ensure(8ull * cap);
+        d->item_overflow.ensure(items_max);
+        d->overflow_items.ensure(4ull * items_max);
+        d->wave_counts.ensure(4 * 4);
+        cuda_check(cudaMemsetAsync(d->item_overflow.p, 0, items_max, s), "memset");
+        cuda_check(cudaMemsetAsync(d->wave_counts.p, 0, 16, s), "memset");
+        uint32_t* wc = d->wave_counts.as<uint32_t>();  // [0] candidates, [1] overflowed items, [2] fallback work
+        WaveArgs W{};
+        W.d = A;
+        W.cand = d->cand.as<uint2>();
+        W.cand_count = wc;
+        W.cand_cap = cap;
+        W.item_overflow = d->item_overflow.as<uint8_t>();
+        W.overflow_items = d->overflow_items.as<uint32_t>();
+        W.overflow_count = wc + 1;
+        uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
+        launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
+        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, s);
+        DiscreteArgs F = A;
+        F.items = d->overflow_items.as<uint32_t>();
+        F.n_items = wc + 1;
+        F.work_counter = wc + 2;
+        launch_discrete(r2o, R, d->scene->dev, F, d->blocks, s);
+    }
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     d->timed = timed;
     if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);

@@ -181,32 +181,59 @@ void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t
 // ---------------------------------------------------------------- exact tests
 // Segment pq against triangle abc, FP32 with an error filter.
 // 0 = certain miss, 1 = certain hit, 2 = too close to call in FP32.
-// Five signed volumes decide the crossing: the endpoint sides of the plane
-// and the three edge volumes of the segment's line (Plucker sides).  A value
-// within kRel of its magnitude bound is uncertain; the bound covers both the
-// FP32 rounding here and the rounding of the frame change before it.
+// Five signed volumes decide the crossing: the endpoint sides of the plane,
+// n.(p - a) and n.(q - a), and the three edge volumes of the segment's line,
+// d.((a - p) x (b - a)) and its two rotations (Plucker sides, written with the
+// short triangle edges so no large cross product cancels).  Each volume is a
+// distance times known lengths; it is uncertain when that distance is below
+// kDist plus a relative rounding term.  kDist (1 um) is twenty times the
+// coordinate error of the frame change before the test and far below the
+// 1e-5 m parity band, so FP32 decides everything outside the band and the
+// FP64 re-test only sees true near-degeneracies.
 __device__ __forceinline__ float l1(f3 v) { return fabsf(v.x) + fabsf(v.y) + fabsf(v.z); }
 
 __device__ __forceinline__ int sgn_tol(float v, float tol) { return v > tol ? 1 : (v < -tol ? -1 : 0); }
 
 __device__ __forceinline__ int seg_tri_f32(f3 p, f3 q, f3 a, f3 b, f3 c) {
-    constexpr float kRel = 1e-4f;
-    f3 e1 = b - a, e2 = c - a, n = cross(e1, e2);
+    constexpr float kDist = 1e-6f, kRel = 4e-6f;
+    f3 ab = b - a, bc = c - b, ca = a - c;
+    f3 n = cross(ab, c - a);
     f3 pa = p - a, qa = q - a;
     float nl = l1(n);
-    int sp = sgn_tol(dot(n, pa), kRel * nl * l1(pa));
-    int sq = sgn_tol(dot(n, qa), kRel * nl * l1(qa));
+    int sp = sgn_tol(dot(n, pa), nl * (kDist + kRel * l1(pa)));
+    int sq = sgn_tol(dot(n, qa), nl * (kDist + kRel * l1(qa)));
     if (sp == sq && sp != 0) return 0;
     f3 d = q - p, ap = a - p, bp = b - p, cp = c - p;
-    float dl = l1(d), al = l1(ap), bl = l1(bp), cl = l1(cp);
-    int s1 = sgn_tol(dot(d, cross(ap, bp)), kRel * dl * al * bl);
-    int s2 = sgn_tol(dot(d, cross(bp, cp)), kRel * dl * bl * cl);
-    int s3 = sgn_tol(dot(d, cross(cp, ap)), kRel * dl * cl * al);
+    float dl = l1(d);
+    int s1 = sgn_tol(dot(d, cross(ap, ab)), dl * l1(ab) * (kDist + kRel * l1(ap)));
+    int s2 = sgn_tol(dot(d, cross(bp, bc)), dl * l1(bc) * (kDist + kRel * l1(bp)));
+    int s3 = sgn_tol(dot(d, cross(cp, ca)), dl * l1(ca) * (kDist + kRel * l1(cp)));
     bool pos = s1 > 0 || s2 > 0 || s3 > 0, neg = s1 < 0 || s2 < 0 || s3 < 0;
     if (pos && neg) return 0;
     if (sp != 0 && sq != 0 && s1 != 0 && s2 != 0 && s3 != 0) return 1;
     return 2;
 }
+
+// Segment p + t d, t in [0, 1], against a box (slab test); inv = 1 / d per axis
+// (infinite for a zero component), boxes padded by `pad`.
+__device__ __forceinline__ bool seg_box(const f3& p, const f3& inv, const Box& b, float pad) {
+    float t0x = (b.lo[0] - pad - p.x) * inv.x, t1x = (b.hi[0] + pad - p.x) * inv.x;
+    float t0y = (b.lo[1] - pad - p.y) * inv.y, t1y = (b.hi[1] + pad - p.y) * inv.y;
+    float t0z = (b.lo[2] - pad - p.z) * inv.z, t1z = (b.hi[2] + pad - p.z) * inv.z;
+    float tmin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+    float tmax = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), 1.0f));
+    return tmin <= tmax;
+}
+
+// A box that straddles (or touches, within pad) the plane n.x = w.
+__device__ __forceinline__ bool plane_box(const f3& n, float w, const Box& b, float pad) {
+    float cx = 0.5f * (b.lo[0] + b.hi[0]), cy = 0.5f * (b.lo[1] + b.hi[1]), cz = 0.5f * (b.lo[2] + b.hi[2]);
+    float r = fabsf(n.x) * (0.5f * (b.hi[0] - b.lo[0]) + pad) + fabsf(n.y) * (0.5f * (b.hi[1] - b.lo[1]) + pad) +
+              fabsf(n.z) * (0.5f * (b.hi[2] - b.lo[2]) + pad);
+    return fabsf(n.x * cx + n.y * cy + n.z * cz - w) <= r;
+}
+
+__device__ __forceinline__ float safe_inv(float v) { return v != 0.0f ? 1.0f / v : copysignf(3.0e38f, v); }
 
 __device__ __forceinline__ double orient2(double ax, double ay, double bx, double by, double cx, double cy) {
     return (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
@@ -252,6 +279,25 @@ __device__ __noinline__ bool seg_tri_f64(d3 p, d3 q, d3 a, d3 b, d3 c) {
            seg_seg_2d(U(p), V(p), U(q), V(q), U(c), V(c), U(a), V(a));
 }
 
+// The FP64 re-test of one (scene primitive, link primitive) pair, rebuilt in
+// the world frame from the stored floats and the link transform (out of line
+// so its double registers do not weigh on the traversal loop).
+// R2O: link edge li against scene triangle wi; else scene edge wi against link triangle li.
+template <bool R2O>
+__device__ __noinline__ bool retest_f64(const float4* T, const float4* __restrict__ lp, uint32_t li,
+                                        const float4* __restrict__ wp, uint32_t wi) {
+    if (R2O) {
+        const float4* e = lp + 2ull * li;
+        const float4* t = wp + 3ull * wi;
+        return seg_tri_f64(xf_d(T, f3of(__ldg(e))), xf_d(T, f3of(__ldg(e + 1))), d3of(f3of(__ldg(t))),
+                           d3of(f3of(__ldg(t + 1))), d3of(f3of(__ldg(t + 2))));
+    }
+    const float4* e = wp + 2ull * wi;
+    const float4* t = lp + 3ull * li;
+    return seg_tri_f64(d3of(f3of(__ldg(e))), d3of(f3of(__ldg(e + 1))), xf_d(T, f3of(__ldg(t))),
+                       xf_d(T, f3of(__ldg(t + 1))), xf_d(T, f3of(__ldg(t + 2))));
+}
+
 // Conservative OBB-vs-AABB test: the box's projection on the three world axes
 // and on the three OBB axes (6 of the 15 SAT axes).
 __device__ __forceinline__ bool obb_aabb(const Box& b, const ObbW& o, const f3& ext) {
@@ -289,6 +335,8 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
     ObbW ob;
     f3 ext;
     f3 c0, c1, c2;  // candidate in the link frame (c2 unused for edges)
+    f3 cn, cinv;    // candidate triangle normal (RobotToObs) / inverse segment direction (ObsToRobot)
+    float cw = 0.f; // plane offset n.c0 of the candidate triangle
     float blo[3], bhi[3];
 
     while (true) {
@@ -333,11 +381,21 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
                 cand = ref & ~kLeaf;
                 uint32_t lroot = R2O ? R.edge_root[link] : R.tri_root[link];
                 if (lroot == kNone) continue;
+                // link OBB in its own frame: the candidate must reach it
+                const float* lo = R.obb[link];
+                const f3 oc = mk(lo[0], lo[1], lo[2]);
+                const f3 u0 = mk(lo[6], lo[7], lo[8]), u1 = mk(lo[9], lo[10], lo[11]), u2 = mk(lo[12], lo[13], lo[14]);
                 if (R2O) {
                     const float4* t = wp + 3ull * cand;
                     c0 = xf_inv(T, f3of(__ldg(t)));
                     c1 = xf_inv(T, f3of(__ldg(t + 1)));
                     c2 = xf_inv(T, f3of(__ldg(t + 2)));
+                    cn = cross(c1 - c0, c2 - c0);
+                    cw = dot(cn, c0);
+                    // the triangle's plane must cut the link OBB
+                    float rr = (lo[3] + kBoxTol) * fabsf(dot(cn, u0)) + (lo[4] + kBoxTol) * fabsf(dot(cn, u1)) +
+                               (lo[5] + kBoxTol) * fabsf(dot(cn, u2));
+                    if (fabsf(dot(cn, oc) - cw) > rr) continue;
                     blo[0] = fminf(c0.x, fminf(c1.x, c2.x)); bhi[0] = fmaxf(c0.x, fmaxf(c1.x, c2.x));
                     blo[1] = fminf(c0.y, fminf(c1.y, c2.y)); bhi[1] = fmaxf(c0.y, fmaxf(c1.y, c2.y));
                     blo[2] = fminf(c0.z, fminf(c1.z, c2.z)); bhi[2] = fmaxf(c0.z, fmaxf(c1.z, c2.z));
@@ -345,6 +403,16 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
                     const float4* e = wp + 2ull * cand;
                     c0 = xf_inv(T, f3of(__ldg(e)));
                     c1 = xf_inv(T, f3of(__ldg(e + 1)));
+                    f3 d = c1 - c0;
+                    cinv = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+                    // the segment must pass through the link OBB (slab test in the OBB frame)
+                    f3 pr = c0 - oc;
+                    f3 po = mk(dot(pr, u0), dot(pr, u1), dot(pr, u2));
+                    f3 dd = mk(dot(d, u0), dot(d, u1), dot(d, u2));
+                    Box ob_local;
+                    ob_local.lo[0] = -lo[3]; ob_local.lo[1] = -lo[4]; ob_local.lo[2] = -lo[5];
+                    ob_local.hi[0] = lo[3]; ob_local.hi[1] = lo[4]; ob_local.hi[2] = lo[5];
+                    if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), ob_local, kBoxTol)) continue;
                     blo[0] = fminf(c0.x, c1.x); bhi[0] = fmaxf(c0.x, c1.x);
                     blo[1] = fminf(c0.y, c1.y); bhi[1] = fmaxf(c0.y, c1.y);
                     blo[2] = fminf(c0.z, c1.z); bhi[2] = fmaxf(c0.z, c1.z);
@@ -393,19 +461,7 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
             r = seg_tri_f32(p, q, a, b, c);
             if (r == 2) {
                 atomicAdd(A.stats, 1ull);
-                bool h;
-                if (R2O) {
-                    const float4* e = lp + 2ull * li;
-                    const float4* t = wp + 3ull * cand;
-                    h = seg_tri_f64(xf_d(T, f3of(__ldg(e))), xf_d(T, f3of(__ldg(e + 1))), d3of(f3of(__ldg(t))),
-                                    d3of(f3of(__ldg(t + 1))), d3of(f3of(__ldg(t + 2))));
-                } else {
-                    const float4* e = wp + 2ull * cand;
-                    const float4* t = lp + 3ull * li;
-                    h = seg_tri_f64(d3of(f3of(__ldg(e))), d3of(f3of(__ldg(e + 1))), xf_d(T, f3of(__ldg(t))),
-                                    xf_d(T, f3of(__ldg(t + 1))), xf_d(T, f3of(__ldg(t + 2))));
-                }
-                r = h ? 1 : 0;
+                r = retest_f64<R2O>(T, lp, li, wp, cand) ? 1 : 0;
             }
             if (r == 1) {
                 if (!A.want_counts) {
@@ -426,7 +482,14 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
         Box bl, br;
         uint32_t rl, rr;
         load_node(ln, ref, bl, br, rl, rr);
-        bool hr = box_overlap(br, blo, bhi), hl = box_overlap(bl, blo, bhi);
+        bool hr, hl;
+        if (R2O) {  // node box overlaps the triangle's box and straddles its plane
+            hr = box_overlap(br, blo, bhi) && plane_box(cn, cw, br, kBoxTol);
+            hl = box_overlap(bl, blo, bhi) && plane_box(cn, cw, bl, kBoxTol);
+        } else {    // the segment passes through the node box
+            hr = seg_box(c0, cinv, br, kBoxTol);
+            hl = seg_box(c0, cinv, bl, kBoxTol);
+        }
         if (spB + 2 > kStack) {
             atomicOr(A.err, kErrStack);
             hr = hl = false;
@@ -434,6 +497,249 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
         if (hr) stB[spB++] = rr;
         if (hl) stB[spB++] = rl;
     }
+}
+
+// ---------------------------------------------------------------- wavefront form
+// Stage A: one warp per (pose, link) item.  The warp descends the scene LBVH
+// with the link's world OBB through a shared LIFO frontier: each step the
+// lanes take up to 32 nodes off the top, test both children, push the
+// internal survivors and emit the leaf survivors as candidates - contiguously
+// per item, so stage B's neighbouring lanes share a link and a transform.
+template <bool R2O>
+__global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R, const SceneDev S, const WaveArgs W) {
+    constexpr float kBoxTol = 2e-5f;
+    __shared__ uint32_t s_front[kStageAWarps][kFrontier];
+    const DiscreteArgs& A = W.d;
+    const int lane = threadIdx.x & 31;
+    uint32_t* fr = s_front[threadIdx.x >> 5];
+    const uint32_t lt = (1u << lane) - 1u;
+    const float4* __restrict__ wn = R2O ? S.tri_nodes : S.edge_nodes;
+    const uint32_t wroot = R2O ? S.tri_root : S.edge_root;
+    const uint32_t n_items = *A.n_items;
+    while (true) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(A.work_counter, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        const uint32_t item = A.items[it];
+        const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
+        if (pose >= A.n_poses) {
+            if (lane == 0) atomicOr(A.err, kErrRange);
+            continue;
+        }
+        if (wroot == kNone || (!A.want_counts && ld_flag(A.pose_hit + pose))) continue;
+        float4 T[3];
+        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
+        ObbW ob = world_obb(R.obb[link], T);
+        ob.h = mk(ob.h.x + kBoxTol, ob.h.y + kBoxTol, ob.h.z + kBoxTol);
+        const f3 ext = mk(fabsf(ob.ax[0].x) * ob.h.x + fabsf(ob.ax[1].x) * ob.h.y + fabsf(ob.ax[2].x) * ob.h.z,
+                          fabsf(ob.ax[0].y) * ob.h.x + fabsf(ob.ax[1].y) * ob.h.y + fabsf(ob.ax[2].y) * ob.h.z,
+                          fabsf(ob.ax[0].z) * ob.h.x + fabsf(ob.ax[1].z) * ob.h.y + fabsf(ob.ax[2].z) * ob.h.z);
+        int sp = 1;
+        if (lane == 0) fr[0] = wroot;
+        __syncwarp();
+        bool overflow = false;
+        while (sp > 0 && !overflow) {
+            const int take = min(sp, 32);
+            sp -= take;
+            uint32_t ref = lane < take ? fr[sp + lane] : kNone;
+            __syncwarp();
+            bool hl = false, hr = false;
+            uint32_t rl = kNone, rr = kNone;
+            if (ref != kNone) {
+                if (ref & kLeaf) {  // a one-primitive scene: the root itself is a leaf
+                    hl = true;
+                    rl = ref;
+                } else {
+                    Box bl, br;
+                    load_node(wn, ref, bl, br, rl, rr);
+                    hl = obb_aabb(bl, ob, ext);
+                    hr = obb_aabb(br, ob, ext);
+                }
+            }
+            const bool pl = hl && !(rl & kLeaf), pr = hr && !(rr & kLeaf);
+            const bool el = hl && (rl & kLeaf), er = hr && (rr & kLeaf);
+            const uint32_t mpl = __ballot_sync(0xffffffffu, pl), mpr = __ballot_sync(0xffffffffu, pr);
+            const int npush = __popc(mpl) + __popc(mpr);
+            if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
+                if (lane == 0) atomicOr(A.err, kErrStack);
+                break;
+            }
+            if (pl) fr[sp + __popc(mpl & lt)] = rl;
+            if (pr) fr[sp + __popc(mpl) + __popc(mpr & lt)] = rr;
+            sp += npush;
+            const uint32_t mel = __ballot_sync(0xffffffffu, el), mer = __ballot_sync(0xffffffffu, er);
+            const int nemit = __popc(mel) + __popc(mer);
+            if (nemit) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(W.cand_count, (uint32_t) nemit);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base + (uint32_t) nemit > W.cand_cap) {
+                    // slots below the capacity still get written (as blanks) so stage B
+                    // never reads an unwritten candidate
+                    overflow = true;
+                    const uint32_t pl_ = base + __popc(mel & lt), pr_ = base + __popc(mel) + __popc(mer & lt);
+                    if (el && pl_ < W.cand_cap) W.cand[pl_] = make_uint2(kNone, kNone);
+                    if (er && pr_ < W.cand_cap) W.cand[pr_] = make_uint2(kNone, kNone);
+                } else {
+                    if (el) W.cand[base + __popc(mel & lt)] = make_uint2(it, rl & ~kLeaf);
+                    if (er) W.cand[base + __popc(mel) + __popc(mer & lt)] = make_uint2(it, rr & ~kLeaf);
+                }
+            }
+            __syncwarp();
+        }
+        if (overflow && lane == 0) {
+            W.item_overflow[it] = 1;
+            W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
+        }
+    }
+}
+
+// Stage B: one lane per candidate (grid-stride, so neighbouring lanes take
+// neighbouring candidates of the same item): move the scene primitive into
+// the link frame, reject it against the link OBB, descend the link LBVH and
+// run the exact segment-triangle test at the leaves.
+template <bool R2O>
+__global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, const SceneDev S, const WaveArgs W) {
+    constexpr float kBoxTol = 2e-5f;
+    const DiscreteArgs& A = W.d;
+    const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
+    const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
+    const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
+    const uint32_t total = min(*W.cand_count, W.cand_cap);
+    uint32_t st[kStack];
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+        const uint2 cd = W.cand[c];
+        if (cd.x == kNone || W.item_overflow[cd.x]) continue;  // blank, or the fused kernel re-runs this item
+        const uint32_t item = A.items[cd.x];
+        const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
+        if (!A.want_counts && ld_flag(A.pose_hit + pose)) continue;
+        const uint32_t lroot = R2O ? R.edge_root[link] : R.tri_root[link];
+        if (lroot == kNone) continue;
+        float4 T[3];
+        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
+        const float* lo = R.obb[link];
+        const f3 oc = mk(lo[0], lo[1], lo[2]);
+        const f3 u0 = mk(lo[6], lo[7], lo[8]), u1 = mk(lo[9], lo[10], lo[11]), u2 = mk(lo[12], lo[13], lo[14]);
+        f3 c0, c1, c2 = mk(0.f, 0.f, 0.f), cn = mk(0.f, 0.f, 0.f), cinv = mk(0.f, 0.f, 0.f);
+        float cw = 0.f;
+        float blo[3], bhi[3];
+        if (R2O) {
+            const float4* t = wp + 3ull * cd.y;
+            c0 = xf_inv(T, f3of(__ldg(t)));
+            c1 = xf_inv(T, f3of(__ldg(t + 1)));
+            c2 = xf_inv(T, f3of(__ldg(t + 2)));
+            cn = cross(c1 - c0, c2 - c0);
+            cw = dot(cn, c0);
+            float rr = (lo[3] + kBoxTol) * fabsf(dot(cn, u0)) + (lo[4] + kBoxTol) * fabsf(dot(cn, u1)) +
+                       (lo[5] + kBoxTol) * fabsf(dot(cn, u2));
+            if (fabsf(dot(cn, oc) - cw) > rr) continue;
+            blo[0] = fminf(c0.x, fminf(c1.x, c2.x)) - kBoxTol; bhi[0] = fmaxf(c0.x, fmaxf(c1.x, c2.x)) + kBoxTol;
+            blo[1] = fminf(c0.y, fminf(c1.y, c2.y)) - kBoxTol; bhi[1] = fmaxf(c0.y, fmaxf(c1.y, c2.y)) + kBoxTol;
+            blo[2] = fminf(c0.z, fminf(c1.z, c2.z)) - kBoxTol; bhi[2] = fmaxf(c0.z, fmaxf(c1.z, c2.z)) + kBoxTol;
+        } else {
+            const float4* e = wp + 2ull * cd.y;
+            c0 = xf_inv(T, f3of(__ldg(e)));
+            c1 = xf_inv(T, f3of(__ldg(e + 1)));
+            const f3 d = c1 - c0;
+            cinv = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+            const f3 pr = c0 - oc;
+            const f3 po = mk(dot(pr, u0), dot(pr, u1), dot(pr, u2));
+            const f3 dd = mk(dot(d, u0), dot(d, u1), dot(d, u2));
+            Box obl;
+            obl.lo[0] = -lo[3]; obl.lo[1] = -lo[4]; obl.lo[2] = -lo[5];
+            obl.hi[0] = lo[3]; obl.hi[1] = lo[4]; obl.hi[2] = lo[5];
+            if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), obl, kBoxTol)) continue;
+        }
+        int sp = 0;
+        st[sp++] = lroot;
+        while (sp > 0) {
+            const uint32_t ref = st[--sp];
+            if (ref & kLeaf) {
+                const uint32_t li = ref & ~kLeaf;
+                f3 p, q, a, b, c;
+                if (R2O) {
+                    const float4* e = lp + 2ull * li;
+                    p = f3of(__ldg(e)); q = f3of(__ldg(e + 1));
+                    a = c0; b = c1; c = c2;
+                } else {
+                    const float4* t = lp + 3ull * li;
+                    p = c0; q = c1;
+                    a = f3of(__ldg(t)); b = f3of(__ldg(t + 1)); c = f3of(__ldg(t + 2));
+                }
+                int r = seg_tri_f32(p, q, a, b, c);
+                if (r == 2) {
+                    atomicAdd(A.stats, 1ull);
+                    r = retest_f64<R2O>(T, lp, li, wp, cd.y) ? 1 : 0;
+                }
+                if (r == 1) {
+                    if (!A.want_counts) {
+                        atomicExch(A.pose_hit + pose, 1u);
+                        break;
+                    }
+                    A.pose_hit[pose] = 1u;
+                    if (R2O) {
+                        const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
+                        atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
+                    } else {
+                        atomicAdd(A.counts + pose, 1u);
+                    }
+                }
+                continue;
+            }
+            Box bl, br;
+            uint32_t rl, rr;
+            load_node(ln, ref, bl, br, rl, rr);
+            bool hr, hl;
+            if (R2O) {
+                hr = box_overlap(br, blo, bhi) && plane_box(cn, cw, br, kBoxTol);
+                hl = box_overlap(bl, blo, bhi) && plane_box(cn, cw, bl, kBoxTol);
+            } else {
+                hr = seg_box(c0, cinv, br, kBoxTol);
+                hl = seg_box(c0, cinv, bl, kBoxTol);
+            }
+            if (sp + 2 > kStack) {
+                atomicOr(A.err, kErrStack);
+                break;
+            }
+            if (hr) st[sp++] = rr;
+            if (hl) st[sp++] = rl;
+        }
+    }
+}
+
+template <class K>
+static uint32_t grid_for(K kernel, int threads) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
+}
+
+uint32_t stage_a_blocks(bool r2o) {
+    return r2o ? grid_for(k_stage_a<true>, kStageAWarps * 32) : grid_for(k_stage_a<false>, kStageAWarps * 32);
+}
+uint32_t stage_b_blocks(bool r2o) {
+    return r2o ? grid_for(k_stage_b<true>, kTravThreads) : grid_for(k_stage_b<false>, kTravThreads);
+}
+
+void launch_stage_a(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                    cudaStream_t s) {
+    if (r2o)
+        k_stage_a<true><<<blocks, kStageAWarps * 32, 0, s>>>(R, S, W);
+    else
+        k_stage_a<false><<<blocks, kStageAWarps * 32, 0, s>>>(R, S, W);
+    cuda_check(cudaGetLastError(), "k_stage_a");
+}
+
+void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                    cudaStream_t s) {
+    if (r2o)
+        k_stage_b<true><<<blocks, kTravThreads, 0, s>>>(R, S, W);
+    else
+        k_stage_b<false><<<blocks, kTravThreads, 0, s>>>(R, S, W);
+    cuda_check(cudaGetLastError(), "k_stage_b");
 }
 
 uint32_t discrete_persistent_blocks(bool robot_to_obs) {

@@ -269,9 +269,30 @@ __device__ T seg_quad2(V3<T> p, V3<T> q, V3<T> B0, V3<T> B1, V3<T> B2, int iters
     return best;
 }
 
+// Out of line: the root finding keeps many registers live, the traversal
+// loop should not pay for them.
+__device__ __noinline__ float seg_quad_dist_f32(float4 ea, float4 eb, float4 P0, float4 P1, float4 P2) {
+    return sqrtf(fmaxf(seg_quad2<float>(v3cast<float>(ea), v3cast<float>(eb), v3cast<float>(P0), v3cast<float>(P1),
+                                        v3cast<float>(P2), 12),
+                       0.f));
+}
+
+// FP64 decision for a pair whose FP32 distance lies within the band around r.
+template <bool QUAD>
+__device__ __noinline__ bool sweep_retest_f64(float4 ea, float4 eb, float4 P0, float4 P1, float4 P2, float r) {
+    double dd2;
+    if (!QUAD)
+        dd2 = seg_seg2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0), v3cast<double>(P1));
+    else
+        dd2 = seg_quad2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0), v3cast<double>(P1),
+                                v3cast<double>(P2), 48);
+    return dd2 <= (double) r * (double) r;
+}
+
 // ---------------------------------------------------------------- traversal
 __device__ __forceinline__ uint32_t ldflag(const uint32_t* p) { return __ldcg(p); }
 
+template <bool QUAD>
 __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const SweepArgs A) {
     const uint32_t* __restrict__ piece_traj = A.piece_traj;
     constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
@@ -305,7 +326,7 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
                 continue;
             uint32_t piece = piece_g - A.traj_piece_off[traj];
             uint32_t w0 = A.traj_wp_off[traj], nwp = A.traj_wp_off[traj + 1] - w0;
-            if (!A.quad) {
+            if (!QUAD) {
                 P0 = A.centers[(size_t) (w0 + piece) * A.n_spheres + s];
                 P1 = A.centers[(size_t) (w0 + piece + 1) * A.n_spheres + s];
                 P2 = P1;
@@ -345,23 +366,25 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
             const float4* e = ep + 2ull * (ref & ~kLeaf);
             float4 ea = __ldg(e), eb = __ldg(e + 1);
             V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
-            float d2;
-            if (!A.quad)
-                d2 = seg_seg2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1));
-            else
-                d2 = seg_quad2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1), v3cast<float>(P2), 12);
-            float dist = sqrtf(fmaxf(d2, 0.f));
+            float dist;
+            if (!QUAD) {
+                dist = sqrtf(fmaxf(seg_seg2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1)), 0.f));
+            } else {
+                // C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
+                // within e of the chord B0-B2 and back, so the chord distance +- e
+                // brackets the exact distance; only the undecided middle needs roots
+                V3<float> b0 = v3cast<float>(P0), b1 = v3cast<float>(P1), b2 = v3cast<float>(P2);
+                V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
+                float e = 0.5f * sqrtf(vdot(dv, dv));
+                float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
+                if (dc - e > r + kBand + 1e-6f * r) continue;       // certain miss
+                if (dc + e < r - kBand - 1e-6f * r) dist = dc + e;  // certain hit
+                else dist = seg_quad_dist_f32(ea, eb, P0, P1, P2);
+            }
             bool hit = dist <= r;
             if (fabsf(dist - r) <= kBand + 1e-6f * r) {
                 atomicAdd(A.stats, 1ull);
-                double dd2;
-                if (!A.quad)
-                    dd2 = seg_seg2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0),
-                                           v3cast<double>(P1));
-                else
-                    dd2 = seg_quad2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(P0),
-                                            v3cast<double>(P1), v3cast<double>(P2), 48);
-                hit = dd2 <= (double) r * (double) r;
+                hit = sweep_retest_f64<QUAD>(ea, eb, P0, P1, P2, r);
             }
             if (hit) {
                 if (A.want_pieces) atomicExch(A.piece_hit + piece_g, 1u);
@@ -388,14 +411,20 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
     }
 }
 
-uint32_t sweep_persistent_blocks() {
+uint32_t sweep_persistent_blocks(bool quad) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep, kTravThreads, 0);
+    if (quad)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<true>, kTravThreads, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<false>, kTravThreads, 0);
     return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
 }
 
 void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, cudaStream_t s) {
-    k_sweep<<<blocks, kTravThreads, 0, s>>>(S, A);
+    if (A.quad)
+        k_sweep<true><<<blocks, kTravThreads, 0, s>>>(S, A);
+    else
+        k_sweep<false><<<blocks, kTravThreads, 0, s>>>(S, A);
     cuda_check(cudaGetLastError(), "k_sweep");
 }
 

@@ -26,6 +26,7 @@ CHECK_NO_CULL = 1 << 2
 CHECK_PLAIN = 1 << 3
 CHECK_NO_ENDPOINTS = 1 << 4
 CHECK_TIMING = 1 << 5
+CHECK_FUSED = 1 << 6
 
 STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
           4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}
@@ -33,7 +34,9 @@ STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: '
 EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_context_destroy', 'rtcd_robot_create',
            'rtcd_robot_destroy', 'rtcd_scene_create', 'rtcd_scene_destroy', 'rtcd_scene_info', 'rtcd_detector_create',
            'rtcd_detector_destroy', 'rtcd_check', 'rtcd_sync', 'rtcd_segment_offsets', 'rtcd_last_stats',
-           'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build']
+           'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
+           'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
+           'rtcd_server_get_stats', 'rtcd_server_reset_stats']
 
 
 class RTCDError(RuntimeError):
@@ -375,3 +378,81 @@ class CollisionDetector:
 
     def clearResult(self):
         self.result = None
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [('slots', C.c_uint32), ('max_batch_units', C.c_uint32), ('memory_budget', C.c_uint64),
+                ('reserved', C.c_uint32 * 4)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [('submitted', C.c_uint64), ('completed', C.c_uint64), ('failed', C.c_uint64),
+                ('units_completed', C.c_uint64), ('batches', C.c_uint64), ('inflight_bytes_peak', C.c_uint64),
+                ('queue_depth', C.c_uint32), ('reserved0', C.c_uint32), ('p50_ms', C.c_double),
+                ('p99_ms', C.c_double), ('mean_ms', C.c_double), ('max_ms', C.c_double),
+                ('reserved', C.c_uint64 * 4)]
+
+
+class Server:
+    """Continuous-batching request server (rtcd_server_*): submit from any
+    thread, wait for tickets; requests for the same detector are merged into
+    shared launches across ``slots`` concurrent streams."""
+
+    def __init__(self, ctx, slots=4, max_batch_units=65536, memory_budget=0):
+        cfg = ServerConfig()
+        cfg.slots, cfg.max_batch_units, cfg.memory_budget = slots, max_batch_units, memory_budget
+        self.ctx = ctx
+        self.h = VP()
+        _ok(lib().rtcd_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
+        self._meta = {}
+
+    def submit(self, det, q, traj_off=None, counts=False, endpoints=True):
+        q = _arr(q, np.float32)
+        flags = (CHECK_COUNTS if counts else 0) | (0 if endpoints else CHECK_NO_ENDPOINTS)
+        if det.sweep:
+            traj_off = _arr(traj_off, np.uint32)
+            n = len(traj_off) - 1
+            segs = int(segment_offsets(det.kind, traj_off, flags)[-1])
+        else:
+            n, segs = len(q), 0
+        t = C.c_uint64()
+        _ok(lib().rtcd_server_submit(self.h, det.h, _ptr(q, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
+                                     C.c_uint32(flags), C.byref(t)))
+        self._meta[t.value] = (n, segs, counts)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        n, segs, counts = self._meta[ticket]
+        out = {'flags': np.zeros(max(n, 1), np.uint8)}
+        seg = np.zeros(max(segs, 1), np.uint8) if segs else None
+        cnt = np.zeros(max(n, 1), np.uint32) if counts else None
+        lat = C.c_double()
+        _ok(lib().rtcd_server_wait(self.h, C.c_uint64(ticket), C.c_int32(timeout_ms), _ptr(out['flags'], C.c_uint8),
+                                   _ptr(seg, C.c_uint8), _ptr(cnt, C.c_uint32), C.byref(lat)))
+        del self._meta[ticket]
+        out['flags'] = out['flags'][:n]
+        if seg is not None:
+            out['seg_flags'] = seg[:segs]
+        if cnt is not None:
+            out['counts'] = cnt[:n]
+        out['latency_ms'] = lat.value
+        return out
+
+    def stats(self):
+        s = ServerStats()
+        _ok(lib().rtcd_server_get_stats(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_ if not k.startswith('reserved')}
+
+    def reset_stats(self):
+        _ok(lib().rtcd_server_reset_stats(self.h))
+
+    def close(self):
+        if self.h:
+            lib().rtcd_server_destroy(self.h)
+            self.h = VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,100 @@
+"""The continuous-batching server: requests of mixed kinds, sizes and scenes
+submitted concurrently from several threads; every result must equal the
+result of the same request checked alone (flags, segment flags, counts)."""
+import threading
+
+import numpy as np
+import pytest
+
+from rtcollisiondetection_b200 import rtcd, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def world(ctx, panda):
+    sph = scenes.synth_spheres(panda)
+    robot = rtcd.Robot(ctx, panda, spheres=sph)
+    small = rtcd.Scene.from_mesh(ctx, scenes.discrete_small())
+    sweep = rtcd.Scene.from_mesh(ctx, scenes.sweep_scene())
+    dets = {
+        'r2o_small': rtcd.Detector(ctx, 'RobotToObs', robot, small),
+        'o2r_small': rtcd.Detector(ctx, 'ObsToRobot', robot, small),
+        'r2o_sweep': rtcd.Detector(ctx, 'RobotToObs', robot, sweep),
+        'lin': rtcd.Detector(ctx, 'Linear', robot, sweep),
+        'quad': rtcd.Detector(ctx, 'Quadratic', robot, sweep),
+    }
+    return robot, dets
+
+
+def _requests(panda, n_req, seed):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n_req):
+        kind = ['r2o_small', 'o2r_small', 'r2o_sweep', 'lin', 'quad'][i % 5]
+        counts = bool(rng.integers(0, 2))
+        if kind in ('lin', 'quad'):
+            nt = int(np.exp(rng.uniform(0, np.log(48))))
+            wp = scenes.log_uniform_counts(nt, 8, 40, seed=seed * 1000 + i)
+            q, off = scenes.random_walk_trajectories(panda, nt, wp, seed=seed * 1000 + i)
+        else:
+            n = int(np.exp(rng.uniform(0, np.log(700))))
+            q, off = scenes.uniform_poses(panda, n, seed=seed * 1000 + i), None
+        reqs.append((kind, q, off, counts))
+    return reqs
+
+
+def test_server_results_equal_alone(world, panda):
+    _, dets = world
+    server = rtcd.Server(dets['lin'].ctx, slots=3, max_batch_units=4096)
+    reqs = _requests(panda, 60, seed=3)
+    tickets = [None] * len(reqs)
+
+    def submitter(idx):
+        for i in idx:
+            kind, q, off, counts = reqs[i]
+            tickets[i] = server.submit(dets[kind], q, off, counts=counts)
+
+    threads = [threading.Thread(target=submitter, args=(range(k, len(reqs), 3),)) for k in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    results = [server.wait(t, timeout_ms=120000) for t in tickets]
+    st = server.stats()
+    server.close()
+    assert st['completed'] == len(reqs) and st['failed'] == 0
+    assert st['batches'] <= len(reqs)
+    assert st['p99_ms'] >= st['p50_ms'] > 0
+    for (kind, q, off, counts), got in zip(reqs, results):
+        det = dets[kind]
+        alone = det.check(q, off, counts=counts, segments=det.sweep)
+        assert np.array_equal(got['flags'], alone['flags']), kind
+        if counts:
+            assert np.array_equal(got['counts'], alone['counts']), kind
+        if det.sweep:
+            assert np.array_equal(got['seg_flags'], alone['seg_flags']), kind
+
+
+def test_server_merges_queued_requests(world, panda):
+    _, dets = world
+    server = rtcd.Server(dets['r2o_small'].ctx, slots=1, max_batch_units=65536)
+    qs = [scenes.uniform_poses(panda, 50, seed=100 + i) for i in range(40)]
+    tickets = [server.submit(dets['r2o_small'], q) for q in qs]
+    outs = [server.wait(t) for t in tickets]
+    st = server.stats()
+    server.close()
+    assert st['batches'] < len(qs)           # queued requests shared launches
+    whole = dets['r2o_small'].check(np.concatenate(qs))['flags']
+    assert np.array_equal(np.concatenate([o['flags'] for o in outs]), whole)
+
+
+def test_server_rejects_bad_requests(world, panda):
+    _, dets = world
+    server = rtcd.Server(dets['lin'].ctx, slots=1)
+    with pytest.raises(rtcd.RTCDError):
+        server.submit(dets['lin'], np.zeros((4, 7), np.float32), np.array([0, 3, 1], np.uint32))
+    with pytest.raises(rtcd.RTCDError):
+        rtcd._ok(rtcd.lib().rtcd_server_wait(server.h, rtcd.C.c_uint64(12345), rtcd.C.c_int32(0), None, None, None,
+                                             None))
+    server.close()
