@@ -168,6 +168,105 @@ def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512):
             'collision_rate': float(ref['traj_hit'].mean())}
 
 
+def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0):
+    """Mixed request stream against three resident scenes (5k, 50k, ~500k
+    triangles): Poisson arrivals at `rate` req/s for `seconds`; half discrete
+    RobotToObs batches of log-uniform[1, 4096] poses, half continuous batches
+    (linear / quadratic alternately) of log-uniform[1, 1024] trajectories with
+    log-uniform[8, 128] waypoints.  Requests go to the continuous-batching
+    server from a submitter thread at their arrival times; latency is submit
+    to result.  The same arrivals (first `plain_seconds`) are then replayed on
+    the plain form - one request at a time, each a frame-by-frame check with a
+    host round trip per frame - for comparison."""
+    import threading
+    from rtcollisiondetection_b200 import rtcd, scenes
+    model = scenes.load_panda()
+    sph = scenes.synth_spheres(model)
+    robot = rtcd.Robot(ctx, model, spheres=sph)
+    meshes = [scenes.discrete_small(), scenes.sweep_scene(), scenes.served_large_scene()]
+    scn = [rtcd.Scene.from_mesh(ctx, m) for m in meshes]
+    dets = [{k: rtcd.Detector(ctx, k, robot, s) for k in ('RobotToObs', 'Linear', 'Quadratic')} for s in scn]
+    rng = np.random.default_rng(seed)
+    n_req = int(rate * seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    pose_pool = scenes.uniform_poses(model, 1 << 17, seed=seed + 1)
+    traj_q, traj_off = scenes.random_walk_trajectories(model, 2048, scenes.log_uniform_counts(2048, 8, 128, seed=seed + 2),
+                                                       seed=seed + 3)
+    reqs = []
+    for i in range(n_req):
+        s = int(rng.integers(0, 3))
+        if rng.random() < 0.5:
+            n = int(np.rint(np.exp(rng.uniform(0, np.log(4096)))))
+            a = int(rng.integers(0, len(pose_pool) - n))
+            reqs.append((dets[s]['RobotToObs'], pose_pool[a:a + n], None, n))
+        else:
+            k = 'Linear' if rng.random() < 0.5 else 'Quadratic'
+            nt = int(np.rint(np.exp(rng.uniform(0, np.log(1024)))))
+            t0 = int(rng.integers(0, 2048 - nt + 1))
+            off = traj_off[t0:t0 + nt + 1] - traj_off[t0]
+            reqs.append((dets[s][k], traj_q[traj_off[t0]:traj_off[t0 + nt]], off, nt))
+
+    def run_server():
+        server = rtcd.Server(ctx, slots=slots)
+        for d in dets:              # first-touch of every clone outside the measured window
+            for det in d.values():
+                t = server.submit(det, pose_pool[:8] if not det.sweep else traj_q[:traj_off[2]],
+                                  None if not det.sweep else traj_off[:3])
+                server.wait(t)
+        server.reset_stats()
+        tickets = [None] * n_req
+        lat = np.zeros(n_req)
+        start = time.perf_counter()
+
+        def submitter():
+            for i, (det, q, off, n) in enumerate(reqs):
+                delay = arrivals[i] - (time.perf_counter() - start)
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = server.submit(det, q, off)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        for i in range(n_req):
+            while tickets[i] is None:
+                time.sleep(0.0002)
+            lat[i] = server.wait(tickets[i])['latency_ms']
+        th.join()
+        wall = time.perf_counter() - start
+        st = server.stats()
+        server.close()
+        return lat, wall, st
+
+    lat, wall, st = run_server()
+    disc = np.array([r[2] is None for r in reqs])
+    sizes = np.array([r[3] for r in reqs])
+    poses = int(sizes[disc].sum())
+    trajs = int(sizes[~disc].sum())
+    out = {'seconds': seconds, 'rate_req_s': rate, 'requests': n_req, 'slots': slots, 'wall_s': wall,
+           'p50_ms_discrete_le4096': float(np.percentile(lat[disc], 50)),
+           'p99_ms_discrete_le4096': float(np.percentile(lat[disc], 99)),
+           'p50_ms_all': float(np.percentile(lat, 50)), 'p99_ms_all': float(np.percentile(lat, 99)),
+           'poses_per_s': poses / wall, 'trajectories_per_s': trajs / wall, 'batches': st['batches'],
+           'scenes_tris': [m.n_tris for m in meshes]}
+    # plain: the same arrivals, one request at a time through the frame-by-frame path
+    m = int(rate * plain_seconds)
+    plat = np.zeros(m)
+    start = time.perf_counter()
+    for i in range(m):
+        det, q, off, n = reqs[i]
+        delay = arrivals[i] - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        det.check(q, off, flags=0 if det.sweep else rtcd.CHECK_PLAIN)
+        plat[i] = (time.perf_counter() - start - arrivals[i]) * 1e3
+    pwall = time.perf_counter() - start
+    pd = disc[:m]
+    out['plain'] = {'requests': m, 'wall_s': pwall, 'p50_ms_discrete_le4096': float(np.percentile(plat[pd], 50)),
+                    'p99_ms_discrete_le4096': float(np.percentile(plat[pd], 99)),
+                    'poses_per_s': float(sizes[:m][pd].sum() / pwall)}
+    return out
+
+
 def run_reference(args, cfg, rank, world):
     from rtcollisiondetection_b200 import scenes
     if rank != 0:
@@ -225,6 +324,8 @@ def main():
     ap.add_argument('--ref-sample', type=int, default=8192)
     ap.add_argument('--plain-frame', type=int, default=64)
     ap.add_argument('--fused', action='store_true', help='discrete: the single fused traversal kernel')
+    ap.add_argument('--serve-seconds', type=float, default=5.0,
+                    help='length of the served mixed stream reported under "served" (0: skip)')
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     rank = int(os.environ.get('RANK', 0))
@@ -363,6 +464,8 @@ def main():
     if not args.no_check and rank == 0:
         line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags)
         line['fp64_retests'] = st['fp64_retests']
+    if args.serve_seconds > 0 and rank == 0 and args.config == 'c2':
+        line['served'] = served_stream(ctx, args.serve_seconds)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         line['cpu_baseline'] = cpu_baseline(cfg, model, mesh, spheres, q, off)
     if rank == 0:

@@ -65,6 +65,8 @@ typedef enum {
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
 #define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
 #define RTCD_CHECK_FUSED (1u << 6)         /* discrete: one fused traversal kernel instead of the two-stage wavefront */
+#define RTCD_CHECK_GRAPH (1u << 7)         /* discrete, device buffers: replay the launch sequence as a CUDA graph
+                                              (captured on the first call with these pointers, sizes and flags) */
 
 typedef struct rtcd_ctx rtcd_ctx;
 typedef struct rtcd_robot rtcd_robot;
@@ -95,8 +97,10 @@ typedef struct {
 } rtcd_robot_desc;
 
 typedef struct {
-    uint32_t frame_size; /* poses (or trajectories) per frame of the plain path; 0 = 64 */
-    uint32_t reserved[7];
+    uint32_t frame_size;             /* poses per frame of the plain path; 0 = 64 */
+    uint32_t traverse_threads;       /* threads per block of the traversal kernel: 64, 128 or 256; 0 = 128 */
+    uint32_t traverse_blocks_per_sm; /* resident traversal blocks per SM; 0 = as many as fit */
+    uint32_t reserved[5];
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -158,6 +162,16 @@ RTCD_API rtcd_status rtcd_check(rtcd_detector* det, const float* q, const uint32
  * (upstream final CUDA_SYNC_CHECK, CollisionDetector.h:470). */
 RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
 
+/* Autotuner: runs the given device-resident batch (q_dev; traj_offsets on the
+ * host for sweeps) with every traversal launch shape - 64, 128 and 256
+ * threads per block, each at a quarter, half and all of the blocks per SM
+ * that fit - times the traversal kernel with device events (median of
+ * three after a warm-up run), keeps the fastest shape in the detector and
+ * writes it to best_out (optional).  The upstream picks its batch size per
+ * experiment by hand (CollisionDetector.h:365-394). */
+RTCD_API rtcd_status rtcd_detector_autotune(rtcd_detector* det, const float* q_dev, const uint32_t* traj_offsets,
+                                            uint32_t n, void* stream, rtcd_config* best_out, float* best_ms);
+
 /* Segments per trajectory for the sweep kinds: linear n_wp - 1; quadratic
  * max(3, ceil(n_wp/2)) - 2 (+2 start/end spheres unless RTCD_CHECK_NO_ENDPOINTS).
  * offsets_out (n + 1 entries, host) is the exclusive prefix sum. */
@@ -173,7 +187,10 @@ typedef struct {
     float ms_cull;         /* OBB prefilter + compaction (discrete) */
     float ms_traverse;     /* the traversal kernel */
     float ms_total;        /* whole check on the device */
-    uint64_t reserved[3];
+    uint64_t candidates;   /* discrete: (item, scene primitive) candidates of the scene stage;
+                              quadratic sweep: pairs that needed the root finding */
+    uint64_t exact_tests;  /* primitive-pair tests run in FP32 */
+    uint64_t skipped;      /* candidates dropped because their pose (trajectory) was already decided */
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 

@@ -268,11 +268,16 @@ struct rtcd_detector {
     cudaEvent_t ev_end = nullptr;
     bool timed = false;
     cudaStream_t last_stream = nullptr;  // stream of the last check (stats read on it)
+    cudaGraph_t graph = nullptr;         // captured launch sequence (RTCD_CHECK_GRAPH)
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    bool timed_total_only = false;       // the last check timed only ev[0] -> ev_end (graph path)
     uint32_t blocks = 0;
     // discrete workspace
     DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
     DevBuf cand, item_overflow, overflow_items, wave_counts;  // wavefront traversal
     uint32_t blocks_a = 0, blocks_b = 0;
+    uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
     ScanScratch scan;
     // sweep workspace
     DevBuf centers, ctrl, aux, piece_hit, W, W_off;
@@ -316,6 +321,22 @@ static rtcd_status guarded(F&& f) {
     do {                        \
         if (!(cond)) fail(RTCD_ERR_INVALID_ARGUMENT, msg); \
     } while (0)
+
+// Traversal launch shape from the detector config: threads per block (64, 128
+// or 256) and resident blocks per SM (0 or more than fit: as many as fit).
+static void apply_launch_shape(rtcd_detector* d) {
+    uint32_t t = d->cfg.traverse_threads ? d->cfg.traverse_threads : 128;
+    if (t != 64 && t != 128 && t != 256) fail(RTCD_ERR_INVALID_ARGUMENT, "traverse_threads must be 64, 128 or 256");
+    const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
+    uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
+                            : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
+    uint32_t per_sm = d->cfg.traverse_blocks_per_sm ? std::min(d->cfg.traverse_blocks_per_sm, fit) : fit;
+    d->threads = t;
+    if (discrete)
+        d->blocks_b = per_sm * (uint32_t) device_sm_count();
+    else
+        d->blocks = per_sm * (uint32_t) device_sm_count();
+}
 
 struct DeviceScope {
     int prev = 0;
@@ -592,10 +613,8 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS) {
             d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
             d->blocks_a = stage_a_blocks(kind == RTCD_ROBOT_TO_OBS);
-            d->blocks_b = stage_b_blocks(kind == RTCD_ROBOT_TO_OBS);
-        } else {
-            d->blocks = sweep_persistent_blocks(kind == RTCD_QUAD_SWEEP);
         }
+        apply_launch_shape(d.get());
         d->err.ensure(4);
         d->stats.ensure(8 * 8);
         d->work.ensure(4);
@@ -629,6 +648,8 @@ rtcd_status rtcd_detector_destroy(rtcd_detector* d) {
         if (!d) return;
         DeviceScope ds(d->ctx->device);
         cudaStreamSynchronize(d->stream);
+        if (d->graph_exec) cudaGraphExecDestroy(d->graph_exec);
+        if (d->graph) cudaGraphDestroy(d->graph);
         cudaEventDestroy(d->staged);
         for (auto& e : d->ev) cudaEventDestroy(e);
         cudaEventDestroy(d->ev_end);
@@ -800,7 +821,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         W.overflow_count = wc + 1;
         uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
-        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, s);
+        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, s);
         DiscreteArgs F = A;
         F.items = d->overflow_items.as<uint32_t>();
         F.n_items = wc + 1;
@@ -983,7 +1004,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         cuda_check(cudaEventRecord(d->ev[1], s), "event");
         cuda_check(cudaEventRecord(d->ev[2], s), "event");
     }
-    if (A.total_units) launch_sweep(d->scene->dev, A, d->blocks, s);
+    if (A.total_units) launch_sweep(d->scene->dev, A, d->blocks, d->threads, s);
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     // outputs
     uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
@@ -1025,8 +1046,58 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
         DeviceScope ds(d->ctx->device);
         cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
         d->timed = false;
+        d->timed_total_only = false;
         d->last_stream = s;
+        if (n) cuda_check(cudaMemsetAsync(d->stats.p, 0, 64, s), "stats reset");
         if (n == 0) return;
+        if (flags & RTCD_CHECK_GRAPH) {
+            RTCD_REQUIRE(d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS,
+                         "graph replay is offered for the discrete detectors");
+            RTCD_REQUIRE(!(flags & (RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_PLAIN)) && !seg_flags_out,
+                         "graph replay needs device buffers and the batched path");
+            RTCD_REQUIRE(flags_out, "graph replay needs a device flags buffer");
+            // events recorded inside a graph cannot be timed: a replay is timed as a whole
+            const bool want_time = (flags & RTCD_CHECK_TIMING) != 0;
+            const uint32_t f = flags & ~(RTCD_CHECK_GRAPH | RTCD_CHECK_TIMING);
+            const uint64_t key[6] = {(uint64_t) q, n, (uint64_t) flags_out, (uint64_t) counts_out, f, (uint64_t) s};
+            if (d->graph_exec && std::equal(key, key + 6, d->graph_key)) {
+                if (want_time) cuda_check(cudaEventRecord(d->ev[0], s), "event");
+                cuda_check(cudaGraphLaunch(d->graph_exec, s), "cudaGraphLaunch");
+                if (want_time) cuda_check(cudaEventRecord(d->ev_end, s), "event");
+                d->timed_total_only = want_time;
+                return;
+            }
+            // run once normally (this also sizes every workspace), then capture the
+            // same sequence - which now allocates nothing - for the next calls
+            if (want_time) cuda_check(cudaEventRecord(d->ev[0], s), "event");
+            check_discrete(d, q, n, flags_out, counts_out, f, s);
+            if (want_time) cuda_check(cudaEventRecord(d->ev_end, s), "event");
+            d->timed_total_only = want_time;
+            if (d->graph_exec) cudaGraphExecDestroy(d->graph_exec);
+            if (d->graph) cudaGraphDestroy(d->graph);
+            d->graph_exec = nullptr;
+            d->graph = nullptr;
+            cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+            try {
+                check_discrete(d, q, n, flags_out, counts_out, f, s);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            cuda_check(cudaStreamEndCapture(s, &d->graph), "cudaStreamEndCapture");
+            cuda_check(cudaGraphInstantiate(&d->graph_exec, d->graph, 0), "cudaGraphInstantiate");
+            std::copy(key, key + 6, d->graph_key);
+            return;
+        }
+        if (d->graph_exec) {  // this call may grow (move) workspaces the graph points into
+            cuda_check(cudaStreamSynchronize(s), "graph retire");
+            cudaGraphExecDestroy(d->graph_exec);
+            cudaGraphDestroy(d->graph);
+            d->graph_exec = nullptr;
+            d->graph = nullptr;
+        }
         if (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) {
             RTCD_REQUIRE(!seg_flags_out, "segment flags exist only for sweep detectors");
             check_discrete(d, q, n, flags_out, counts_out, flags, s);
@@ -1073,16 +1144,72 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
         cudaStream_t s = d->last_stream ? d->last_stream : d->stream;
         cuda_check(cudaMemcpyAsync(st, d->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, s), "stats");
+        uint32_t cand = 0;
+        if (d->wave_counts.p)
+            cuda_check(cudaMemcpyAsync(&cand, d->wave_counts.p, 4, cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaStreamSynchronize(s), "stats sync");
         out->fp64_retests = st[0];
+        out->candidates = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) ? cand : st[5];
+        out->exact_tests = st[4];
+        out->skipped = st[2];
         if (d->timed) {
             cuda_check(cudaEventElapsedTime(&out->ms_prepare, d->ev[0], d->ev[1]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_cull, d->ev[1], d->ev[2]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_traverse, d->ev[2], d->ev[3]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_total, d->ev[0], d->ev_end), "elapsed");
+        } else if (d->timed_total_only) {
+            cuda_check(cudaEventElapsedTime(&out->ms_total, d->ev[0], d->ev_end), "elapsed");
         }
         out->work_items = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) && !d->last_items ? cnt
                                                                                                           : d->last_items;
+    });
+}
+
+rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const uint32_t* traj_offsets, uint32_t n,
+                                   void* stream, rtcd_config* best_out, float* best_ms) {
+    return guarded([&] {
+        RTCD_REQUIRE(d && q_dev && n, "NULL argument");
+        DeviceScope ds(d->ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
+        const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
+        DevBuf flags;
+        flags.ensure(n);
+        const rtcd_config saved = d->cfg;
+        rtcd_config best = saved;
+        float best_t = 3.0e38f;
+        for (uint32_t t : {64u, 128u, 256u}) {
+            uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
+                                    : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
+            std::vector<uint32_t> shapes = {std::max(1u, fit / 4), std::max(1u, fit / 2), fit};
+            shapes.erase(std::unique(shapes.begin(), shapes.end()), shapes.end());
+            for (uint32_t per_sm : shapes) {
+                d->cfg.traverse_threads = t;
+                d->cfg.traverse_blocks_per_sm = per_sm;
+                apply_launch_shape(d);
+                float ms[4];
+                for (int rep = 0; rep < 4; ++rep) {
+                    rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(), nullptr, nullptr,
+                                                RTCD_CHECK_TIMING, s);
+                    rtcd_stats stt;
+                    if (st == RTCD_OK) st = rtcd_last_stats(d, &stt);
+                    if (st != RTCD_OK) {
+                        d->cfg = saved;
+                        apply_launch_shape(d);
+                        fail(st, g_last_error);
+                    }
+                    ms[rep] = stt.ms_traverse;
+                }
+                std::sort(ms + 1, ms + 4);
+                if (ms[2] < best_t) {
+                    best_t = ms[2];
+                    best = d->cfg;
+                }
+            }
+        }
+        d->cfg = best;
+        apply_launch_shape(d);
+        if (best_out) *best_out = best;
+        if (best_ms) *best_ms = best_t;
     });
 }
 

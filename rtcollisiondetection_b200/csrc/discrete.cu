@@ -583,14 +583,14 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
                     if (el && pl_ < W.cand_cap) W.cand[pl_] = make_uint2(kNone, kNone);
                     if (er && pr_ < W.cand_cap) W.cand[pr_] = make_uint2(kNone, kNone);
                 } else {
-                    if (el) W.cand[base + __popc(mel & lt)] = make_uint2(it, rl & ~kLeaf);
-                    if (er) W.cand[base + __popc(mel) + __popc(mer & lt)] = make_uint2(it, rr & ~kLeaf);
+                    if (el) W.cand[base + __popc(mel & lt)] = make_uint2(item, rl & ~kLeaf);
+                    if (er) W.cand[base + __popc(mel) + __popc(mer & lt)] = make_uint2(item, rr & ~kLeaf);
                 }
             }
             __syncwarp();
         }
         if (overflow && lane == 0) {
-            W.item_overflow[it] = 1;
+            W.item_overflow[item] = 1;
             W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
         }
     }
@@ -599,9 +599,11 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
 // Stage B: one lane per candidate (grid-stride, so neighbouring lanes take
 // neighbouring candidates of the same item): move the scene primitive into
 // the link frame, reject it against the link OBB, descend the link LBVH and
-// run the exact segment-triangle test at the leaves.
-template <bool R2O>
-__global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, const SceneDev S, const WaveArgs W) {
+// run the exact segment-triangle test at the leaves.  A candidate carries its
+// (pose, link) item word, so one whose pose is already decided costs two
+// loads.
+template <bool R2O, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const SceneDev S, const WaveArgs W) {
     constexpr float kBoxTol = 2e-5f;
     const DiscreteArgs& A = W.d;
     const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
@@ -609,12 +611,17 @@ __global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, cons
     const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
     const uint32_t total = min(*W.cand_count, W.cand_cap);
     uint32_t st[kStack];
+    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
         const uint2 cd = W.cand[c];
-        if (cd.x == kNone || W.item_overflow[cd.x]) continue;  // blank, or the fused kernel re-runs this item
-        const uint32_t item = A.items[cd.x];
+        if (cd.x == kNone) continue;  // blank slot of an overflowed emission
+        const uint32_t item = cd.x;
         const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
-        if (!A.want_counts && ld_flag(A.pose_hit + pose)) continue;
+        if (!A.want_counts && ld_flag(A.pose_hit + pose)) {
+            ++n_skip;
+            continue;
+        }
+        if (W.item_overflow[item]) continue;  // the fused kernel re-runs this item
         const uint32_t lroot = R2O ? R.edge_root[link] : R.tri_root[link];
         if (lroot == kNone) continue;
         float4 T[3];
@@ -635,7 +642,10 @@ __global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, cons
             cw = dot(cn, c0);
             float rr = (lo[3] + kBoxTol) * fabsf(dot(cn, u0)) + (lo[4] + kBoxTol) * fabsf(dot(cn, u1)) +
                        (lo[5] + kBoxTol) * fabsf(dot(cn, u2));
-            if (fabsf(dot(cn, oc) - cw) > rr) continue;
+            if (fabsf(dot(cn, oc) - cw) > rr) {
+                ++n_rej;
+                continue;
+            }
             blo[0] = fminf(c0.x, fminf(c1.x, c2.x)) - kBoxTol; bhi[0] = fmaxf(c0.x, fmaxf(c1.x, c2.x)) + kBoxTol;
             blo[1] = fminf(c0.y, fminf(c1.y, c2.y)) - kBoxTol; bhi[1] = fmaxf(c0.y, fmaxf(c1.y, c2.y)) + kBoxTol;
             blo[2] = fminf(c0.z, fminf(c1.z, c2.z)) - kBoxTol; bhi[2] = fmaxf(c0.z, fmaxf(c1.z, c2.z)) + kBoxTol;
@@ -651,13 +661,18 @@ __global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, cons
             Box obl;
             obl.lo[0] = -lo[3]; obl.lo[1] = -lo[4]; obl.lo[2] = -lo[5];
             obl.hi[0] = lo[3]; obl.hi[1] = lo[4]; obl.hi[2] = lo[5];
-            if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), obl, kBoxTol)) continue;
+            if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), obl, kBoxTol)) {
+                ++n_rej;
+                continue;
+            }
         }
+        ++n_acc;
         int sp = 0;
         st[sp++] = lroot;
         while (sp > 0) {
             const uint32_t ref = st[--sp];
             if (ref & kLeaf) {
+                ++n_leaf;
                 const uint32_t li = ref & ~kLeaf;
                 f3 p, q, a, b, c;
                 if (R2O) {
@@ -708,6 +723,10 @@ __global__ void __launch_bounds__(kTravThreads) k_stage_b(const RobotDev R, cons
             if (hl) st[sp++] = rl;
         }
     }
+    atomicAdd(A.stats + 1, n_acc);
+    atomicAdd(A.stats + 2, n_skip);
+    atomicAdd(A.stats + 3, n_rej);
+    atomicAdd(A.stats + 4, n_leaf);
 }
 
 template <class K>
@@ -720,9 +739,23 @@ static uint32_t grid_for(K kernel, int threads) {
 uint32_t stage_a_blocks(bool r2o) {
     return r2o ? grid_for(k_stage_a<true>, kStageAWarps * 32) : grid_for(k_stage_a<false>, kStageAWarps * 32);
 }
-uint32_t stage_b_blocks(bool r2o) {
-    return r2o ? grid_for(k_stage_b<true>, kTravThreads) : grid_for(k_stage_b<false>, kTravThreads);
+template <bool R2O>
+static int stage_b_per_sm(int threads) {
+    int per_sm = 0;
+    if (threads == 64)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_b<R2O, 64>, 64, 0);
+    else if (threads == 256)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_b<R2O, 256>, 256, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_b<R2O, 128>, 128, 0);
+    return std::max(1, per_sm);
 }
+
+uint32_t stage_b_max_blocks_per_sm(bool r2o, uint32_t threads) {
+    return (uint32_t) (r2o ? stage_b_per_sm<true>((int) threads) : stage_b_per_sm<false>((int) threads));
+}
+
+uint32_t stage_b_blocks(bool r2o) { return stage_b_max_blocks_per_sm(r2o, kTravThreads) * device_sm_count(); }
 
 void launch_stage_a(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                     cudaStream_t s) {
@@ -733,12 +766,23 @@ void launch_stage_a(bool r2o, const RobotDev& R, const SceneDev& S, const WaveAr
     cuda_check(cudaGetLastError(), "k_stage_a");
 }
 
-void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                    cudaStream_t s) {
-    if (r2o)
-        k_stage_b<true><<<blocks, kTravThreads, 0, s>>>(R, S, W);
+template <bool R2O>
+static void stage_b_dispatch(const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                             uint32_t threads, cudaStream_t s) {
+    if (threads == 64)
+        k_stage_b<R2O, 64><<<blocks, 64, 0, s>>>(R, S, W);
+    else if (threads == 256)
+        k_stage_b<R2O, 256><<<blocks, 256, 0, s>>>(R, S, W);
     else
-        k_stage_b<false><<<blocks, kTravThreads, 0, s>>>(R, S, W);
+        k_stage_b<R2O, 128><<<blocks, 128, 0, s>>>(R, S, W);
+}
+
+void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                    uint32_t threads, cudaStream_t s) {
+    if (r2o)
+        stage_b_dispatch<true>(R, S, W, blocks, threads, s);
+    else
+        stage_b_dispatch<false>(R, S, W, blocks, threads, s);
     cuda_check(cudaGetLastError(), "k_stage_b");
 }
 

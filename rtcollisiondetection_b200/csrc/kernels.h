@@ -60,10 +60,10 @@ constexpr int kTravThreads = 128;
 // the buffer are flagged and re-run by the fused kernel.
 struct WaveArgs {
     DiscreteArgs d;
-    uint2* cand;               // (item position, scene primitive)
+    uint2* cand;               // (item word pose * n_links + link, scene primitive)
     uint32_t* cand_count;      // zeroed before stage A; may exceed cand_cap
     uint32_t cand_cap;
-    uint8_t* item_overflow;    // [item position] set when its candidates overflowed; zeroed before stage A
+    uint8_t* item_overflow;    // [item word] set when its candidates overflowed; zeroed before stage A
     uint32_t* overflow_items;  // compacted overflowed items (item words, for the fused kernel)
     uint32_t* overflow_count;  // zeroed before stage A
 };
@@ -74,9 +74,10 @@ constexpr int kFrontier = 32 * (kStack + 2);  // bound of a 32-wide LIFO frontie
 void launch_stage_a(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                     cudaStream_t s);
 void launch_stage_b(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                    cudaStream_t s);
+                    uint32_t threads, cudaStream_t s);
 uint32_t stage_a_blocks(bool robot_to_obs);
 uint32_t stage_b_blocks(bool robot_to_obs);
+uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256
 
 void launch_fk_poses(const Chain& ch, const float* d_q, uint32_t n, float4* d_T, cudaStream_t s);
 void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, cudaStream_t s);
@@ -113,7 +114,8 @@ struct SweepArgs {
 void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s);
 void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_t* d_ctrl_off, const float* d_W,
                 const uint32_t* d_W_off, uint32_t n_traj, uint32_t n_spheres, float4* d_ctrl, cudaStream_t s);
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, cudaStream_t s);
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s);
 uint32_t sweep_persistent_blocks(bool quad);
+uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads);  // threads: 64, 128 or 256
 
 }  // namespace rtcd

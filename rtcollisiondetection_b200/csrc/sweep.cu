@@ -292,8 +292,8 @@ __device__ __noinline__ bool sweep_retest_f64(float4 ea, float4 eb, float4 P0, f
 // ---------------------------------------------------------------- traversal
 __device__ __forceinline__ uint32_t ldflag(const uint32_t* p) { return __ldcg(p); }
 
-template <bool QUAD>
-__global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const SweepArgs A) {
+template <bool QUAD, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepArgs A) {
     const uint32_t* __restrict__ piece_traj = A.piece_traj;
     constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
     const float4* __restrict__ en = S.edge_nodes;
@@ -304,16 +304,18 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
     uint32_t traj = 0, piece_g = 0;
     float4 P0 = make_float4(0, 0, 0, 0), P1 = P0, P2 = P0;  // linear: P0-P1 axis; quadratic: Bezier B0,B1,B2
     float r = 0.f;
-    float blo[3], bhi[3];
+    float blo[3] = {0.f, 0.f, 0.f}, bhi[3] = {0.f, 0.f, 0.f};
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t next = blockIdx.x * blockDim.x + threadIdx.x;  // neighbouring lanes: spheres of one piece
+    unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0;
 
+    // "While-while" (Aila and Laine 2009): lanes without a unit take their next
+    // one, every lane descends to its next leaf, then the warp's leaf tests run
+    // together.
     while (true) {
-        if (!busy) {
-            cg::coalesced_group g = cg::coalesced_threads();
-            uint32_t base = 0;
-            if (g.thread_rank() == 0) base = atomicAdd(A.work_counter, g.size());
-            base = g.shfl(base, 0);
-            uint32_t u = base + g.thread_rank();
-            if (u >= A.total_units) break;
+        while (!busy && next < A.total_units) {
+            const uint32_t u = next;
+            next += stride;
             piece_g = u / A.n_spheres;
             uint32_t s = u - piece_g * A.n_spheres;
             traj = piece_traj[piece_g];
@@ -322,8 +324,10 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
                 continue;
             }
             if (A.want_pieces ? ldflag(A.piece_hit + piece_g) && !A.want_counts
-                              : (!A.want_counts && ldflag(A.traj_hit + traj)))
+                              : (!A.want_counts && ldflag(A.traj_hit + traj))) {
+                ++n_skip;
                 continue;
+            }
             uint32_t piece = piece_g - A.traj_piece_off[traj];
             uint32_t w0 = A.traj_wp_off[traj], nwp = A.traj_wp_off[traj + 1] - w0;
             if (!QUAD) {
@@ -355,34 +359,78 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
             st[0] = S.edge_root;
             sp = 1;
             busy = true;
-            continue;
+            ++n_acc;
         }
-        if (sp == 0) {
-            busy = false;
-            continue;
+        if (!busy) break;
+        uint32_t leaf = kNone;
+        while (sp > 0) {
+            const uint32_t ref = st[--sp];
+            if (ref & kLeaf) {
+                leaf = ref & ~kLeaf;
+                break;
+            }
+            Box bl, br;
+            uint32_t rl, rr;
+            load_node(en, ref, bl, br, rl, rr);
+            bool hr = box_overlap(br, blo, bhi), hl = box_overlap(bl, blo, bhi);
+            if (sp + 2 > kStack) {
+                atomicOr(A.err, kErrStack);
+                hr = hl = false;
+                sp = 0;
+            }
+            if (hr) st[sp++] = rr;
+            if (hl) st[sp++] = rl;
         }
-        uint32_t ref = st[--sp];
-        if (ref & kLeaf) {
-            const float4* e = ep + 2ull * (ref & ~kLeaf);
-            float4 ea = __ldg(e), eb = __ldg(e + 1);
-            V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
+        if (leaf != kNone) {
+            ++n_leaf;
+            const float4* e = ep + 2ull * leaf;
+            const float4 ea = __ldg(e), eb = __ldg(e + 1);
+            const V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
             float dist;
+            bool decided = false;
             if (!QUAD) {
                 dist = sqrtf(fmaxf(seg_seg2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1)), 0.f));
             } else {
                 // C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
                 // within e of the chord B0-B2 and back, so the chord distance +- e
                 // brackets the exact distance; only the undecided middle needs roots
-                V3<float> b0 = v3cast<float>(P0), b1 = v3cast<float>(P1), b2 = v3cast<float>(P2);
-                V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
-                float e = 0.5f * sqrtf(vdot(dv, dv));
-                float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
-                if (dc - e > r + kBand + 1e-6f * r) continue;       // certain miss
-                if (dc + e < r - kBand - 1e-6f * r) dist = dc + e;  // certain hit
-                else dist = seg_quad_dist_f32(ea, eb, P0, P1, P2);
+                const V3<float> b0 = v3cast<float>(P0), b1 = v3cast<float>(P1), b2 = v3cast<float>(P2);
+                const V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
+                const float e = 0.5f * sqrtf(vdot(dv, dv));
+                const float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
+                const float tol = kBand + 1e-6f * r;
+                if (dc - e > r + tol) {  // certain miss
+                    dist = dc - e;
+                    decided = true;
+                } else if (dc + e < r - tol) {  // certain hit
+                    dist = dc + e;
+                } else {
+                    // halve the piece twice more (de Casteljau: the chord deviation of a
+                    // half is a quarter), bracketing with the polyline through C(k/4)
+                    const float e2 = 0.0625f * e;  // deviation of a quarter piece from its chord
+                    float lo = 3.0e38f;
+                    V3<float> prev = b0;
+                    for (int k = 1; k <= 4; ++k) {
+                        const float u = 0.25f * (float) k;
+                        const V3<float> cu = vadd(vadd(vscale(b0, (1.f - u) * (1.f - u)), vscale(b1, 2.f * u * (1.f - u))),
+                                                  vscale(b2, u * u));
+                        lo = fminf(lo, seg_seg2<float>(p, q, prev, cu));
+                        prev = cu;
+                    }
+                    const float dq = sqrtf(fmaxf(lo, 0.f));
+                    if (dq - e2 > r + tol) {
+                        dist = dq - e2;
+                        decided = true;
+                    } else if (dq + e2 < r - tol) {
+                        dist = dq + e2;
+                    } else {
+                        ++n_roots;
+                        dist = seg_quad_dist_f32(ea, eb, P0, P1, P2);
+                    }
+                }
             }
             bool hit = dist <= r;
-            if (fabsf(dist - r) <= kBand + 1e-6f * r) {
+            if (!decided && fabsf(dist - r) <= kBand + 1e-6f * r) {
                 atomicAdd(A.stats, 1ull);
                 hit = sweep_retest_f64<QUAD>(ea, eb, P0, P1, P2, r);
             }
@@ -393,38 +441,51 @@ __global__ void __launch_bounds__(kTravThreads) k_sweep(const SceneDev S, const 
                     atomicAdd(A.counts + traj, 1u);
                 } else {
                     atomicExch(A.traj_hit + traj, 1u);
-                    busy = false;
+                    sp = 0;  // this unit is decided
                 }
             }
-            continue;
         }
-        Box bl, br;
-        uint32_t rl, rr;
-        load_node(en, ref, bl, br, rl, rr);
-        bool hr = box_overlap(br, blo, bhi), hl = box_overlap(bl, blo, bhi);
-        if (sp + 2 > kStack) {
-            atomicOr(A.err, kErrStack);
-            hr = hl = false;
-        }
-        if (hr) st[sp++] = rr;
-        if (hl) st[sp++] = rl;
+        if (sp == 0) busy = false;
     }
+    atomicAdd(A.stats + 1, n_acc);
+    atomicAdd(A.stats + 2, n_skip);
+    atomicAdd(A.stats + 4, n_leaf);
+    atomicAdd(A.stats + 5, n_roots);
 }
 
-uint32_t sweep_persistent_blocks(bool quad) {
+template <bool QUAD>
+static int sweep_per_sm(int threads) {
     int per_sm = 0;
-    if (quad)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<true>, kTravThreads, 0);
+    if (threads == 64)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 64>, 64, 0);
+    else if (threads == 256)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 256>, 256, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<false>, kTravThreads, 0);
-    return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 128>, 128, 0);
+    return std::max(1, per_sm);
 }
 
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, cudaStream_t s) {
-    if (A.quad)
-        k_sweep<true><<<blocks, kTravThreads, 0, s>>>(S, A);
+uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads) {
+    return (uint32_t) (quad ? sweep_per_sm<true>((int) threads) : sweep_per_sm<false>((int) threads));
+}
+
+uint32_t sweep_persistent_blocks(bool quad) { return sweep_max_blocks_per_sm(quad, kTravThreads) * device_sm_count(); }
+
+template <bool QUAD>
+static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s) {
+    if (threads == 64)
+        k_sweep<QUAD, 64><<<blocks, 64, 0, s>>>(S, A);
+    else if (threads == 256)
+        k_sweep<QUAD, 256><<<blocks, 256, 0, s>>>(S, A);
     else
-        k_sweep<false><<<blocks, kTravThreads, 0, s>>>(S, A);
+        k_sweep<QUAD, 128><<<blocks, 128, 0, s>>>(S, A);
+}
+
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s) {
+    if (A.quad)
+        sweep_dispatch<true>(S, A, blocks, threads, s);
+    else
+        sweep_dispatch<false>(S, A, blocks, threads, s);
     cuda_check(cudaGetLastError(), "k_sweep");
 }
 

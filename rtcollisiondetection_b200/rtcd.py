@@ -27,6 +27,7 @@ CHECK_PLAIN = 1 << 3
 CHECK_NO_ENDPOINTS = 1 << 4
 CHECK_TIMING = 1 << 5
 CHECK_FUSED = 1 << 6
+CHECK_GRAPH = 1 << 7
 
 STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
           4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}
@@ -36,7 +37,8 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_detector_destroy', 'rtcd_check', 'rtcd_sync', 'rtcd_segment_offsets', 'rtcd_last_stats',
            'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
-           'rtcd_server_get_stats', 'rtcd_server_reset_stats']
+           'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune',
+           'rtcd_select_flags_u8_noalloc']
 
 
 class RTCDError(RuntimeError):
@@ -56,13 +58,15 @@ class RobotDesc(C.Structure):
 
 
 class Config(C.Structure):
-    _fields_ = [('frame_size', C.c_uint32), ('reserved', C.c_uint32 * 7)]
+    _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
+                ('reserved', C.c_uint32 * 5)]
 
 
 class Stats(C.Structure):
     _fields_ = [('work_items', C.c_uint64), ('culled_items', C.c_uint64), ('fp64_retests', C.c_uint64),
                 ('ms_prepare', C.c_float), ('ms_cull', C.c_float), ('ms_traverse', C.c_float),
-                ('ms_total', C.c_float), ('reserved', C.c_uint64 * 3)]
+                ('ms_total', C.c_float), ('candidates', C.c_uint64), ('exact_tests', C.c_uint64),
+                ('skipped', C.c_uint64)]
 
 
 _lib = None
@@ -255,12 +259,14 @@ def segment_offsets(kind, traj_off, flags=0):
 class Detector:
     """One detector of one kind over a robot and a scene."""
 
-    def __init__(self, ctx, kind, robot, scene, frame_size=0):
+    def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
         cfg = Config()
         cfg.frame_size = frame_size
+        cfg.traverse_threads = traverse_threads
+        cfg.traverse_blocks_per_sm = traverse_blocks_per_sm
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -304,11 +310,22 @@ class Detector:
     def sync(self, stream=None):
         _ok(lib().rtcd_sync(self.h, C.c_void_p(stream) if stream else None))
 
+    def autotune(self, q_dev, n, traj_off=None, stream=None):
+        """Pick the fastest traversal launch shape on this device-resident batch."""
+        traj_off = _arr(traj_off, np.uint32)
+        best = Config()
+        ms = C.c_float()
+        _ok(lib().rtcd_detector_autotune(self.h, _ptr(q_dev, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
+                                         C.c_void_p(stream) if stream else None, C.byref(best), C.byref(ms)))
+        return {'traverse_threads': best.traverse_threads, 'traverse_blocks_per_sm': best.traverse_blocks_per_sm,
+                'traverse_ms': ms.value}
+
     def stats(self):
         s = Stats()
         _ok(lib().rtcd_last_stats(self.h, C.byref(s)))
         return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests, 'ms_prepare': s.ms_prepare,
-                'ms_cull': s.ms_cull, 'ms_traverse': s.ms_traverse, 'ms_total': s.ms_total}
+                'ms_cull': s.ms_cull, 'ms_traverse': s.ms_traverse, 'ms_total': s.ms_total,
+                'candidates': s.candidates, 'exact_tests': s.exact_tests, 'skipped': s.skipped}
 
     def close(self):
         if self.h:
