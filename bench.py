@@ -208,11 +208,9 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0)
 
     def run_server():
         server = rtcd.Server(ctx, slots=slots)
-        for d in dets:              # first-touch of every clone outside the measured window
+        for d in dets:              # every slot's workspace sized outside the measured window
             for det in d.values():
-                t = server.submit(det, pose_pool[:8] if not det.sweep else traj_q[:traj_off[2]],
-                                  None if not det.sweep else traj_off[:3])
-                server.wait(t)
+                server.prepare(det, 1 << 17 if det.sweep else 0)
         server.reset_stats()
         tickets = [None] * n_req
         lat = np.zeros(n_req)

@@ -100,7 +100,10 @@ typedef struct {
     uint32_t frame_size;             /* poses per frame of the plain path; 0 = 64 */
     uint32_t traverse_threads;       /* threads per block of the traversal kernel: 64, 128 or 256; 0 = 128 */
     uint32_t traverse_blocks_per_sm; /* resident traversal blocks per SM; 0 = as many as fit */
-    uint32_t reserved[5];
+    int32_t stream_priority;         /* priority of the detector's own stream (CUDA convention: lower = higher) */
+    uint32_t residency_percent;      /* share of each SM its persistent kernels may hold (room for other
+                                        launches to run alongside); 0 = 100 */
+    uint32_t reserved[3];
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -207,10 +210,13 @@ RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 typedef struct rtcd_server rtcd_server;
 
 typedef struct {
-    uint32_t slots;           /* launches in flight at once; 0 = 4 */
-    uint32_t max_batch_units; /* poses / trajectory waypoints merged into one launch; 0 = 65536 */
-    uint64_t memory_budget;   /* bytes the in-flight launches may hold; 0 = half the free device memory */
-    uint32_t reserved[4];
+    uint32_t slots;              /* launches in flight at once; 0 = 4 */
+    uint32_t max_batch_units;    /* poses / trajectory waypoints merged into one launch; 0 = 65536 */
+    uint64_t memory_budget;      /* bytes the in-flight launches may hold; 0 = half the free device memory */
+    uint32_t fast_slots;         /* slots reserved for small requests, on high-priority streams; 0 = 1 when slots > 1 */
+    uint32_t fast_max_units;     /* a request is small up to this many units; 0 = 4096 */
+    uint32_t bulk_share;         /* percent of each SM's traversal residency the other slots may take; 0 = 50 */
+    uint32_t reserved[1];
 } rtcd_server_config;
 
 typedef struct {
@@ -227,6 +233,10 @@ typedef struct {
 #define RTCD_WAIT_FOREVER (-1)
 
 RTCD_API rtcd_status rtcd_server_create(rtcd_ctx* ctx, const rtcd_server_config* config, rtcd_server** out);
+/* Creates every slot's workspace for `det` and sizes it for launches of up to
+ * max_units units (0 = the server's max_batch_units), so serving never
+ * allocates (an allocation would synchronise the device).  Optional. */
+RTCD_API rtcd_status rtcd_server_prepare(rtcd_server* server, rtcd_detector* det, uint32_t max_units);
 /* Finishes every accepted request, then stops the workers. */
 RTCD_API rtcd_status rtcd_server_destroy(rtcd_server* server);
 /* Copies the inputs (host memory, as rtcd_check with RTCD_CHECK_HOST_BUFFERS)

@@ -39,10 +39,12 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+// Growth is geometric (at least 1.5x): cudaFree synchronises the device, so a
+// workspace that follows slowly rising batch sizes must not re-allocate often.
 void DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return;
+    size_t want = std::max<size_t>(std::max<size_t>(n, 256), bytes + bytes / 2);
     release();
-    size_t want = std::max<size_t>(n, 256);
     cuda_check(cudaMalloc(&p, want), "cudaMalloc");
     bytes = want;
 }
@@ -55,8 +57,8 @@ void HostBuf::release() {
 
 void HostBuf::ensure(size_t n) {
     if (n <= bytes && p) return;
+    size_t want = std::max<size_t>(std::max<size_t>(n, 256), bytes + bytes / 2);
     release();
-    size_t want = std::max<size_t>(n, 256);
     cuda_check(cudaMallocHost(&p, want), "cudaMallocHost");
     bytes = want;
 }
@@ -276,7 +278,7 @@ struct rtcd_detector {
     // discrete workspace
     DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
     DevBuf cand, item_overflow, overflow_items, wave_counts;  // wavefront traversal
-    uint32_t blocks_a = 0, blocks_b = 0;
+    uint32_t blocks_a = 0, blocks_b = 0, blocks_a_full = 0;
     uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
     ScanScratch scan;
     // sweep workspace
@@ -331,11 +333,17 @@ static void apply_launch_shape(rtcd_detector* d) {
     uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
                             : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
     uint32_t per_sm = d->cfg.traverse_blocks_per_sm ? std::min(d->cfg.traverse_blocks_per_sm, fit) : fit;
+    const uint32_t pct = d->cfg.residency_percent;
+    if (pct > 100) fail(RTCD_ERR_INVALID_ARGUMENT, "residency_percent must be at most 100");
+    const uint32_t sms = (uint32_t) device_sm_count();
+    if (pct) per_sm = std::max(1u, per_sm * pct / 100);
     d->threads = t;
-    if (discrete)
-        d->blocks_b = per_sm * (uint32_t) device_sm_count();
-    else
-        d->blocks = per_sm * (uint32_t) device_sm_count();
+    if (discrete) {
+        d->blocks_b = per_sm * sms;
+        if (pct) d->blocks_a = std::max(sms, d->blocks_a_full * pct / 100);
+    } else {
+        d->blocks = per_sm * sms;
+    }
 }
 
 struct DeviceScope {
@@ -606,13 +614,16 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         d->scene = scene;
         if (config) d->cfg = *config;
         if (!d->cfg.frame_size) d->cfg.frame_size = 64;
-        cuda_check(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        int lo_prio = 0, hi_prio = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio), "cudaDeviceGetStreamPriorityRange");
+        const int prio = std::min(lo_prio, std::max(hi_prio, (int) d->cfg.stream_priority));
+        cuda_check(cudaStreamCreateWithPriority(&d->stream, cudaStreamNonBlocking, prio), "cudaStreamCreate");
         cuda_check(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming), "cudaEventCreate");
         for (auto& e : d->ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         cuda_check(cudaEventCreate(&d->ev_end), "cudaEventCreate");
         if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS) {
             d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
-            d->blocks_a = stage_a_blocks(kind == RTCD_ROBOT_TO_OBS);
+            d->blocks_a = d->blocks_a_full = stage_a_blocks(kind == RTCD_ROBOT_TO_OBS);
         }
         apply_launch_shape(d.get());
         d->err.ensure(4);

@@ -1,14 +1,19 @@
 // server.cu - continuous-batching request server over resident scenes.
 //
-// Requests (any size, any thread) queue up; each of `slots` worker threads
-// owns one stream and its own workspace (a clone of every detector it serves,
-// sharing the resident robot and scene) and repeatedly takes the oldest
-// request plus every queued request for the same detector and flags, up to
-// max_batch_units, merges them into one launch, runs it, and splits the
-// flags back.  A launch is admitted only while the estimated bytes of the
-// launches in flight fit the memory budget.  Poses and trajectories are
-// independent, so a request's result in a merged launch equals its result
-// alone.
+// Requests (any size, any thread) queue up.  Each of `slots` worker threads
+// owns one stream and, per detector it serves, a clone of that detector (own
+// workspace, shared resident robot and scene).  A worker repeatedly takes the
+// oldest request it may serve plus every queued request for the same
+// detector and flags that fits, merges them into one launch, runs it and
+// splits the results.  Two classes of slots keep small requests fast:
+//  - fast slots serve only requests of at most fast_max_units units, on the
+//    highest-priority stream, with persistent kernels allowed the whole GPU;
+//  - bulk slots serve anything, on normal-priority streams, with persistent
+//    kernels limited to bulk_share percent of each SM, so a fast launch finds
+//    room to run beside a long bulk launch instead of queueing behind it.
+// A launch is admitted only while the estimated bytes of the launches in
+// flight fit the memory budget.  Poses and trajectories are independent, so
+// a request's result in a merged launch equals its result alone.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -38,8 +43,8 @@ struct Request {
     int kind = 0;
     uint32_t flags = 0;
     uint32_t n = 0;
-    uint32_t units = 0;            // poses, or waypoints of a sweep request
-    uint32_t segments = 0;         // sweep: segments of the request
+    uint32_t units = 0;     // poses, or waypoints of a sweep request
+    uint32_t segments = 0;  // sweep: segments of the request
     std::vector<float> q;
     std::vector<uint32_t> traj_off;
     std::vector<uint8_t> out_flags, out_seg;
@@ -53,6 +58,12 @@ struct Request {
 
 bool is_sweep(int kind) { return kind == RTCD_LINEAR_SWEEP || kind == RTCD_QUAD_SWEEP; }
 
+struct Slot {
+    bool fast = false;
+    std::mutex mu;                                      // held while the slot runs a launch or is prepared
+    std::map<rtcd_detector*, rtcd_detector*> clones;    // user detector -> this slot's clone
+};
+
 }  // namespace
 
 struct rtcd_server {
@@ -65,9 +76,9 @@ struct rtcd_server {
     uint64_t next_ticket = 1;
     bool stopping = false;
     uint64_t inflight_bytes = 0;
-    // statistics
     uint64_t submitted = 0, completed = 0, failed = 0, units_completed = 0, batches = 0, inflight_peak = 0;
     std::vector<double> latencies;
+    std::vector<std::unique_ptr<Slot>> slots;
     std::vector<std::thread> workers;
 };
 
@@ -80,24 +91,86 @@ uint64_t estimate_bytes(int kind, uint64_t n, uint64_t units, uint32_t n_links, 
     return units * (4ull * dof + 2ull * 16 * n_spheres) + n * 16 + units * 8;
 }
 
-void worker(rtcd_server* S) {
-    std::map<std::pair<rtcd_detector*, uint32_t>, rtcd_detector*> clones;
+// The slot's clone of a user detector (created on first use).
+rtcd_detector* clone_for(rtcd_server* S, Slot& slot, rtcd_detector* det) {
+    rtcd_detector*& c = slot.clones[det];
+    if (c) return c;
+    rtcd_ctx* ctx;
+    int kind;
+    rtcd_robot* rb;
+    rtcd_scene* sc;
+    rtcd_config cfg;
+    uint32_t nl, ns, dof;
+    rtcd::detector_info(det, &ctx, &kind, &rb, &sc, &cfg, &nl, &ns, &dof);
+    if (slot.fast) {
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        cfg.stream_priority = hi;
+        cfg.residency_percent = 0;
+    } else {
+        cfg.stream_priority = 0;
+        cfg.residency_percent = S->cfg.bulk_share;
+    }
+    rtcd_status st = rtcd_detector_create(ctx, (rtcd_detector_kind) kind, rb, sc, &cfg, &c);
+    if (st != RTCD_OK) {
+        c = nullptr;
+        char buf[256];
+        rtcd_last_error(buf, sizeof(buf));
+        rtcd::fail(st, buf);
+    }
+    return c;
+}
+
+// Runs one merged launch on the slot's clone; host buffers in and out.
+rtcd_status run_launch(rtcd_server* S, Slot& slot, rtcd_detector* det, int kind, const std::vector<float>& q,
+                       const std::vector<uint32_t>& off, uint32_t n, uint32_t flags, std::vector<uint8_t>& out_flags,
+                       std::vector<uint8_t>& out_seg, std::vector<uint32_t>& out_counts, std::string& msg) {
+    rtcd_detector* c = nullptr;
+    try {
+        c = clone_for(S, slot, det);
+    } catch (const rtcd::Error& e) {
+        msg = e.msg;
+        return (rtcd_status) e.status;
+    }
+    const bool sweep = is_sweep(kind);
+    const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
+    rtcd_status st = rtcd_check(c, q.data(), sweep ? off.data() : nullptr, n, out_flags.data(),
+                                sweep ? out_seg.data() : nullptr, counts ? out_counts.data() : nullptr,
+                                (flags & (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS)) | RTCD_CHECK_HOST_BUFFERS,
+                                nullptr);
+    if (st != RTCD_OK) {
+        char buf[512];
+        rtcd_last_error(buf, sizeof(buf));
+        msg = buf;
+    }
+    return st;
+}
+
+void worker(rtcd_server* S, Slot* slot) {
     std::vector<float> q;
-    std::vector<uint32_t> off, counts, seg_off;
+    std::vector<uint32_t> off, counts;
     std::vector<uint8_t> flags, seg;
+    const uint32_t limit = slot->fast ? std::max(S->cfg.fast_max_units, 1u) * 2 : S->cfg.max_batch_units;
     while (true) {
         std::vector<Request*> batch;
         uint64_t bytes = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stopping || !S->pending.empty(); });
-            if (S->pending.empty()) break;  // stopping and drained
-            Request* first = S->pending.front();
+            auto servable = [&](const Request* r) { return !slot->fast || r->units <= S->cfg.fast_max_units; };
+            auto has_work = [&] {
+                for (const Request* r : S->pending)
+                    if (servable(r)) return true;
+                return false;
+            };
+            S->cv_work.wait(lk, [&] { return S->stopping || has_work(); });
+            if (!has_work()) break;  // stopping, and nothing this slot may serve is left
+            auto first_it = std::find_if(S->pending.begin(), S->pending.end(), servable);
+            Request* first = *first_it;
             uint64_t units = 0;
-            for (auto it = S->pending.begin(); it != S->pending.end();) {
+            for (auto it = first_it; it != S->pending.end();) {
                 Request* r = *it;
-                if (r->det == first->det && r->flags == first->flags &&
-                    (batch.empty() || units + r->units <= S->cfg.max_batch_units)) {
+                if (servable(r) && r->det == first->det && r->flags == first->flags &&
+                    (batch.empty() || units + r->units <= limit)) {
                     batch.push_back(r);
                     units += r->units;
                     it = S->pending.erase(it);
@@ -115,19 +188,21 @@ void worker(rtcd_server* S) {
             uint64_t n = 0;
             for (Request* r : batch) n += r->n;
             bytes = estimate_bytes(kind, n, units, nl, ns, dof);
-            // admission: wait while other launches hold the budget
             S->cv_mem.wait(lk, [&] { return S->inflight_bytes == 0 || S->inflight_bytes + bytes <= S->cfg.memory_budget; });
             S->inflight_bytes += bytes;
             S->inflight_peak = std::max(S->inflight_peak, S->inflight_bytes);
             ++S->batches;
+            if (!S->pending.empty()) S->cv_work.notify_all();  // others may serve what is left
         }
         // merge the inputs
         Request* r0 = batch[0];
         const bool sweep = is_sweep(r0->kind);
         size_t nq = 0, n = 0;
+        uint32_t total_seg = 0;
         for (Request* r : batch) {
             nq += r->q.size();
             n += r->n;
+            total_seg += r->segments;
         }
         q.resize(nq);
         size_t pos = 0;
@@ -135,45 +210,25 @@ void worker(rtcd_server* S) {
         for (Request* r : batch) {
             std::memcpy(q.data() + pos, r->q.data(), r->q.size() * sizeof(float));
             if (sweep) {
-                uint32_t base = off.back();
+                const uint32_t base = off.back();
                 for (uint32_t i = 1; i <= r->n; ++i) off.push_back(base + r->traj_off[i]);
             }
             pos += r->q.size();
         }
         flags.assign(n, 0);
         counts.assign(n, 0);
-        const bool want_counts = (r0->flags & RTCD_CHECK_COUNTS) != 0;
-        uint32_t total_seg = 0;
-        for (Request* r : batch) total_seg += r->segments;
         seg.assign(sweep ? std::max<uint32_t>(total_seg, 1) : 0, 0);
-        rtcd_detector*& clone = clones[{r0->det, r0->flags}];
-        rtcd_status st = RTCD_OK;
         std::string msg;
-        if (!clone) {
-            rtcd_ctx* c;
-            int kind;
-            rtcd_robot* rb;
-            rtcd_scene* sc;
-            rtcd_config dc;
-            uint32_t nl, ns, dof;
-            rtcd::detector_info(r0->det, &c, &kind, &rb, &sc, &dc, &nl, &ns, &dof);
-            st = rtcd_detector_create(c, (rtcd_detector_kind) kind, rb, sc, &dc, &clone);
+        rtcd_status st;
+        {
+            std::lock_guard<std::mutex> sl(slot->mu);
+            st = run_launch(S, *slot, r0->det, r0->kind, q, off, (uint32_t) n, r0->flags, flags, seg, counts, msg);
         }
-        if (st == RTCD_OK)
-            st = rtcd_check(clone, q.data(), sweep ? off.data() : nullptr, (uint32_t) n, flags.data(),
-                            sweep ? seg.data() : nullptr, want_counts ? counts.data() : nullptr,
-                            (r0->flags & (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS)) | RTCD_CHECK_HOST_BUFFERS,
-                            nullptr);
-        if (st != RTCD_OK) {
-            char buf[512];
-            rtcd_last_error(buf, sizeof(buf));
-            msg = buf;
-        }
-        // split the results
+        const bool want_counts = (r0->flags & RTCD_CHECK_COUNTS) != 0;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             size_t p = 0, sp = 0;
-            auto now = Clock::now();
+            const auto now = Clock::now();
             for (Request* r : batch) {
                 r->status = st;
                 r->error = msg;
@@ -197,8 +252,6 @@ void worker(rtcd_server* S) {
         S->cv_done.notify_all();
         S->cv_mem.notify_all();
     }
-    for (auto& kv : clones)
-        if (kv.second) rtcd_detector_destroy(kv.second);
 }
 
 template <class F>
@@ -227,15 +280,25 @@ rtcd_status rtcd_server_create(rtcd_ctx* ctx, const rtcd_server_config* config, 
         std::unique_ptr<rtcd_server> S(new rtcd_server());
         S->ctx = ctx;
         if (config) S->cfg = *config;
-        if (!S->cfg.slots) S->cfg.slots = 4;
-        if (S->cfg.slots > 64) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "at most 64 slots");
-        if (!S->cfg.max_batch_units) S->cfg.max_batch_units = 65536;
-        if (!S->cfg.memory_budget) {
+        rtcd_server_config& c = S->cfg;
+        if (!c.slots) c.slots = 4;
+        if (c.slots > 64) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "at most 64 slots");
+        if (!c.max_batch_units) c.max_batch_units = 65536;
+        if (!c.fast_max_units) c.fast_max_units = 4096;
+        if (!c.fast_slots) c.fast_slots = c.slots > 1 ? 1 : 0;
+        if (c.fast_slots >= c.slots) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "at least one slot must serve any request");
+        if (!c.bulk_share) c.bulk_share = 50;
+        if (c.bulk_share > 100) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "bulk_share is a percentage");
+        if (!c.memory_budget) {
             size_t free_b = 0, total_b = 0;
             rtcd::cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
-            S->cfg.memory_budget = free_b / 2;
+            c.memory_budget = free_b / 2;
         }
-        for (uint32_t i = 0; i < S->cfg.slots; ++i) S->workers.emplace_back(worker, S.get());
+        for (uint32_t i = 0; i < c.slots; ++i) {
+            S->slots.emplace_back(new Slot());
+            S->slots.back()->fast = i < c.fast_slots;
+        }
+        for (auto& sl : S->slots) S->workers.emplace_back(worker, S.get(), sl.get());
         *out = S.release();
     });
 }
@@ -249,7 +312,48 @@ rtcd_status rtcd_server_destroy(rtcd_server* S) {
         }
         S->cv_work.notify_all();
         for (auto& t : S->workers) t.join();
+        for (auto& sl : S->slots)
+            for (auto& kv : sl->clones)
+                if (kv.second) rtcd_detector_destroy(kv.second);
         delete S;
+    });
+}
+
+rtcd_status rtcd_server_prepare(rtcd_server* S, rtcd_detector* det, uint32_t max_units) {
+    return guard([&] {
+        if (!S || !det) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "NULL argument");
+        rtcd_ctx* c;
+        int kind;
+        rtcd_robot* rb;
+        rtcd_scene* sc;
+        rtcd_config dc;
+        uint32_t nl, ns, dof;
+        rtcd::detector_info(det, &c, &kind, &rb, &sc, &dc, &nl, &ns, &dof);
+        if (c != S->ctx) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "detector belongs to another context");
+        for (auto& sl : S->slots) {
+            uint32_t units = max_units ? max_units : S->cfg.max_batch_units;
+            if (sl->fast) units = std::min(units, std::max(S->cfg.fast_max_units, 1u) * 2);
+            // a synthetic launch of that size: the zero pose (or 16-waypoint zero trajectories)
+            std::vector<uint32_t> off;
+            uint32_t n = units;
+            if (is_sweep(kind)) {
+                n = std::max(1u, units / 16);
+                off.resize(n + 1);
+                for (uint32_t i = 0; i <= n; ++i) off[i] = 16 * i;
+                units = 16 * n;
+            }
+            std::vector<float> q((size_t) units * dof, 0.0f);
+            std::vector<uint8_t> fl(n), seg;
+            std::vector<uint32_t> cnt(n);
+            if (is_sweep(kind)) seg.resize((size_t) units + 2 * n);
+            std::string msg;
+            std::lock_guard<std::mutex> lk(sl->mu);
+            // flags-only and counting launches size different buffers
+            for (uint32_t fl_mode : {0u, (uint32_t) RTCD_CHECK_COUNTS}) {
+                rtcd_status st = run_launch(S, *sl, det, kind, q, off, n, fl_mode, fl, seg, cnt, msg);
+                if (st != RTCD_OK) rtcd::fail(st, msg);
+            }
+        }
     });
 }
 
@@ -274,10 +378,10 @@ rtcd_status rtcd_server_submit(rtcd_server* S, rtcd_detector* det, const float* 
         r->n = n;
         if (is_sweep(kind)) {
             if (!traj_offsets) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "traj_offsets required for sweep detectors");
+            if (traj_offsets[0] != 0) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "traj_offsets must start at 0");
             std::vector<uint32_t> seg(n + 1);
             rtcd_status st = rtcd_segment_offsets((rtcd_detector_kind) kind, traj_offsets, n, flags, seg.data());
             if (st != RTCD_OK) rtcd::fail(st, "bad traj_offsets");
-            if (traj_offsets[0] != 0) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "traj_offsets must start at 0");
             r->traj_off.assign(traj_offsets, traj_offsets + n + 1);
             r->units = traj_offsets[n];
             r->segments = seg[n];
@@ -293,7 +397,7 @@ rtcd_status rtcd_server_submit(rtcd_server* S, rtcd_detector* det, const float* 
         ++S->submitted;
         S->pending.push_back(r.get());
         S->requests[r->ticket] = std::move(r);
-        S->cv_work.notify_one();
+        S->cv_work.notify_all();
     });
 }
 

@@ -37,7 +37,7 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_detector_destroy', 'rtcd_check', 'rtcd_sync', 'rtcd_segment_offsets', 'rtcd_last_stats',
            'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
-           'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune',
+           'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
            'rtcd_select_flags_u8_noalloc']
 
 
@@ -59,7 +59,7 @@ class RobotDesc(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
-                ('reserved', C.c_uint32 * 5)]
+                ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('reserved', C.c_uint32 * 3)]
 
 
 class Stats(C.Structure):
@@ -399,7 +399,8 @@ class CollisionDetector:
 
 class ServerConfig(C.Structure):
     _fields_ = [('slots', C.c_uint32), ('max_batch_units', C.c_uint32), ('memory_budget', C.c_uint64),
-                ('reserved', C.c_uint32 * 4)]
+                ('fast_slots', C.c_uint32), ('fast_max_units', C.c_uint32), ('bulk_share', C.c_uint32),
+                ('reserved', C.c_uint32 * 1)]
 
 
 class ServerStats(C.Structure):
@@ -415,13 +416,19 @@ class Server:
     thread, wait for tickets; requests for the same detector are merged into
     shared launches across ``slots`` concurrent streams."""
 
-    def __init__(self, ctx, slots=4, max_batch_units=65536, memory_budget=0):
+    def __init__(self, ctx, slots=4, max_batch_units=65536, memory_budget=0, fast_slots=0, fast_max_units=0,
+                 bulk_share=0):
         cfg = ServerConfig()
         cfg.slots, cfg.max_batch_units, cfg.memory_budget = slots, max_batch_units, memory_budget
+        cfg.fast_slots, cfg.fast_max_units, cfg.bulk_share = fast_slots, fast_max_units, bulk_share
         self.ctx = ctx
         self.h = VP()
         _ok(lib().rtcd_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
         self._meta = {}
+
+    def prepare(self, det, max_units=0):
+        """Size every slot's workspace for `det` up front (serving then never allocates)."""
+        _ok(lib().rtcd_server_prepare(self.h, det.h, C.c_uint32(max_units)))
 
     def submit(self, det, q, traj_off=None, counts=False, endpoints=True):
         q = _arr(q, np.float32)

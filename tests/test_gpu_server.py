@@ -89,6 +89,46 @@ def test_server_merges_queued_requests(world, panda):
     assert np.array_equal(np.concatenate([o['flags'] for o in outs]), whole)
 
 
+def test_server_fast_lane_prepared(world, panda):
+    """A prepared server with one fast slot (requests of <= 256 units on a
+    high-priority stream) and two bulk slots at 25 % residency: small and
+    large requests interleaved, results equal to the requests checked alone."""
+    _, dets = world
+    server = rtcd.Server(dets['lin'].ctx, slots=3, max_batch_units=8192, fast_slots=1, fast_max_units=256,
+                         bulk_share=25)
+    for k in ('r2o_small', 'o2r_small', 'lin', 'quad'):
+        server.prepare(dets[k], 4096)
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(40):
+        k = ['r2o_small', 'o2r_small', 'lin', 'quad'][i % 4]
+        big = i % 3 == 0
+        if k in ('lin', 'quad'):
+            nt = 200 if big else int(rng.integers(1, 12))
+            q, off = scenes.random_walk_trajectories(panda, nt, scenes.log_uniform_counts(nt, 8, 24, seed=i), seed=i)
+        else:
+            q, off = scenes.uniform_poses(panda, 3000 if big else int(rng.integers(1, 200)), seed=500 + i), None
+        reqs.append((k, q, off))
+    tickets = [server.submit(dets[k], q, off) for k, q, off in reqs]
+    outs = [server.wait(t, timeout_ms=120000) for t in tickets]
+    st = server.stats()
+    server.close()
+    assert st['completed'] == len(reqs) and st['failed'] == 0
+    for (k, q, off), got in zip(reqs, outs):
+        alone = dets[k].check(q, off, segments=dets[k].sweep)
+        assert np.array_equal(got['flags'], alone['flags']), k
+        if dets[k].sweep:
+            assert np.array_equal(got['seg_flags'], alone['seg_flags']), k
+
+
+def test_server_rejects_bad_config(world):
+    _, dets = world
+    with pytest.raises(rtcd.RTCDError):
+        rtcd.Server(dets['lin'].ctx, slots=2, fast_slots=2)        # no slot would take large requests
+    with pytest.raises(rtcd.RTCDError):
+        rtcd.Server(dets['lin'].ctx, slots=2, bulk_share=150)
+
+
 def test_server_rejects_bad_requests(world, panda):
     _, dets = world
     server = rtcd.Server(dets['lin'].ctx, slots=1)
