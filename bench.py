@@ -168,7 +168,7 @@ def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512):
             'collision_rate': float(ref['traj_hit'].mean())}
 
 
-def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0):
+def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0, server_kw=None, details=False):
     """Mixed request stream against three resident scenes (5k, 50k, ~500k
     triangles): Poisson arrivals at `rate` req/s for `seconds`; half discrete
     RobotToObs batches of log-uniform[1, 4096] poses, half continuous batches
@@ -207,7 +207,7 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0)
             reqs.append((dets[s][k], traj_q[traj_off[t0]:traj_off[t0 + nt]], off, nt))
 
     def run_server():
-        server = rtcd.Server(ctx, slots=slots)
+        server = rtcd.Server(ctx, slots=slots, **(server_kw or {}))
         for d in dets:              # every slot's workspace sized outside the measured window
             for det in d.values():
                 server.prepare(det, 1 << 17 if det.sweep else 0)
@@ -245,7 +245,15 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0)
            'p99_ms_discrete_le4096': float(np.percentile(lat[disc], 99)),
            'p50_ms_all': float(np.percentile(lat, 50)), 'p99_ms_all': float(np.percentile(lat, 99)),
            'poses_per_s': poses / wall, 'trajectories_per_s': trajs / wall, 'batches': st['batches'],
+           'queue_p50_ms': st['queue_p50_ms'], 'queue_p99_ms': st['queue_p99_ms'], 'run_p99_ms': st['run_p99_ms'],
            'scenes_tris': [m.n_tris for m in meshes]}
+    if details:
+        scene_of = {id(det): i for i, d in enumerate(dets) for det in d.values()}
+        out['details'] = {'latency_ms': lat, 'discrete': disc, 'size': sizes,
+                          'scene': np.array([scene_of[id(r[0])] for r in reqs]),
+                          'kind': [r[0].kind for r in reqs]}
+    if plain_seconds <= 0:
+        return out
     # plain: the same arrivals, one request at a time through the frame-by-frame path
     m = int(rate * plain_seconds)
     plat = np.zeros(m)
@@ -355,13 +363,16 @@ def main():
     sp = stream.cuda_stream
     qd = torch.from_numpy(q).cuda()
     fd = torch.zeros(n, dtype=torch.uint8, device='cuda')
+    # sweeps: per-trajectory and per-segment flags (segment = linear capsule / quadratic piece or end sphere)
+    n_seg = int(rtcd.segment_offsets(det.kind, off, 0)[-1]) if sweep else 0
+    segd = torch.zeros(max(n_seg, 1), dtype=torch.uint8, device='cuda') if sweep else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
 
     tuned = det.autotune(qd, n, off, stream=sp)   # untimed: picks the traversal launch shape
     base_flags = rtcd.CHECK_TIMING | (rtcd.CHECK_FUSED if args.fused else 0)
 
     def step(extra=0):
-        det.check_device(qd, n, fd, traj_off=off, flags=base_flags | extra, stream=sp)
+        det.check_device(qd, n, fd, traj_off=off, seg_dev=segd, flags=base_flags | extra, stream=sp)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -404,14 +415,16 @@ def main():
         flush.fill_(k & 255)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        out = det.check(q, off)
+        out = det.check(q, off, segments=sweep)
         dt = (time.perf_counter() - t0) * 1e3
         if k >= 2:
             e2e_ms.append(dt)
     e2e_step = float(np.mean(e2e_ms))
     assert np.array_equal(out['flags'], flags), 'host-buffer path disagrees with the device path'
+    if sweep:
+        assert np.array_equal(out['seg_flags'], segd.cpu().numpy()[:n_seg]), 'segment flags disagree'
     h2d = q.nbytes + (0 if off is None else off.nbytes)
-    d2h = n
+    d2h = n + n_seg
 
     # plain path: frames of 64 poses, host round trip per frame (the upstream check() shape)
     plain = None
@@ -449,7 +462,9 @@ def main():
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
-        'gpu_launches': args.steps * (5 if not sweep else (4 if cfg['kind'] == 'Linear' else 5)),
+        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_a, k_stage_b, k_discrete (overflow), k_flags;
+        # sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2 (trajectories, segments)
+        'gpu_launches': args.steps * (7 if not sweep else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in trav])),
                       'cull': float(np.mean([s['ms_cull'] for s in trav])), 'traverse': t_trav},
         'roofline': {'bound': 'hbm', 'kernel': 'k_sweep' if sweep else 'k_discrete', 'achieved': achieved,

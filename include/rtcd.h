@@ -103,7 +103,10 @@ typedef struct {
     int32_t stream_priority;         /* priority of the detector's own stream (CUDA convention: lower = higher) */
     uint32_t residency_percent;      /* share of each SM its persistent kernels may hold (room for other
                                         launches to run alongside); 0 = 100 */
-    uint32_t reserved[3];
+    uint32_t sweep_light_steps;      /* sweeps: node + leaf visits one lane spends on a (piece, sphere) unit
+                                        before a whole warp takes the unit over; 0 = 32 linear / 16 quadratic,
+                                        0xFFFFFFFF = never */
+    uint32_t reserved[2];
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -168,7 +171,9 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
 /* Autotuner: runs the given device-resident batch (q_dev; traj_offsets on the
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
- * that fit - times the traversal kernel with device events (median of
+ * that fit, and for the sweep detectors each at a light-pass budget of 16, 32
+ * and 64 visits (sweeps are timed with segment flags on) - times the
+ * traversal with device events (median of
  * three after a warm-up run), keeps the fastest shape in the detector and
  * writes it to best_out (optional).  The upstream picks its batch size per
  * experiment by hand (CollisionDetector.h:365-394). */
@@ -227,7 +232,9 @@ typedef struct {
     uint32_t queue_depth;       /* requests waiting for a slot */
     uint32_t reserved0;
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result ready, over completed requests */
-    uint64_t reserved[4];
+    double queue_p50_ms, queue_p99_ms;      /* submit -> its launch started */
+    double run_p99_ms;                      /* launch started -> result ready */
+    uint64_t reserved[1];
 } rtcd_server_stats;
 
 #define RTCD_WAIT_FOREVER (-1)

@@ -282,7 +282,7 @@ struct rtcd_detector {
     uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
     ScanScratch scan;
     // sweep workspace
-    DevBuf centers, ctrl, aux, piece_hit, W, W_off;
+    DevBuf centers, ctrl, aux, piece_hit, W, W_off, heavy;
     std::vector<float> W_host;
     std::vector<uint32_t> W_off_host;
     uint32_t W_max = 0;
@@ -628,7 +628,7 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         apply_launch_shape(d.get());
         d->err.ensure(4);
         d->stats.ensure(8 * 8);
-        d->work.ensure(4);
+        d->work.ensure(16);  // [0] work counter, [1] heavy units appended, [2] heavy-pass counter
         d->count.ensure(4);
         cuda_check(cudaMemset(d->err.p, 0, 4), "memset");
         cuda_check(cudaMemset(d->stats.p, 0, 64), "memset");
@@ -989,7 +989,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         d_counts = d->counts.as<uint32_t>();
         cuda_check(cudaMemsetAsync(d_counts, 0, 4ull * n, s), "memset");
     }
-    cuda_check(cudaMemsetAsync(d->work.p, 0, 4, s), "memset");
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 12, s), "memset");
     SweepArgs A{};
     A.centers = d->centers.as<float4>();
     A.ctrl = quad ? d->ctrl.as<float4>() : nullptr;
@@ -1010,12 +1010,24 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.stats = d->stats.as<unsigned long long>();
     A.want_counts = counts;
     A.want_pieces = want_pieces;
+    A.light_steps = d->cfg.sweep_light_steps == 0xFFFFFFFFu ? 0u
+                    : d->cfg.sweep_light_steps                ? d->cfg.sweep_light_steps
+                                                              : (quad ? 16u : 32u);
+    if (A.light_steps) {
+        const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns / 4, 1024), 1u << 22);
+        d->heavy.ensure(4ull * cap);
+        A.heavy = d->heavy.as<uint32_t>();
+        A.heavy_cap = cap;
+        A.heavy_count = d->work.as<uint32_t>() + 1;
+        A.heavy_work = d->work.as<uint32_t>() + 2;
+    }
     d->last_items = A.total_units;
     if (timed) {
         cuda_check(cudaEventRecord(d->ev[1], s), "event");
         cuda_check(cudaEventRecord(d->ev[2], s), "event");
     }
-    if (A.total_units) launch_sweep(d->scene->dev, A, d->blocks, d->threads, s);
+    if (A.total_units)
+        launch_sweep(d->scene->dev, A, d->blocks, d->threads, d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     // outputs
     uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
@@ -1183,11 +1195,22 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         DeviceScope ds(d->ctx->device);
         cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
         const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
-        DevBuf flags;
+        DevBuf flags, seg;
         flags.ensure(n);
+        uint32_t n_seg = 0;
+        if (!discrete) {  // sweeps are tuned with segment flags on (no trajectory-level early exit)
+            std::vector<uint32_t> so(n + 1);
+            rtcd_status st = rtcd_segment_offsets(d->kind, traj_offsets, n, 0, so.data());
+            if (st != RTCD_OK) fail(st, g_last_error);
+            n_seg = so[n];
+            seg.ensure(std::max(n_seg, 1u));
+        }
         const rtcd_config saved = d->cfg;
         rtcd_config best = saved;
         float best_t = 3.0e38f;
+        const std::vector<uint32_t> lights = discrete ? std::vector<uint32_t>{saved.sweep_light_steps}
+                                                      : std::vector<uint32_t>{16u, 32u, 64u};
+        for (uint32_t light : lights)
         for (uint32_t t : {64u, 128u, 256u}) {
             uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
                                     : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
@@ -1196,11 +1219,12 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
             for (uint32_t per_sm : shapes) {
                 d->cfg.traverse_threads = t;
                 d->cfg.traverse_blocks_per_sm = per_sm;
+                d->cfg.sweep_light_steps = light;
                 apply_launch_shape(d);
                 float ms[4];
                 for (int rep = 0; rep < 4; ++rep) {
-                    rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(), nullptr, nullptr,
-                                                RTCD_CHECK_TIMING, s);
+                    rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(),
+                                                discrete ? nullptr : seg.as<uint8_t>(), nullptr, RTCD_CHECK_TIMING, s);
                     rtcd_stats stt;
                     if (st == RTCD_OK) st = rtcd_last_stats(d, &stt);
                     if (st != RTCD_OK) {

@@ -109,12 +109,20 @@ struct SweepArgs {
     unsigned long long* stats;
     int want_counts;
     int want_pieces;
+    uint32_t light_steps;      // visits before a unit moves to the heavy pass; 0 = no heavy pass
+    uint32_t* heavy;           // [heavy_cap] units handed to the heavy pass
+    uint32_t heavy_cap;
+    uint32_t* heavy_count;     // units appended (may exceed heavy_cap: those stayed in the light pass)
+    uint32_t* heavy_work;      // heavy-pass work counter
 };
 
 void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s);
 void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_t* d_ctrl_off, const float* d_W,
                 const uint32_t* d_W_off, uint32_t n_traj, uint32_t n_spheres, float4* d_ctrl, cudaStream_t s);
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s);
+// The light pass on `blocks` blocks of `threads`, then (when A.light_steps)
+// the heavy pass on heavy_share percent of its full persistent grid.
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, uint32_t heavy_share,
+                  cudaStream_t s);
 uint32_t sweep_persistent_blocks(bool quad);
 uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads);  // threads: 64, 128 or 256
 

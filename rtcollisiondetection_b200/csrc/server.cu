@@ -77,7 +77,7 @@ struct rtcd_server {
     bool stopping = false;
     uint64_t inflight_bytes = 0;
     uint64_t submitted = 0, completed = 0, failed = 0, units_completed = 0, batches = 0, inflight_peak = 0;
-    std::vector<double> latencies;
+    std::vector<double> latencies, queue_ms, run_ms;
     std::vector<std::unique_ptr<Slot>> slots;
     std::vector<std::thread> workers;
 };
@@ -220,6 +220,7 @@ void worker(rtcd_server* S, Slot* slot) {
         seg.assign(sweep ? std::max<uint32_t>(total_seg, 1) : 0, 0);
         std::string msg;
         rtcd_status st;
+        const auto started = Clock::now();
         {
             std::lock_guard<std::mutex> sl(slot->mu);
             st = run_launch(S, *slot, r0->det, r0->kind, q, off, (uint32_t) n, r0->flags, flags, seg, counts, msg);
@@ -229,6 +230,7 @@ void worker(rtcd_server* S, Slot* slot) {
             std::lock_guard<std::mutex> lk(S->mu);
             size_t p = 0, sp = 0;
             const auto now = Clock::now();
+            const double run = std::chrono::duration<double, std::milli>(now - started).count();
             for (Request* r : batch) {
                 r->status = st;
                 r->error = msg;
@@ -242,7 +244,11 @@ void worker(rtcd_server* S, Slot* slot) {
                     ++S->failed;
                 }
                 r->latency_ms = std::chrono::duration<double, std::milli>(now - r->submitted).count();
-                if (st == RTCD_OK) S->latencies.push_back(r->latency_ms);
+                if (st == RTCD_OK) {
+                    S->latencies.push_back(r->latency_ms);
+                    S->queue_ms.push_back(std::chrono::duration<double, std::milli>(started - r->submitted).count());
+                    S->run_ms.push_back(run);
+                }
                 r->done = true;
                 p += r->n;
                 sp += r->segments;
@@ -433,7 +439,7 @@ rtcd_status rtcd_server_get_stats(rtcd_server* S, rtcd_server_stats* out) {
     return guard([&] {
         if (!S || !out) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "NULL argument");
         std::memset(out, 0, sizeof(*out));
-        std::vector<double> lat;
+        std::vector<double> lat, qms, rms;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             out->submitted = S->submitted;
@@ -444,15 +450,18 @@ rtcd_status rtcd_server_get_stats(rtcd_server* S, rtcd_server_stats* out) {
             out->inflight_bytes_peak = S->inflight_peak;
             out->queue_depth = (uint32_t) S->pending.size();
             lat = S->latencies;
+            qms = S->queue_ms;
+            rms = S->run_ms;
         }
+        auto pct = [](std::vector<double>& v, double p) {
+            if (v.empty()) return 0.0;
+            size_t k = std::min(v.size() - 1, (size_t) (p * (double) (v.size() - 1) + 0.5));
+            std::nth_element(v.begin(), v.begin() + (long) k, v.end());
+            return v[k];
+        };
         if (!lat.empty()) {
-            auto pct = [&](double p) {
-                size_t k = std::min(lat.size() - 1, (size_t) (p * (double) (lat.size() - 1) + 0.5));
-                std::nth_element(lat.begin(), lat.begin() + (long) k, lat.end());
-                return lat[k];
-            };
-            out->p50_ms = pct(0.50);
-            out->p99_ms = pct(0.99);
+            out->p50_ms = pct(lat, 0.50);
+            out->p99_ms = pct(lat, 0.99);
             double s = 0, mx = 0;
             for (double v : lat) {
                 s += v;
@@ -461,6 +470,9 @@ rtcd_status rtcd_server_get_stats(rtcd_server* S, rtcd_server_stats* out) {
             out->mean_ms = s / (double) lat.size();
             out->max_ms = mx;
         }
+        out->queue_p50_ms = pct(qms, 0.50);
+        out->queue_p99_ms = pct(qms, 0.99);
+        out->run_p99_ms = pct(rms, 0.99);
     });
 }
 
@@ -471,6 +483,8 @@ rtcd_status rtcd_server_reset_stats(rtcd_server* S) {
         S->submitted = S->completed = S->failed = S->units_completed = S->batches = 0;
         S->inflight_peak = S->inflight_bytes;
         S->latencies.clear();
+        S->queue_ms.clear();
+        S->run_ms.clear();
     });
 }
 

@@ -292,79 +292,207 @@ __device__ __noinline__ bool sweep_retest_f64(float4 ea, float4 eb, float4 P0, f
 // ---------------------------------------------------------------- traversal
 __device__ __forceinline__ uint32_t ldflag(const uint32_t* p) { return __ldcg(p); }
 
+// 1 / v, or a huge value of the same sign for v == 0 (a zero chord component:
+// the slab test then keeps the box exactly when the origin lies in its slab).
+__device__ __forceinline__ float chord_inv(float v) { return v != 0.0f ? 1.0f / v : copysignf(3.0e38f, v); }
+
+// One unit of work: one sphere over one trajectory piece.  Linear: the
+// capsule axis P0-P1.  Quadratic: the Bezier piece B0, B1, B2 (P0, P1, P2),
+// or an end sphere (P0 = P1 = P2).
+struct SweepUnit {
+    float4 P0, P1, P2;
+    float r;
+    uint32_t traj, piece_g;
+};
+
+template <bool QUAD>
+__device__ __forceinline__ bool load_unit(const SweepArgs& A, uint32_t u, SweepUnit& U) {
+    U.piece_g = u / A.n_spheres;
+    const uint32_t s = u - U.piece_g * A.n_spheres;
+    U.traj = A.piece_traj[U.piece_g];
+    if (U.traj >= A.n_traj) return false;
+    const uint32_t piece = U.piece_g - A.traj_piece_off[U.traj];
+    const uint32_t w0 = A.traj_wp_off[U.traj], nwp = A.traj_wp_off[U.traj + 1] - w0;
+    if (!QUAD) {
+        U.P0 = A.centers[(size_t) (w0 + piece) * A.n_spheres + s];
+        U.P1 = A.centers[(size_t) (w0 + piece + 1) * A.n_spheres + s];
+        U.P2 = U.P1;
+    } else {
+        const uint32_t c0 = A.traj_ctrl_off[U.traj], nc = A.traj_ctrl_off[U.traj + 1] - c0;
+        if (piece + 2 < nc) {
+            const float4 a = A.ctrl[(size_t) (c0 + piece) * A.n_spheres + s];
+            const float4 b = A.ctrl[(size_t) (c0 + piece + 1) * A.n_spheres + s];
+            const float4 c = A.ctrl[(size_t) (c0 + piece + 2) * A.n_spheres + s];
+            U.P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), a.w);
+            U.P1 = b;
+            U.P2 = make_float4(0.5f * (b.x + c.x), 0.5f * (b.y + c.y), 0.5f * (b.z + c.z), a.w);
+        } else {
+            const uint32_t w = (piece + 2 == nc) ? w0 : w0 + nwp - 1;
+            U.P0 = A.centers[(size_t) w * A.n_spheres + s];
+            U.P1 = U.P0;
+            U.P2 = U.P0;
+        }
+    }
+    U.r = U.P0.w;
+    return true;
+}
+
+// The node-box test of a unit.  The swept sphere lies inside the capsule of
+// radius r + e around the chord P0-P2, e the chord deviation (0 for a linear
+// piece; for the Bezier piece max |C(u) - chord(u)| = |B1 - (B0 + B2)/2| / 2,
+// reached at u = 1/2); a box passes when the chord meets it grown by r + e.
+// A curved piece (e >> r) fattens that capsule sideways, so the quadratic
+// test also requires the box to meet the control points' box grown by r.
+struct SweepCull {
+    float co[3], cinv[3], fat;
+    float blo[3], bhi[3];
+};
+
+template <bool QUAD>
+__device__ __forceinline__ void make_cull(const SweepUnit& U, SweepCull& c) {
+    float e = 0.f;
+    if (QUAD) {
+        const float dx = U.P1.x - 0.5f * (U.P0.x + U.P2.x), dy = U.P1.y - 0.5f * (U.P0.y + U.P2.y),
+                    dz = U.P1.z - 0.5f * (U.P0.z + U.P2.z);
+        e = 0.5f * sqrtf(dx * dx + dy * dy + dz * dz);
+    }
+    const float4 Pe = QUAD ? U.P2 : U.P1;
+    c.co[0] = U.P0.x; c.co[1] = U.P0.y; c.co[2] = U.P0.z;
+    c.cinv[0] = chord_inv(Pe.x - U.P0.x); c.cinv[1] = chord_inv(Pe.y - U.P0.y); c.cinv[2] = chord_inv(Pe.z - U.P0.z);
+    c.fat = U.r + e + 2e-5f;
+    if (QUAD) {
+        const float pad = U.r + 2e-5f;
+        c.blo[0] = fminf(U.P0.x, fminf(U.P1.x, U.P2.x)) - pad; c.bhi[0] = fmaxf(U.P0.x, fmaxf(U.P1.x, U.P2.x)) + pad;
+        c.blo[1] = fminf(U.P0.y, fminf(U.P1.y, U.P2.y)) - pad; c.bhi[1] = fmaxf(U.P0.y, fmaxf(U.P1.y, U.P2.y)) + pad;
+        c.blo[2] = fminf(U.P0.z, fminf(U.P1.z, U.P2.z)) - pad; c.bhi[2] = fmaxf(U.P0.z, fmaxf(U.P1.z, U.P2.z)) + pad;
+    }
+}
+
+// t_enter: the chord parameter where it enters the grown box (visit order).
+template <bool QUAD>
+__device__ __forceinline__ bool cull_box(const SweepCull& c, const Box& b, float& t_enter) {
+    const float t0x = (b.lo[0] - c.fat - c.co[0]) * c.cinv[0], t1x = (b.hi[0] + c.fat - c.co[0]) * c.cinv[0];
+    const float t0y = (b.lo[1] - c.fat - c.co[1]) * c.cinv[1], t1y = (b.hi[1] + c.fat - c.co[1]) * c.cinv[1];
+    const float t0z = (b.lo[2] - c.fat - c.co[2]) * c.cinv[2], t1z = (b.hi[2] + c.fat - c.co[2]) * c.cinv[2];
+    t_enter = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+    const float t_exit = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), 1.0f));
+    bool in = t_enter <= t_exit;
+    if (QUAD) in = in && box_overlap(b, c.blo, c.bhi);
+    return in;
+}
+
+// The exact leaf test: does obstacle edge `leaf` come within r of the unit's
+// path?  FP32 with brackets; FP64 inside a narrow band around r.
+template <bool QUAD>
+__device__ __forceinline__ bool leaf_hit(const float4* __restrict__ ep, uint32_t leaf, const SweepUnit& U,
+                                         unsigned long long* stats, unsigned long long& n_roots) {
+    constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
+    const float4* e = ep + 2ull * leaf;
+    const float4 ea = __ldg(e), eb = __ldg(e + 1);
+    const V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
+    const float r = U.r;
+    float dist;
+    bool decided = false;
+    if (!QUAD) {
+        dist = sqrtf(fmaxf(seg_seg2<float>(p, q, v3cast<float>(U.P0), v3cast<float>(U.P1)), 0.f));
+    } else {
+        // C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
+        // within e of the chord B0-B2 and back, so the chord distance +- e
+        // brackets the exact distance; only the undecided middle needs roots
+        const V3<float> b0 = v3cast<float>(U.P0), b1 = v3cast<float>(U.P1), b2 = v3cast<float>(U.P2);
+        const V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
+        const float e = 0.5f * sqrtf(vdot(dv, dv));
+        const float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
+        const float tol = kBand + 1e-6f * r;
+        if (dc - e > r + tol) {  // certain miss
+            dist = dc - e;
+            decided = true;
+        } else if (dc + e < r - tol) {  // certain hit
+            dist = dc + e;
+        } else {
+            // halve the piece twice more (de Casteljau: the chord deviation of a
+            // half is a quarter), bracketing with the polyline through C(k/4)
+            const float e2 = 0.0625f * e;  // deviation of a quarter piece from its chord
+            float lo = 3.0e38f;
+            V3<float> prev = b0;
+            for (int k = 1; k <= 4; ++k) {
+                const float u = 0.25f * (float) k;
+                const V3<float> cu = vadd(vadd(vscale(b0, (1.f - u) * (1.f - u)), vscale(b1, 2.f * u * (1.f - u))),
+                                          vscale(b2, u * u));
+                lo = fminf(lo, seg_seg2<float>(p, q, prev, cu));
+                prev = cu;
+            }
+            const float dq = sqrtf(fmaxf(lo, 0.f));
+            if (dq - e2 > r + tol) {
+                dist = dq - e2;
+                decided = true;
+            } else if (dq + e2 < r - tol) {
+                dist = dq + e2;
+            } else {
+                ++n_roots;
+                dist = seg_quad_dist_f32(ea, eb, U.P0, U.P1, U.P2);
+            }
+        }
+    }
+    bool hit = dist <= r;
+    if (!decided && fabsf(dist - r) <= kBand + 1e-6f * r) {
+        atomicAdd(stats, 1ull);
+        hit = sweep_retest_f64<QUAD>(ea, eb, U.P0, U.P1, U.P2, r);
+    }
+    return hit;
+}
+
+// Light pass: one lane per unit, "while-while" (Aila and Laine 2009): lanes
+// without a unit take their next one, every lane descends to its next leaf,
+// then the warp's leaf tests run together.  A unit still open after
+// A.light_steps node and leaf visits is handed to the heavy pass (its hits
+// so far are set as flags, which are idempotent; its counts are dropped and
+// recounted there), so one lane never serialises a unit that meets thousands
+// of nodes.
 template <bool QUAD, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepArgs A) {
-    const uint32_t* __restrict__ piece_traj = A.piece_traj;
-    constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
     const float4* __restrict__ en = S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
     uint32_t st[kStack];
     int sp = 0;
     bool busy = false;
-    uint32_t traj = 0, piece_g = 0;
-    float4 P0 = make_float4(0, 0, 0, 0), P1 = P0, P2 = P0;  // linear: P0-P1 axis; quadratic: Bezier B0,B1,B2
-    float r = 0.f;
-    float blo[3] = {0.f, 0.f, 0.f}, bhi[3] = {0.f, 0.f, 0.f};
+    uint32_t cur = 0, steps = 0, u_hits = 0;
+    SweepUnit U;
+    SweepCull c;
+    U.traj = U.piece_g = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t next = blockIdx.x * blockDim.x + threadIdx.x;  // neighbouring lanes: spheres of one piece
     unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0;
+    const uint32_t budget = A.light_steps ? A.light_steps : 0xFFFFFFFFu;
 
-    // "While-while" (Aila and Laine 2009): lanes without a unit take their next
-    // one, every lane descends to its next leaf, then the warp's leaf tests run
-    // together.
     while (true) {
         while (!busy && next < A.total_units) {
             const uint32_t u = next;
             next += stride;
-            piece_g = u / A.n_spheres;
-            uint32_t s = u - piece_g * A.n_spheres;
-            traj = piece_traj[piece_g];
-            if (traj >= A.n_traj) {
+            if (!load_unit<QUAD>(A, u, U)) {
                 atomicOr(A.err, kErrRange);
                 continue;
             }
-            if (A.want_pieces ? ldflag(A.piece_hit + piece_g) && !A.want_counts
-                              : (!A.want_counts && ldflag(A.traj_hit + traj))) {
+            if (A.want_pieces ? ldflag(A.piece_hit + U.piece_g) && !A.want_counts
+                              : (!A.want_counts && ldflag(A.traj_hit + U.traj))) {
                 ++n_skip;
                 continue;
             }
-            uint32_t piece = piece_g - A.traj_piece_off[traj];
-            uint32_t w0 = A.traj_wp_off[traj], nwp = A.traj_wp_off[traj + 1] - w0;
-            if (!QUAD) {
-                P0 = A.centers[(size_t) (w0 + piece) * A.n_spheres + s];
-                P1 = A.centers[(size_t) (w0 + piece + 1) * A.n_spheres + s];
-                P2 = P1;
-            } else {
-                uint32_t c0 = A.traj_ctrl_off[traj], nc = A.traj_ctrl_off[traj + 1] - c0;
-                if (piece + 2 < nc) {
-                    float4 a = A.ctrl[(size_t) (c0 + piece) * A.n_spheres + s];
-                    float4 b = A.ctrl[(size_t) (c0 + piece + 1) * A.n_spheres + s];
-                    float4 c = A.ctrl[(size_t) (c0 + piece + 2) * A.n_spheres + s];
-                    P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), a.w);
-                    P1 = b;
-                    P2 = make_float4(0.5f * (b.x + c.x), 0.5f * (b.y + c.y), 0.5f * (b.z + c.z), a.w);
-                } else {
-                    uint32_t w = (piece + 2 == nc) ? w0 : w0 + nwp - 1;
-                    P0 = A.centers[(size_t) w * A.n_spheres + s];
-                    P1 = P0;
-                    P2 = P0;
-                }
-            }
-            r = P0.w;
-            float pad = r + 2e-5f;
-            blo[0] = fminf(P0.x, fminf(P1.x, P2.x)) - pad; bhi[0] = fmaxf(P0.x, fmaxf(P1.x, P2.x)) + pad;
-            blo[1] = fminf(P0.y, fminf(P1.y, P2.y)) - pad; bhi[1] = fmaxf(P0.y, fmaxf(P1.y, P2.y)) + pad;
-            blo[2] = fminf(P0.z, fminf(P1.z, P2.z)) - pad; bhi[2] = fmaxf(P0.z, fmaxf(P1.z, P2.z)) + pad;
             if (S.edge_root == kNone) continue;
+            make_cull<QUAD>(U, c);
             st[0] = S.edge_root;
             sp = 1;
             busy = true;
+            cur = u;
+            steps = 0;
+            u_hits = 0;
             ++n_acc;
         }
         if (!busy) break;
         uint32_t leaf = kNone;
         while (sp > 0) {
             const uint32_t ref = st[--sp];
+            ++steps;
             if (ref & kLeaf) {
                 leaf = ref & ~kLeaf;
                 break;
@@ -372,83 +500,159 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepAr
             Box bl, br;
             uint32_t rl, rr;
             load_node(en, ref, bl, br, rl, rr);
-            bool hr = box_overlap(br, blo, bhi), hl = box_overlap(bl, blo, bhi);
+            float tl, tr;
+            bool hr = cull_box<QUAD>(c, br, tr), hl = cull_box<QUAD>(c, bl, tl);
             if (sp + 2 > kStack) {
                 atomicOr(A.err, kErrStack);
                 hr = hl = false;
                 sp = 0;
             }
-            if (hr) st[sp++] = rr;
-            if (hl) st[sp++] = rl;
+            // the child met first along the chord is visited first
+            if (hr && hl && tr < tl) {
+                st[sp++] = rl;
+                st[sp++] = rr;
+            } else {
+                if (hr) st[sp++] = rr;
+                if (hl) st[sp++] = rl;
+            }
         }
         if (leaf != kNone) {
             ++n_leaf;
-            const float4* e = ep + 2ull * leaf;
-            const float4 ea = __ldg(e), eb = __ldg(e + 1);
-            const V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
-            float dist;
-            bool decided = false;
-            if (!QUAD) {
-                dist = sqrtf(fmaxf(seg_seg2<float>(p, q, v3cast<float>(P0), v3cast<float>(P1)), 0.f));
-            } else {
-                // C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
-                // within e of the chord B0-B2 and back, so the chord distance +- e
-                // brackets the exact distance; only the undecided middle needs roots
-                const V3<float> b0 = v3cast<float>(P0), b1 = v3cast<float>(P1), b2 = v3cast<float>(P2);
-                const V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
-                const float e = 0.5f * sqrtf(vdot(dv, dv));
-                const float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
-                const float tol = kBand + 1e-6f * r;
-                if (dc - e > r + tol) {  // certain miss
-                    dist = dc - e;
-                    decided = true;
-                } else if (dc + e < r - tol) {  // certain hit
-                    dist = dc + e;
-                } else {
-                    // halve the piece twice more (de Casteljau: the chord deviation of a
-                    // half is a quarter), bracketing with the polyline through C(k/4)
-                    const float e2 = 0.0625f * e;  // deviation of a quarter piece from its chord
-                    float lo = 3.0e38f;
-                    V3<float> prev = b0;
-                    for (int k = 1; k <= 4; ++k) {
-                        const float u = 0.25f * (float) k;
-                        const V3<float> cu = vadd(vadd(vscale(b0, (1.f - u) * (1.f - u)), vscale(b1, 2.f * u * (1.f - u))),
-                                                  vscale(b2, u * u));
-                        lo = fminf(lo, seg_seg2<float>(p, q, prev, cu));
-                        prev = cu;
-                    }
-                    const float dq = sqrtf(fmaxf(lo, 0.f));
-                    if (dq - e2 > r + tol) {
-                        dist = dq - e2;
-                        decided = true;
-                    } else if (dq + e2 < r - tol) {
-                        dist = dq + e2;
-                    } else {
-                        ++n_roots;
-                        dist = seg_quad_dist_f32(ea, eb, P0, P1, P2);
-                    }
-                }
-            }
-            bool hit = dist <= r;
-            if (!decided && fabsf(dist - r) <= kBand + 1e-6f * r) {
-                atomicAdd(A.stats, 1ull);
-                hit = sweep_retest_f64<QUAD>(ea, eb, P0, P1, P2, r);
-            }
-            if (hit) {
-                if (A.want_pieces) atomicExch(A.piece_hit + piece_g, 1u);
+            if (leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
+                if (A.want_pieces) atomicExch(A.piece_hit + U.piece_g, 1u);
                 if (A.want_counts) {
-                    A.traj_hit[traj] = 1u;
-                    atomicAdd(A.counts + traj, 1u);
+                    A.traj_hit[U.traj] = 1u;
+                    ++u_hits;
                 } else {
-                    atomicExch(A.traj_hit + traj, 1u);
+                    atomicExch(A.traj_hit + U.traj, 1u);
                     sp = 0;  // this unit is decided
                 }
             }
         }
-        if (sp == 0) busy = false;
+        if (sp > 0 && steps > budget) {
+            const uint32_t slot = atomicAdd(A.heavy_count, 1u);
+            if (slot < A.heavy_cap) {
+                A.heavy[slot] = cur;
+                busy = false;
+                continue;
+            }
+            steps = 0;  // the heavy list is full: finish the unit here
+        }
+        if (sp == 0) {
+            busy = false;
+            if (u_hits) atomicAdd(A.counts + U.traj, u_hits);
+        }
     }
     atomicAdd(A.stats + 1, n_acc);
     atomicAdd(A.stats + 2, n_skip);
+    atomicAdd(A.stats + 4, n_leaf);
+    atomicAdd(A.stats + 5, n_roots);
+}
+
+// Heavy pass: one warp per spilled unit.  The warp descends the obstacle-edge
+// LBVH through a shared LIFO frontier (up to 32 nodes a step, survivors
+// pushed), collects leaf survivors in a shared buffer and tests them 32 at a
+// time, one leaf per lane.  The unit's serial depth drops from its node count
+// to about its node count / 32 plus the tree depth.
+constexpr int kHeavyWarps = 4;
+constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
+
+template <bool QUAD>
+__global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev S, const SweepArgs A) {
+    __shared__ uint32_t s_front[kHeavyWarps][kFrontier];
+    __shared__ uint32_t s_leaf[kHeavyWarps][kLeafBuf];
+    const int lane = threadIdx.x & 31;
+    uint32_t* fr = s_front[threadIdx.x >> 5];
+    uint32_t* lf = s_leaf[threadIdx.x >> 5];
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t n_heavy = min(*A.heavy_count, A.heavy_cap);
+    unsigned long long n_leaf = 0, n_roots = 0;
+    while (true) {
+        uint32_t h = 0;
+        if (lane == 0) h = atomicAdd(A.heavy_work, 1u);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (h >= n_heavy) break;
+        SweepUnit U;
+        if (!load_unit<QUAD>(A, A.heavy[h], U)) {
+            if (lane == 0) atomicOr(A.err, kErrRange);
+            continue;
+        }
+        SweepCull c;
+        make_cull<QUAD>(U, c);
+        if (lane == 0) fr[0] = S.edge_root;
+        __syncwarp();
+        int sp = 1, nl = 0, step = 0;
+        uint32_t hits = 0;
+        while (true) {
+            if (nl >= 32 || (sp == 0 && nl > 0)) {  // leaf step
+                const int take = min(nl, 32);
+                nl -= take;
+                const uint32_t leaf = lane < take ? lf[nl + lane] : kNone;
+                __syncwarp();
+                bool hit = false;
+                if (leaf != kNone) {
+                    ++n_leaf;
+                    hit = leaf_hit<QUAD>(S.edge_prims, leaf, U, A.stats, n_roots);
+                }
+                const uint32_t mh = __ballot_sync(0xffffffffu, hit);
+                if (mh) {
+                    if (lane == 0) {
+                        if (A.want_pieces) atomicExch(A.piece_hit + U.piece_g, 1u);
+                        if (A.want_counts) {
+                            A.traj_hit[U.traj] = 1u;
+                            hits += __popc(mh);
+                        } else {
+                            atomicExch(A.traj_hit + U.traj, 1u);
+                        }
+                    }
+                    if (!A.want_counts) break;
+                }
+                continue;
+            }
+            if (sp == 0) break;
+            if (!A.want_counts && (++step & 7) == 0) {  // decided meanwhile by another unit?
+                uint32_t dec = 0;
+                if (lane == 0) dec = A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj);
+                if (__shfl_sync(0xffffffffu, dec, 0)) break;
+            }
+            const int take = min(sp, 32);
+            sp -= take;
+            const uint32_t ref = lane < take ? fr[sp + lane] : kNone;
+            __syncwarp();
+            bool hl = false, hr = false;
+            uint32_t rl = kNone, rr = kNone;
+            if (ref != kNone) {
+                if (ref & kLeaf) {  // a one-edge scene: the root itself is a leaf
+                    hl = true;
+                    rl = ref;
+                } else {
+                    Box bl, br;
+                    float t;
+                    load_node(S.edge_nodes, ref, bl, br, rl, rr);
+                    hl = cull_box<QUAD>(c, bl, t);
+                    hr = cull_box<QUAD>(c, br, t);
+                }
+            }
+            const bool pl = hl && !(rl & kLeaf), pr = hr && !(rr & kLeaf);
+            const bool el = hl && (rl & kLeaf), er = hr && (rr & kLeaf);
+            const uint32_t mpl = __ballot_sync(0xffffffffu, pl), mpr = __ballot_sync(0xffffffffu, pr);
+            const uint32_t mel = __ballot_sync(0xffffffffu, el), mer = __ballot_sync(0xffffffffu, er);
+            const int npush = __popc(mpl) + __popc(mpr);
+            if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
+                if (lane == 0) atomicOr(A.err, kErrStack);
+                break;
+            }
+            if (pl) fr[sp + __popc(mpl & lt)] = rl;
+            if (pr) fr[sp + __popc(mpl) + __popc(mpr & lt)] = rr;
+            sp += npush;
+            if (el) lf[nl + __popc(mel & lt)] = rl & ~kLeaf;
+            if (er) lf[nl + __popc(mel) + __popc(mer & lt)] = rr & ~kLeaf;
+            nl += __popc(mel) + __popc(mer);
+            __syncwarp();
+        }
+        if (lane == 0 && hits) atomicAdd(A.counts + U.traj, hits);
+        __syncwarp();
+    }
     atomicAdd(A.stats + 4, n_leaf);
     atomicAdd(A.stats + 5, n_roots);
 }
@@ -472,21 +676,39 @@ uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads) {
 uint32_t sweep_persistent_blocks(bool quad) { return sweep_max_blocks_per_sm(quad, kTravThreads) * device_sm_count(); }
 
 template <bool QUAD>
-static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s) {
+static uint32_t heavy_blocks() {
+    static uint32_t blocks = 0;
+    if (!blocks) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD>, kHeavyWarps * 32, 0);
+        blocks = (uint32_t) std::max(1, per_sm) * device_sm_count();
+    }
+    return blocks;
+}
+
+template <bool QUAD>
+static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads,
+                           uint32_t heavy_share, cudaStream_t s) {
     if (threads == 64)
         k_sweep<QUAD, 64><<<blocks, 64, 0, s>>>(S, A);
     else if (threads == 256)
         k_sweep<QUAD, 256><<<blocks, 256, 0, s>>>(S, A);
     else
         k_sweep<QUAD, 128><<<blocks, 128, 0, s>>>(S, A);
+    cuda_check(cudaGetLastError(), "k_sweep");
+    if (A.light_steps) {
+        const uint32_t hb = std::max(1u, heavy_blocks<QUAD>() * heavy_share / 100);
+        k_sweep_heavy<QUAD><<<hb, kHeavyWarps * 32, 0, s>>>(S, A);
+        cuda_check(cudaGetLastError(), "k_sweep_heavy");
+    }
 }
 
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, cudaStream_t s) {
+void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, uint32_t heavy_share,
+                  cudaStream_t s) {
     if (A.quad)
-        sweep_dispatch<true>(S, A, blocks, threads, s);
+        sweep_dispatch<true>(S, A, blocks, threads, heavy_share, s);
     else
-        sweep_dispatch<false>(S, A, blocks, threads, s);
-    cuda_check(cudaGetLastError(), "k_sweep");
+        sweep_dispatch<false>(S, A, blocks, threads, heavy_share, s);
 }
 
 }  // namespace rtcd

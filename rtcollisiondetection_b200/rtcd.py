@@ -59,7 +59,8 @@ class RobotDesc(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
-                ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('reserved', C.c_uint32 * 3)]
+                ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('sweep_light_steps', C.c_uint32),
+                ('reserved', C.c_uint32 * 2)]
 
 
 class Stats(C.Structure):
@@ -259,7 +260,8 @@ def segment_offsets(kind, traj_off, flags=0):
 class Detector:
     """One detector of one kind over a robot and a scene."""
 
-    def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0):
+    def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
+                 stream_priority=0, residency_percent=0, sweep_light_steps=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -267,6 +269,9 @@ class Detector:
         cfg.frame_size = frame_size
         cfg.traverse_threads = traverse_threads
         cfg.traverse_blocks_per_sm = traverse_blocks_per_sm
+        cfg.stream_priority = stream_priority
+        cfg.residency_percent = residency_percent
+        cfg.sweep_light_steps = sweep_light_steps
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -318,7 +323,7 @@ class Detector:
         _ok(lib().rtcd_detector_autotune(self.h, _ptr(q_dev, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
                                          C.c_void_p(stream) if stream else None, C.byref(best), C.byref(ms)))
         return {'traverse_threads': best.traverse_threads, 'traverse_blocks_per_sm': best.traverse_blocks_per_sm,
-                'traverse_ms': ms.value}
+                'sweep_light_steps': best.sweep_light_steps, 'traverse_ms': ms.value}
 
     def stats(self):
         s = Stats()
@@ -408,7 +413,8 @@ class ServerStats(C.Structure):
                 ('units_completed', C.c_uint64), ('batches', C.c_uint64), ('inflight_bytes_peak', C.c_uint64),
                 ('queue_depth', C.c_uint32), ('reserved0', C.c_uint32), ('p50_ms', C.c_double),
                 ('p99_ms', C.c_double), ('mean_ms', C.c_double), ('max_ms', C.c_double),
-                ('reserved', C.c_uint64 * 4)]
+                ('queue_p50_ms', C.c_double), ('queue_p99_ms', C.c_double), ('run_p99_ms', C.c_double),
+                ('reserved', C.c_uint64 * 1)]
 
 
 class Server:
