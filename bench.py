@@ -462,9 +462,9 @@ def main():
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
-        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_a, k_stage_b, k_discrete (overflow), k_flags;
-        # sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2 (trajectories, segments)
-        'gpu_launches': args.steps * (7 if not sweep else (5 if cfg['kind'] == 'Linear' else 6)),
+        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_a, k_stage_b, k_stage_b_heavy, k_discrete
+        # (overflow), k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
+        'gpu_launches': args.steps * (8 if not sweep else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in trav])),
                       'cull': float(np.mean([s['ms_cull'] for s in trav])), 'traverse': t_trav},
         'roofline': {'bound': 'hbm', 'kernel': 'k_sweep' if sweep else 'k_discrete', 'achieved': achieved,

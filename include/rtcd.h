@@ -103,9 +103,10 @@ typedef struct {
     int32_t stream_priority;         /* priority of the detector's own stream (CUDA convention: lower = higher) */
     uint32_t residency_percent;      /* share of each SM its persistent kernels may hold (room for other
                                         launches to run alongside); 0 = 100 */
-    uint32_t sweep_light_steps;      /* sweeps: node + leaf visits one lane spends on a (piece, sphere) unit
-                                        before a whole warp takes the unit over; 0 = 32 linear / 16 quadratic,
-                                        0xFFFFFFFF = never */
+    uint32_t light_steps;            /* node + leaf visits one lane spends on a unit of traversal work (a
+                                        discrete (link item, scene primitive) candidate, a sweep (piece,
+                                        sphere) unit) before a whole warp takes it over; 0 = 32 (16 for
+                                        the quadratic sweep), 0xFFFFFFFF = never */
     uint32_t reserved[2];
 } rtcd_config;
 
@@ -171,8 +172,8 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
 /* Autotuner: runs the given device-resident batch (q_dev; traj_offsets on the
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
- * that fit, and for the sweep detectors each at a light-pass budget of 16, 32
- * and 64 visits (sweeps are timed with segment flags on) - times the
+ * that fit, each at a light-pass budget (light_steps) of 16, 32 and 64
+ * visits (sweeps are timed with segment flags on) - times the
  * traversal with device events (median of
  * three after a warm-up run), keeps the fastest shape in the detector and
  * writes it to best_out (optional).  The upstream picks its batch size per
@@ -185,6 +186,14 @@ RTCD_API rtcd_status rtcd_detector_autotune(rtcd_detector* det, const float* q_d
  * offsets_out (n + 1 entries, host) is the exclusive prefix sum. */
 RTCD_API rtcd_status rtcd_segment_offsets(rtcd_detector_kind kind, const uint32_t* traj_offsets, uint32_t n, uint32_t flags,
                                  uint32_t* offsets_out);
+
+/* Host-side least-squares quadratic B-spline fit: W_out (n_ctrl x n_wp,
+ * row-major) = pinv(B), B[t][k] the uniform unclamped quadratic basis on knots
+ * 0..n_ctrl+2 sampled at u = linspace(2, n_ctrl, n_wp).  Replaces loading the
+ * shipped tables RTCD/data/weights/quad/normal/{nC}_{nT}.txt
+ * (RTCD/Robot/batchCurveRobot.h:560-605); the quadratic detector fits with
+ * n_ctrl = max(3, ceil(n_wp/2)).  Needs no GPU. */
+RTCD_API rtcd_status rtcd_quad_fit_weights(uint32_t n_ctrl, uint32_t n_wp, float* W_out);
 
 /* Statistics of the last completed check: items after the cull, etc. */
 typedef struct {

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -289,6 +290,11 @@ struct rtcd_detector {
     HostBuf pin_in, pin_out, pin_aux;
     uint64_t last_items = 0, last_culled = 0;
 };
+
+namespace {
+void ensure_weights(rtcd_detector* d, uint32_t max_wp);
+extern const uint32_t kWeightsPrebuilt;
+}  // namespace
 
 static rtcd_status finish(const std::exception_ptr& ep) {
     try {
@@ -632,6 +638,7 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         d->count.ensure(4);
         cuda_check(cudaMemset(d->err.p, 0, 4), "memset");
         cuda_check(cudaMemset(d->stats.p, 0, 64), "memset");
+        if (kind == RTCD_QUAD_SWEEP) ensure_weights(d.get(), kWeightsPrebuilt);
         *out = d.release();
     });
 }
@@ -684,8 +691,13 @@ uint32_t pieces_of(rtcd_detector_kind kind, uint32_t n_wp, uint32_t flags) {
 // Least-squares quadratic B-spline fit W = (B^T B)^{-1} B^T (nc x nt), with B
 // the uniform unclamped quadratic basis sampled at u = linspace(2, nc, nt);
 // the shipped weight tables (RTCD/data/weights/quad/normal/) are this matrix.
+// Each row of B has three consecutive nonzeros, so G = B^T B is pentadiagonal
+// and its Cholesky factor has two subdiagonals: the factor and the nt solves
+// touch only the band (the entries a dense factorisation would compute outside
+// it are exact zeros, so the result is the same).
 std::vector<double> fit_weights(uint32_t nc, uint32_t nt) {
-    std::vector<double> B((size_t) nt * nc, 0.0), G((size_t) nc * nc, 0.0), W((size_t) nc * nt, 0.0);
+    constexpr uint32_t kBand = 2;
+    std::vector<double> B((size_t) nt * nc, 0.0), W((size_t) nc * nt, 0.0);
     for (uint32_t t = 0; t < nt; ++t) {
         double x = nt > 1 ? 2.0 + (double) (nc - 2) * t / (nt - 1) : 2.0;
         int seg = std::min<int>((int) std::floor(x) - 2, (int) nc - 3);
@@ -695,52 +707,73 @@ std::vector<double> fit_weights(uint32_t nc, uint32_t nt) {
         B[(size_t) t * nc + seg + 1] += 0.5 + s - s * s;
         B[(size_t) t * nc + seg + 2] += 0.5 * s * s;
     }
+    // L[i][i - k], k = 0..2, in G's band
+    std::vector<double> L((size_t) nc * (kBand + 1), 0.0);
+    auto Lr = [&](uint32_t i, uint32_t j) -> double& { return L[(size_t) i * (kBand + 1) + (i - j)]; };
     for (uint32_t i = 0; i < nc; ++i)
-        for (uint32_t j = 0; j < nc; ++j) {
+        for (uint32_t j = (i >= kBand ? i - kBand : 0); j <= i; ++j) {
             double acc = 0;
             for (uint32_t t = 0; t < nt; ++t) acc += B[(size_t) t * nc + i] * B[(size_t) t * nc + j];
-            G[(size_t) i * nc + j] = acc;
+            Lr(i, j) = acc;
         }
-    // Cholesky G = L L^T (in place, lower)
     for (uint32_t j = 0; j < nc; ++j) {
-        double dg = G[(size_t) j * nc + j];
-        for (uint32_t k = 0; k < j; ++k) dg -= G[(size_t) j * nc + k] * G[(size_t) j * nc + k];
+        double dg = Lr(j, j);
+        for (uint32_t k = (j >= kBand ? j - kBand : 0); k < j; ++k) dg -= Lr(j, k) * Lr(j, k);
         if (dg <= 0) fail(RTCD_ERR_INVALID_ARGUMENT, "spline fit is singular");
         dg = std::sqrt(dg);
-        G[(size_t) j * nc + j] = dg;
-        for (uint32_t i = j + 1; i < nc; ++i) {
-            double v = G[(size_t) i * nc + j];
-            for (uint32_t k = 0; k < j; ++k) v -= G[(size_t) i * nc + k] * G[(size_t) j * nc + k];
-            G[(size_t) i * nc + j] = v / dg;
+        Lr(j, j) = dg;
+        for (uint32_t i = j + 1; i < nc && i <= j + kBand; ++i) {
+            double v = Lr(i, j);
+            for (uint32_t k = (i >= kBand ? i - kBand : 0); k < j; ++k) v -= Lr(i, k) * Lr(j, k);
+            Lr(i, j) = v / dg;
         }
     }
     std::vector<double> y(nc);
     for (uint32_t t = 0; t < nt; ++t) {
         for (uint32_t i = 0; i < nc; ++i) {
             double v = B[(size_t) t * nc + i];
-            for (uint32_t k = 0; k < i; ++k) v -= G[(size_t) i * nc + k] * y[k];
-            y[i] = v / G[(size_t) i * nc + i];
+            for (uint32_t k = (i >= kBand ? i - kBand : 0); k < i; ++k) v -= Lr(i, k) * y[k];
+            y[i] = v / Lr(i, i);
         }
         for (int i = (int) nc - 1; i >= 0; --i) {
             double v = y[i];
-            for (uint32_t k = i + 1; k < nc; ++k) v -= G[(size_t) k * nc + i] * y[k];
-            y[i] = v / G[(size_t) i * nc + i];
+            for (uint32_t k = i + 1; k < nc && k <= (uint32_t) i + kBand; ++k) v -= Lr(k, i) * y[k];
+            y[i] = v / Lr(i, i);
         }
         for (uint32_t i = 0; i < nc; ++i) W[(size_t) i * nt + t] = y[i];
     }
     return W;
 }
 
+// Process-wide cache of the FP32 tables by waypoint count (they depend on n only).
+const std::vector<float>& weight_table(uint32_t n) {
+    static std::mutex mu;
+    static std::map<uint32_t, std::vector<float>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(n);
+    if (it != cache.end()) return it->second;
+    std::vector<float> f;
+    if (n >= 3) {
+        auto W = fit_weights(quad_ctrl_count(n), n);
+        f.assign(W.begin(), W.end());
+    }
+    return cache.emplace(n, std::move(f)).first->second;
+}
+
+// Tables for every waypoint count up to max_wp on the device.  Growth is
+// geometric (the stream is synchronised before the buffer is replaced), and
+// detectors start with tables up to kWeightsPrebuilt waypoints.
+extern const uint32_t kWeightsPrebuilt = 128;
+
 void ensure_weights(rtcd_detector* d, uint32_t max_wp) {
     if (max_wp <= d->W_max) return;
+    max_wp = std::max(max_wp, d->W_max + d->W_max / 2);
     if (d->W_off_host.empty()) d->W_off_host.assign(1, 0);
     d->W_off_host.resize(max_wp + 2, 0);
     for (uint32_t n = d->W_max + 1; n <= max_wp; ++n) {
         d->W_off_host[n] = (uint32_t) d->W_host.size();
-        if (n >= 3) {
-            auto W = fit_weights(quad_ctrl_count(n), n);
-            for (double v : W) d->W_host.push_back((float) v);
-        }
+        const std::vector<float>& w = weight_table(n);
+        d->W_host.insert(d->W_host.end(), w.begin(), w.end());
     }
     d->W_max = max_wp;
     cuda_check(cudaStreamSynchronize(d->stream), "weights sync");
@@ -793,7 +826,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         if (!cnt) return;
         blocks = (cnt + kTravThreads - 1) / kTravThreads;
     }
-    cuda_check(cudaMemsetAsync(d->work.p, 0, 4, s), "memset");
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 8, s), "memset");
     const bool fused = (flags & RTCD_CHECK_FUSED) != 0;
     DiscreteArgs A{};
     A.T = d->T.as<float4>();
@@ -830,9 +863,21 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         W.item_overflow = d->item_overflow.as<uint8_t>();
         W.overflow_items = d->overflow_items.as<uint32_t>();
         W.overflow_count = wc + 1;
+        W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
+                        : d->cfg.light_steps                ? d->cfg.light_steps
+                                                                  : 32u;
+        if (W.light_steps) {
+            const uint32_t hcap = std::min<uint32_t>(cap, 1u << 24);
+            d->heavy.ensure(4ull * hcap);
+            W.heavy = d->heavy.as<uint32_t>();
+            W.heavy_cap = hcap;
+            W.heavy_count = wc + 3;
+            W.heavy_work = d->work.as<uint32_t>() + 1;
+        }
         uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
-        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, s);
+        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads,
+                       d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
         DiscreteArgs F = A;
         F.items = d->overflow_items.as<uint32_t>();
         F.n_items = wc + 1;
@@ -1010,11 +1055,12 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.stats = d->stats.as<unsigned long long>();
     A.want_counts = counts;
     A.want_pieces = want_pieces;
-    A.light_steps = d->cfg.sweep_light_steps == 0xFFFFFFFFu ? 0u
-                    : d->cfg.sweep_light_steps                ? d->cfg.sweep_light_steps
+    A.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
+                    : d->cfg.light_steps                ? d->cfg.light_steps
                                                               : (quad ? 16u : 32u);
     if (A.light_steps) {
-        const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns / 4, 1024), 1u << 22);
+        // room for every unit (near dense geometry most units of a piece can spill)
+        const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns, 1024), 1u << 24);
         d->heavy.ensure(4ull * cap);
         A.heavy = d->heavy.as<uint32_t>();
         A.heavy_cap = cap;
@@ -1208,8 +1254,7 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         const rtcd_config saved = d->cfg;
         rtcd_config best = saved;
         float best_t = 3.0e38f;
-        const std::vector<uint32_t> lights = discrete ? std::vector<uint32_t>{saved.sweep_light_steps}
-                                                      : std::vector<uint32_t>{16u, 32u, 64u};
+        const std::vector<uint32_t> lights = {16u, 32u, 64u};
         for (uint32_t light : lights)
         for (uint32_t t : {64u, 128u, 256u}) {
             uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
@@ -1219,7 +1264,7 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
             for (uint32_t per_sm : shapes) {
                 d->cfg.traverse_threads = t;
                 d->cfg.traverse_blocks_per_sm = per_sm;
-                d->cfg.sweep_light_steps = light;
+                d->cfg.light_steps = light;
                 apply_launch_shape(d);
                 float ms[4];
                 for (int rep = 0; rep < 4; ++rep) {
@@ -1245,6 +1290,15 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         apply_launch_shape(d);
         if (best_out) *best_out = best;
         if (best_ms) *best_ms = best_t;
+    });
+}
+
+rtcd_status rtcd_quad_fit_weights(uint32_t n_ctrl, uint32_t n_wp, float* W_out) {
+    return guarded([&] {
+        RTCD_REQUIRE(W_out, "NULL argument");
+        RTCD_REQUIRE(n_ctrl >= 3 && n_wp >= n_ctrl, "need 3 <= n_ctrl <= n_wp");
+        const std::vector<double> W = fit_weights(n_ctrl, n_wp);
+        for (size_t i = 0; i < W.size(); ++i) W_out[i] = (float) W[i];
     });
 }
 

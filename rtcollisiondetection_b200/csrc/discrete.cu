@@ -596,110 +596,163 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
     }
 }
 
-// Stage B: one lane per candidate (grid-stride, so neighbouring lanes take
-// neighbouring candidates of the same item): move the scene primitive into
-// the link frame, reject it against the link OBB, descend the link LBVH and
-// run the exact segment-triangle test at the leaves.  A candidate carries its
-// (pose, link) item word, so one whose pose is already decided costs two
-// loads.
+// Stage B works on one candidate (item, scene primitive) at a time: move the
+// scene primitive into the link frame, reject it against the link OBB,
+// descend the link LBVH and run the exact segment-triangle test at the leaves.
+struct StageBCand {
+    float4 T[3];
+    f3 c0, c1, c2, cn, cinv;  // primitive in the link frame; triangle normal (R2O) / 1 / segment (O2R)
+    float cw;                 // plane offset n.c0 (R2O)
+    float blo[3], bhi[3];     // triangle box (R2O)
+    uint32_t pose, lroot, prim;
+};
+
+// 0: nothing to do (blank, decided, overflowed item, empty link, OBB reject); 1: descend.
+// Every outcome but "decided" is a function of the inputs alone, so a warp
+// that sets up one candidate on all lanes (check_decided false) agrees.
+template <bool R2O>
+__device__ __forceinline__ int stage_b_setup(const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint2 cd,
+                                             StageBCand& C, unsigned long long& n_skip, unsigned long long& n_rej,
+                                             bool check_decided = true) {
+    constexpr float kBoxTol = 2e-5f;
+    const DiscreteArgs& A = W.d;
+    if (cd.x == kNone) return 0;  // blank slot of an overflowed emission
+    const uint32_t item = cd.x;
+    const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
+    if (check_decided && !A.want_counts && ld_flag(A.pose_hit + pose)) {
+        ++n_skip;
+        return 0;
+    }
+    if (W.item_overflow[item]) return 0;  // the fused kernel re-runs this item
+    C.lroot = R2O ? R.edge_root[link] : R.tri_root[link];
+    if (C.lroot == kNone) return 0;
+    C.pose = pose;
+    C.prim = cd.y;
+    const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+    C.T[0] = tp[0]; C.T[1] = tp[1]; C.T[2] = tp[2];
+    const float* lo = R.obb[link];
+    const f3 oc = mk(lo[0], lo[1], lo[2]);
+    const f3 u0 = mk(lo[6], lo[7], lo[8]), u1 = mk(lo[9], lo[10], lo[11]), u2 = mk(lo[12], lo[13], lo[14]);
+    const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
+    C.c2 = C.cn = C.cinv = mk(0.f, 0.f, 0.f);
+    C.cw = 0.f;
+    if (R2O) {
+        const float4* t = wp + 3ull * cd.y;
+        C.c0 = xf_inv(C.T, f3of(__ldg(t)));
+        C.c1 = xf_inv(C.T, f3of(__ldg(t + 1)));
+        C.c2 = xf_inv(C.T, f3of(__ldg(t + 2)));
+        C.cn = cross(C.c1 - C.c0, C.c2 - C.c0);
+        C.cw = dot(C.cn, C.c0);
+        const float rr = (lo[3] + kBoxTol) * fabsf(dot(C.cn, u0)) + (lo[4] + kBoxTol) * fabsf(dot(C.cn, u1)) +
+                         (lo[5] + kBoxTol) * fabsf(dot(C.cn, u2));
+        if (fabsf(dot(C.cn, oc) - C.cw) > rr) {
+            ++n_rej;
+            return 0;
+        }
+        C.blo[0] = fminf(C.c0.x, fminf(C.c1.x, C.c2.x)) - kBoxTol; C.bhi[0] = fmaxf(C.c0.x, fmaxf(C.c1.x, C.c2.x)) + kBoxTol;
+        C.blo[1] = fminf(C.c0.y, fminf(C.c1.y, C.c2.y)) - kBoxTol; C.bhi[1] = fmaxf(C.c0.y, fmaxf(C.c1.y, C.c2.y)) + kBoxTol;
+        C.blo[2] = fminf(C.c0.z, fminf(C.c1.z, C.c2.z)) - kBoxTol; C.bhi[2] = fmaxf(C.c0.z, fmaxf(C.c1.z, C.c2.z)) + kBoxTol;
+    } else {
+        const float4* e = wp + 2ull * cd.y;
+        C.c0 = xf_inv(C.T, f3of(__ldg(e)));
+        C.c1 = xf_inv(C.T, f3of(__ldg(e + 1)));
+        const f3 d = C.c1 - C.c0;
+        C.cinv = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+        const f3 pr = C.c0 - oc;
+        const f3 po = mk(dot(pr, u0), dot(pr, u1), dot(pr, u2));
+        const f3 dd = mk(dot(d, u0), dot(d, u1), dot(d, u2));
+        Box obl;
+        obl.lo[0] = -lo[3]; obl.lo[1] = -lo[4]; obl.lo[2] = -lo[5];
+        obl.hi[0] = lo[3]; obl.hi[1] = lo[4]; obl.hi[2] = lo[5];
+        if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), obl, kBoxTol)) {
+            ++n_rej;
+            return 0;
+        }
+    }
+    return 1;
+}
+
+// Node test: the box overlaps the triangle's box and straddles its plane
+// (R2O), or the segment passes through the box (O2R).
+template <bool R2O>
+__device__ __forceinline__ bool stage_b_node(const StageBCand& C, const Box& b) {
+    constexpr float kBoxTol = 2e-5f;
+    if (R2O) return box_overlap(b, C.blo, C.bhi) && plane_box(C.cn, C.cw, b, kBoxTol);
+    return seg_box(C.c0, C.cinv, b, kBoxTol);
+}
+
+// Exact test of link primitive li against the candidate: FP32 with the FP64
+// re-test of the undecided band.
+template <bool R2O>
+__device__ __forceinline__ bool stage_b_leaf(const float4* __restrict__ lp, const float4* __restrict__ wp,
+                                             uint32_t li, const StageBCand& C, unsigned long long* stats) {
+    f3 p, q, a, b, c;
+    if (R2O) {
+        const float4* e = lp + 2ull * li;
+        p = f3of(__ldg(e)); q = f3of(__ldg(e + 1));
+        a = C.c0; b = C.c1; c = C.c2;
+    } else {
+        const float4* t = lp + 3ull * li;
+        p = C.c0; q = C.c1;
+        a = f3of(__ldg(t)); b = f3of(__ldg(t + 1)); c = f3of(__ldg(t + 2));
+    }
+    int r = seg_tri_f32(p, q, a, b, c);
+    if (r == 2) {
+        atomicAdd(stats, 1ull);
+        r = retest_f64<R2O>(C.T, lp, li, wp, C.prim) ? 1 : 0;
+    }
+    return r == 1;
+}
+
+// Stage B, light pass: one lane per candidate (grid-stride, so neighbouring
+// lanes take neighbouring candidates of the same item).  A candidate still
+// open after W.light_steps node and leaf visits goes to the heavy pass (hits
+// already found stay: pose flags and edge bits are idempotent; ObsToRobot
+// hit counts are added only when the candidate finishes here).  A candidate
+// carries its (pose, link) item word, so one whose pose is already decided
+// costs two loads.
 template <bool R2O, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const SceneDev S, const WaveArgs W) {
-    constexpr float kBoxTol = 2e-5f;
     const DiscreteArgs& A = W.d;
     const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
     const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
     const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
     const uint32_t total = min(*W.cand_count, W.cand_cap);
+    const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
     uint32_t st[kStack];
     unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
-        const uint2 cd = W.cand[c];
-        if (cd.x == kNone) continue;  // blank slot of an overflowed emission
-        const uint32_t item = cd.x;
-        const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
-        if (!A.want_counts && ld_flag(A.pose_hit + pose)) {
-            ++n_skip;
-            continue;
-        }
-        if (W.item_overflow[item]) continue;  // the fused kernel re-runs this item
-        const uint32_t lroot = R2O ? R.edge_root[link] : R.tri_root[link];
-        if (lroot == kNone) continue;
-        float4 T[3];
-        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
-        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
-        const float* lo = R.obb[link];
-        const f3 oc = mk(lo[0], lo[1], lo[2]);
-        const f3 u0 = mk(lo[6], lo[7], lo[8]), u1 = mk(lo[9], lo[10], lo[11]), u2 = mk(lo[12], lo[13], lo[14]);
-        f3 c0, c1, c2 = mk(0.f, 0.f, 0.f), cn = mk(0.f, 0.f, 0.f), cinv = mk(0.f, 0.f, 0.f);
-        float cw = 0.f;
-        float blo[3], bhi[3];
-        if (R2O) {
-            const float4* t = wp + 3ull * cd.y;
-            c0 = xf_inv(T, f3of(__ldg(t)));
-            c1 = xf_inv(T, f3of(__ldg(t + 1)));
-            c2 = xf_inv(T, f3of(__ldg(t + 2)));
-            cn = cross(c1 - c0, c2 - c0);
-            cw = dot(cn, c0);
-            float rr = (lo[3] + kBoxTol) * fabsf(dot(cn, u0)) + (lo[4] + kBoxTol) * fabsf(dot(cn, u1)) +
-                       (lo[5] + kBoxTol) * fabsf(dot(cn, u2));
-            if (fabsf(dot(cn, oc) - cw) > rr) {
-                ++n_rej;
-                continue;
-            }
-            blo[0] = fminf(c0.x, fminf(c1.x, c2.x)) - kBoxTol; bhi[0] = fmaxf(c0.x, fmaxf(c1.x, c2.x)) + kBoxTol;
-            blo[1] = fminf(c0.y, fminf(c1.y, c2.y)) - kBoxTol; bhi[1] = fmaxf(c0.y, fmaxf(c1.y, c2.y)) + kBoxTol;
-            blo[2] = fminf(c0.z, fminf(c1.z, c2.z)) - kBoxTol; bhi[2] = fmaxf(c0.z, fmaxf(c1.z, c2.z)) + kBoxTol;
-        } else {
-            const float4* e = wp + 2ull * cd.y;
-            c0 = xf_inv(T, f3of(__ldg(e)));
-            c1 = xf_inv(T, f3of(__ldg(e + 1)));
-            const f3 d = c1 - c0;
-            cinv = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
-            const f3 pr = c0 - oc;
-            const f3 po = mk(dot(pr, u0), dot(pr, u1), dot(pr, u2));
-            const f3 dd = mk(dot(d, u0), dot(d, u1), dot(d, u2));
-            Box obl;
-            obl.lo[0] = -lo[3]; obl.lo[1] = -lo[4]; obl.lo[2] = -lo[5];
-            obl.hi[0] = lo[3]; obl.hi[1] = lo[4]; obl.hi[2] = lo[5];
-            if (!seg_box(po, mk(safe_inv(dd.x), safe_inv(dd.y), safe_inv(dd.z)), obl, kBoxTol)) {
-                ++n_rej;
-                continue;
-            }
-        }
+        StageBCand C;
+        if (!stage_b_setup<R2O>(R, S, W, W.cand[c], C, n_skip, n_rej)) continue;
         ++n_acc;
         int sp = 0;
-        st[sp++] = lroot;
+        st[sp++] = C.lroot;
+        uint32_t steps = 0, hits = 0;
         while (sp > 0) {
+            if (++steps > budget) {
+                const uint32_t slot = atomicAdd(W.heavy_count, 1u);
+                if (slot < W.heavy_cap) {
+                    W.heavy[slot] = c;
+                    hits = 0;
+                    break;
+                }
+                steps = 0;  // the heavy list is full: finish the candidate here
+            }
             const uint32_t ref = st[--sp];
             if (ref & kLeaf) {
                 ++n_leaf;
                 const uint32_t li = ref & ~kLeaf;
-                f3 p, q, a, b, c;
-                if (R2O) {
-                    const float4* e = lp + 2ull * li;
-                    p = f3of(__ldg(e)); q = f3of(__ldg(e + 1));
-                    a = c0; b = c1; c = c2;
-                } else {
-                    const float4* t = lp + 3ull * li;
-                    p = c0; q = c1;
-                    a = f3of(__ldg(t)); b = f3of(__ldg(t + 1)); c = f3of(__ldg(t + 2));
-                }
-                int r = seg_tri_f32(p, q, a, b, c);
-                if (r == 2) {
-                    atomicAdd(A.stats, 1ull);
-                    r = retest_f64<R2O>(T, lp, li, wp, cd.y) ? 1 : 0;
-                }
-                if (r == 1) {
+                if (stage_b_leaf<R2O>(lp, wp, li, C, A.stats)) {
                     if (!A.want_counts) {
-                        atomicExch(A.pose_hit + pose, 1u);
+                        atomicExch(A.pose_hit + C.pose, 1u);
                         break;
                     }
-                    A.pose_hit[pose] = 1u;
+                    A.pose_hit[C.pose] = 1u;
                     if (R2O) {
                         const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
-                        atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
+                        atomicOr(A.edge_bits + (size_t) C.pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
                     } else {
-                        atomicAdd(A.counts + pose, 1u);
+                        ++hits;
                     }
                 }
                 continue;
@@ -707,14 +760,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
             Box bl, br;
             uint32_t rl, rr;
             load_node(ln, ref, bl, br, rl, rr);
-            bool hr, hl;
-            if (R2O) {
-                hr = box_overlap(br, blo, bhi) && plane_box(cn, cw, br, kBoxTol);
-                hl = box_overlap(bl, blo, bhi) && plane_box(cn, cw, bl, kBoxTol);
-            } else {
-                hr = seg_box(c0, cinv, br, kBoxTol);
-                hl = seg_box(c0, cinv, bl, kBoxTol);
-            }
+            const bool hr = stage_b_node<R2O>(C, br), hl = stage_b_node<R2O>(C, bl);
             if (sp + 2 > kStack) {
                 atomicOr(A.err, kErrStack);
                 break;
@@ -722,11 +768,124 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
             if (hr) st[sp++] = rr;
             if (hl) st[sp++] = rl;
         }
+        if (hits) atomicAdd(A.counts + C.pose, hits);
     }
-    atomicAdd(A.stats + 1, n_acc);
-    atomicAdd(A.stats + 2, n_skip);
-    atomicAdd(A.stats + 3, n_rej);
-    atomicAdd(A.stats + 4, n_leaf);
+    warp_count(A.stats + 1, n_acc);
+    warp_count(A.stats + 2, n_skip);
+    warp_count(A.stats + 3, n_rej);
+    warp_count(A.stats + 4, n_leaf);
+}
+
+// Stage B, heavy pass: one warp per spilled candidate.  The warp descends the
+// link LBVH through a shared LIFO frontier (up to 32 nodes a step) and tests
+// the surviving leaves 32 at a time, one per lane.
+constexpr int kHeavyWarps = 4;
+constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
+
+template <bool R2O>
+__global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotDev R, const SceneDev S,
+                                                                   const WaveArgs W) {
+    __shared__ uint32_t s_front[kHeavyWarps][kFrontier];
+    __shared__ uint32_t s_leaf[kHeavyWarps][kLeafBuf];
+    const DiscreteArgs& A = W.d;
+    const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
+    const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
+    const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
+    const int lane = threadIdx.x & 31;
+    uint32_t* fr = s_front[threadIdx.x >> 5];
+    uint32_t* lf = s_leaf[threadIdx.x >> 5];
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t n_heavy = min(*W.heavy_count, W.heavy_cap);
+    unsigned long long n_skip = 0, n_rej = 0, n_leaf = 0;
+    while (true) {
+        uint32_t h = 0;
+        if (lane == 0) h = atomicAdd(W.heavy_work, 1u);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (h >= n_heavy) break;
+        StageBCand C;
+        if (!stage_b_setup<R2O>(R, S, W, W.cand[W.heavy[h]], C, n_skip, n_rej, false)) continue;  // warp-uniform
+        if (!A.want_counts) {  // decided meanwhile? (one lane reads, all follow)
+            uint32_t dec = 0;
+            if (lane == 0) dec = ld_flag(A.pose_hit + C.pose);
+            if (__shfl_sync(0xffffffffu, dec, 0)) continue;
+        }
+        if (lane == 0) fr[0] = C.lroot;
+        __syncwarp();
+        int sp = 1, nl = 0, step = 0;
+        uint32_t hits = 0;
+        while (true) {
+            if (nl >= 32 || (sp == 0 && nl > 0)) {  // leaf step
+                const int take = min(nl, 32);
+                nl -= take;
+                const uint32_t li = lane < take ? lf[nl + lane] : kNone;
+                __syncwarp();
+                bool hit = false;
+                if (li != kNone) {
+                    ++n_leaf;
+                    hit = stage_b_leaf<R2O>(lp, wp, li, C, A.stats);
+                }
+                const uint32_t mh = __ballot_sync(0xffffffffu, hit);
+                if (mh) {
+                    if (!A.want_counts) {
+                        if (lane == 0) atomicExch(A.pose_hit + C.pose, 1u);
+                        break;
+                    }
+                    if (lane == 0) A.pose_hit[C.pose] = 1u;
+                    if (R2O) {
+                        if (hit) {
+                            const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
+                            atomicOr(A.edge_bits + (size_t) C.pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
+                        }
+                    } else {
+                        hits += __popc(mh);
+                    }
+                }
+                continue;
+            }
+            if (sp == 0) break;
+            if (!A.want_counts && (++step & 7) == 0) {  // decided meanwhile by another candidate?
+                uint32_t dec = 0;
+                if (lane == 0) dec = ld_flag(A.pose_hit + C.pose);
+                if (__shfl_sync(0xffffffffu, dec, 0)) break;
+            }
+            const int take = min(sp, 32);
+            sp -= take;
+            const uint32_t ref = lane < take ? fr[sp + lane] : kNone;
+            __syncwarp();
+            bool hl = false, hr = false;
+            uint32_t rl = kNone, rr = kNone;
+            if (ref != kNone) {
+                if (ref & kLeaf) {  // a one-primitive link: the root itself is a leaf
+                    hl = true;
+                    rl = ref;
+                } else {
+                    Box bl, br;
+                    load_node(ln, ref, bl, br, rl, rr);
+                    hl = stage_b_node<R2O>(C, bl);
+                    hr = stage_b_node<R2O>(C, br);
+                }
+            }
+            const bool pl = hl && !(rl & kLeaf), pr = hr && !(rr & kLeaf);
+            const bool el = hl && (rl & kLeaf), er = hr && (rr & kLeaf);
+            const uint32_t mpl = __ballot_sync(0xffffffffu, pl), mpr = __ballot_sync(0xffffffffu, pr);
+            const uint32_t mel = __ballot_sync(0xffffffffu, el), mer = __ballot_sync(0xffffffffu, er);
+            const int npush = __popc(mpl) + __popc(mpr);
+            if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
+                if (lane == 0) atomicOr(A.err, kErrStack);
+                break;
+            }
+            if (pl) fr[sp + __popc(mpl & lt)] = rl;
+            if (pr) fr[sp + __popc(mpl) + __popc(mpr & lt)] = rr;
+            sp += npush;
+            if (el) lf[nl + __popc(mel & lt)] = rl & ~kLeaf;
+            if (er) lf[nl + __popc(mel) + __popc(mer & lt)] = rr & ~kLeaf;
+            nl += __popc(mel) + __popc(mer);
+            __syncwarp();
+        }
+        if (lane == 0 && hits) atomicAdd(A.counts + C.pose, hits);
+        __syncwarp();
+    }
+    warp_count(A.stats + 4, n_leaf);
 }
 
 template <class K>
@@ -778,12 +937,22 @@ static void stage_b_dispatch(const RobotDev& R, const SceneDev& S, const WaveArg
 }
 
 void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                    uint32_t threads, cudaStream_t s) {
+                    uint32_t threads, uint32_t heavy_share, cudaStream_t s) {
     if (r2o)
         stage_b_dispatch<true>(R, S, W, blocks, threads, s);
     else
         stage_b_dispatch<false>(R, S, W, blocks, threads, s);
     cuda_check(cudaGetLastError(), "k_stage_b");
+    if (W.light_steps) {
+        static const uint32_t full_r2o = grid_for(k_stage_b_heavy<true>, kHeavyWarps * 32);
+        static const uint32_t full_o2r = grid_for(k_stage_b_heavy<false>, kHeavyWarps * 32);
+        const uint32_t hb = std::max(1u, (r2o ? full_r2o : full_o2r) * heavy_share / 100);
+        if (r2o)
+            k_stage_b_heavy<true><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
+        else
+            k_stage_b_heavy<false><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
+        cuda_check(cudaGetLastError(), "k_stage_b_heavy");
+    }
 }
 
 uint32_t discrete_persistent_blocks(bool robot_to_obs) {

@@ -38,6 +38,15 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, uint
     cr = __float_as_uint(d.y);
 }
 
+// Adds a per-lane count to a device counter with one atomic per warp, none
+// when the warp's total is zero (per-thread atomics on one address at the
+// end of a large grid serialise in L2 for a noticeable time).  Every lane of
+// the warp must call it; per-lane counts fit 32 bits.
+__device__ __forceinline__ void warp_count(unsigned long long* p, unsigned long long v) {
+    const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned) v);
+    if ((threadIdx.x & 31) == 0 && total) atomicAdd(p, (unsigned long long) total);
+}
+
 __device__ __forceinline__ bool box_overlap(const Box& b, const float* lo, const float* hi) {
     return !(lo[0] > b.hi[0] || hi[0] < b.lo[0] || lo[1] > b.hi[1] || hi[1] < b.lo[1] || lo[2] > b.hi[2] ||
              hi[2] < b.lo[2]);

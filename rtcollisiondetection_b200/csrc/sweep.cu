@@ -543,10 +543,10 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepAr
             if (u_hits) atomicAdd(A.counts + U.traj, u_hits);
         }
     }
-    atomicAdd(A.stats + 1, n_acc);
-    atomicAdd(A.stats + 2, n_skip);
-    atomicAdd(A.stats + 4, n_leaf);
-    atomicAdd(A.stats + 5, n_roots);
+    warp_count(A.stats + 1, n_acc);
+    warp_count(A.stats + 2, n_skip);
+    warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 5, n_roots);
 }
 
 // Heavy pass: one warp per spilled unit.  The warp descends the obstacle-edge
@@ -653,8 +653,8 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
         if (lane == 0 && hits) atomicAdd(A.counts + U.traj, hits);
         __syncwarp();
     }
-    atomicAdd(A.stats + 4, n_leaf);
-    atomicAdd(A.stats + 5, n_roots);
+    warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 5, n_roots);
 }
 
 template <bool QUAD>

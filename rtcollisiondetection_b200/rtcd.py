@@ -38,7 +38,7 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
            'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
-           'rtcd_select_flags_u8_noalloc']
+           'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights']
 
 
 class RTCDError(RuntimeError):
@@ -59,7 +59,7 @@ class RobotDesc(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
-                ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('sweep_light_steps', C.c_uint32),
+                ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('light_steps', C.c_uint32),
                 ('reserved', C.c_uint32 * 2)]
 
 
@@ -139,6 +139,13 @@ def exclusive_scan_u32(ctx, in_dev, out_dev, n, total_dev=None, stream=None):
 def select_flags_u8(ctx, mask_dev, n, idx_dev, count_dev, stream=None):
     _ok(lib().rtcd_select_flags_u8(ctx.h, _ptr(mask_dev, C.c_uint8), C.c_uint32(n), _ptr(idx_dev, C.c_uint32),
                                    _ptr(count_dev, C.c_uint32), C.c_void_p(stream) if stream else None))
+
+
+def quad_fit_weights(n_ctrl, n_wp):
+    """The quadratic B-spline least-squares fit W (n_ctrl x n_wp), computed by the library (host only)."""
+    out = np.zeros((n_ctrl, n_wp), np.float32)
+    _ok(lib().rtcd_quad_fit_weights(C.c_uint32(n_ctrl), C.c_uint32(n_wp), _ptr(out, C.c_float)))
+    return out
 
 
 def robot_fk(robot, q_dev, n, T_dev, stream=None):
@@ -261,7 +268,7 @@ class Detector:
     """One detector of one kind over a robot and a scene."""
 
     def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
-                 stream_priority=0, residency_percent=0, sweep_light_steps=0):
+                 stream_priority=0, residency_percent=0, light_steps=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -271,7 +278,7 @@ class Detector:
         cfg.traverse_blocks_per_sm = traverse_blocks_per_sm
         cfg.stream_priority = stream_priority
         cfg.residency_percent = residency_percent
-        cfg.sweep_light_steps = sweep_light_steps
+        cfg.light_steps = light_steps
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -323,7 +330,7 @@ class Detector:
         _ok(lib().rtcd_detector_autotune(self.h, _ptr(q_dev, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
                                          C.c_void_p(stream) if stream else None, C.byref(best), C.byref(ms)))
         return {'traverse_threads': best.traverse_threads, 'traverse_blocks_per_sm': best.traverse_blocks_per_sm,
-                'sweep_light_steps': best.sweep_light_steps, 'traverse_ms': ms.value}
+                'light_steps': best.light_steps, 'traverse_ms': ms.value}
 
     def stats(self):
         s = Stats()

@@ -49,3 +49,19 @@ def test_segment_offsets_host_only():
         assert False
     except rtcd.RTCDError as e:
         assert e.status == 1
+
+
+def test_library_weight_fit_matches_shipped_tables():
+    """Host-only: the library's banded least-squares fit reproduces every
+    shipped RTCD/data/weights/quad/normal table (the golden fixtures)."""
+    import numpy as np
+    g = np.load(os.path.join(ROOT, 'tests', 'golden', 'quad_weights.npz'))
+    for k in g.files:
+        nc, nt = map(int, k[2:].split('_'))
+        W = rtcd.quad_fit_weights(nc, nt)
+        assert np.abs(W - g[k]).max() < 2e-6, k
+    try:
+        rtcd.quad_fit_weights(2, 8)
+        assert False
+    except rtcd.RTCDError as e:
+        assert e.status == 1
