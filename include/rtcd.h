@@ -107,7 +107,13 @@ typedef struct {
                                         discrete (link item, scene primitive) candidate, a sweep (piece,
                                         sphere) unit) before a whole warp takes it over; 0 = 32 (16 for
                                         the quadratic sweep), 0xFFFFFFFF = never */
-    uint32_t reserved[2];
+    uint32_t stage_b_form;           /* discrete stage B: 1 = one lane per candidate, 2 = 32-candidate packets
+                                        that share each link-BVH node load; 0 = lanes for RobotToObs,
+                                        packets for ObsToRobot (the autotuner tries both) */
+    uint32_t stage_b_chunk;          /* discrete stage B: consecutive candidates one lane takes in order (lanes
+                                        form) or 32-candidate groups one warp takes (packets); a pose's
+                                        candidates then spread over few workers that stop at its first hit;
+                                        0 = 64 lanes / 4 packets; at most 4096 */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -172,10 +178,11 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
 /* Autotuner: runs the given device-resident batch (q_dev; traj_offsets on the
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
- * that fit, each at a light-pass budget (light_steps) of 16, 32 and 64
- * visits (sweeps are timed with segment flags on) - times the
- * traversal with device events (median of
- * three after a warm-up run), keeps the fastest shape in the detector and
+ * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
+ * then, for the discrete kinds, both stage B forms at chunk lengths from 1 to
+ * 256 candidates (coordinate descent; sweeps are timed with segment flags on)
+ * - times the traversal with device events (median of three after a
+ * warm-up run), keeps the fastest configuration in the detector and
  * writes it to best_out (optional).  The upstream picks its batch size per
  * experiment by hand (CollisionDetector.h:365-394). */
 RTCD_API rtcd_status rtcd_detector_autotune(rtcd_detector* det, const float* q_dev, const uint32_t* traj_offsets,

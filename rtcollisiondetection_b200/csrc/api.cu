@@ -341,6 +341,8 @@ static void apply_launch_shape(rtcd_detector* d) {
     uint32_t per_sm = d->cfg.traverse_blocks_per_sm ? std::min(d->cfg.traverse_blocks_per_sm, fit) : fit;
     const uint32_t pct = d->cfg.residency_percent;
     if (pct > 100) fail(RTCD_ERR_INVALID_ARGUMENT, "residency_percent must be at most 100");
+    if (d->cfg.stage_b_form > 2) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_form must be 0, 1 or 2");
+    if (d->cfg.stage_b_chunk > 4096) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_chunk must be at most 4096");
     const uint32_t sms = (uint32_t) device_sm_count();
     if (pct) per_sm = std::max(1u, per_sm * pct / 100);
     d->threads = t;
@@ -863,6 +865,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         W.item_overflow = d->item_overflow.as<uint8_t>();
         W.overflow_items = d->overflow_items.as<uint32_t>();
         W.overflow_count = wc + 1;
+        W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (r2o ? 64u : 4u);
         W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                         : d->cfg.light_steps                ? d->cfg.light_steps
                                                                   : 32u;
@@ -877,7 +880,8 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
         launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads,
-                       d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
+                       d->cfg.residency_percent ? d->cfg.residency_percent : 100,
+                       d->cfg.stage_b_form == 2 || (d->cfg.stage_b_form == 0 && !r2o), s);
         DiscreteArgs F = A;
         F.items = d->overflow_items.as<uint32_t>();
         F.n_items = wc + 1;
@@ -1254,37 +1258,57 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         const rtcd_config saved = d->cfg;
         rtcd_config best = saved;
         float best_t = 3.0e38f;
-        const std::vector<uint32_t> lights = {16u, 32u, 64u};
-        for (uint32_t light : lights)
+        // median of three timed runs after a warm-up run
+        auto time_cfg = [&](const rtcd_config& c) {
+            d->cfg = c;
+            apply_launch_shape(d);
+            float ms[4];
+            for (int rep = 0; rep < 4; ++rep) {
+                rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(),
+                                            discrete ? nullptr : seg.as<uint8_t>(), nullptr, RTCD_CHECK_TIMING, s);
+                rtcd_stats stt;
+                if (st == RTCD_OK) st = rtcd_last_stats(d, &stt);
+                if (st != RTCD_OK) {
+                    d->cfg = saved;
+                    apply_launch_shape(d);
+                    fail(st, g_last_error);
+                }
+                ms[rep] = stt.ms_traverse;
+            }
+            std::sort(ms + 1, ms + 4);
+            if (ms[2] < best_t) {
+                best_t = ms[2];
+                best = c;
+            }
+        };
+        // coordinate descent: the launch shape, then the light-pass budget,
+        // then (discrete) the stage B form and its chunk length
         for (uint32_t t : {64u, 128u, 256u}) {
             uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
                                     : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
             std::vector<uint32_t> shapes = {std::max(1u, fit / 4), std::max(1u, fit / 2), fit};
             shapes.erase(std::unique(shapes.begin(), shapes.end()), shapes.end());
             for (uint32_t per_sm : shapes) {
-                d->cfg.traverse_threads = t;
-                d->cfg.traverse_blocks_per_sm = per_sm;
-                d->cfg.light_steps = light;
-                apply_launch_shape(d);
-                float ms[4];
-                for (int rep = 0; rep < 4; ++rep) {
-                    rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(),
-                                                discrete ? nullptr : seg.as<uint8_t>(), nullptr, RTCD_CHECK_TIMING, s);
-                    rtcd_stats stt;
-                    if (st == RTCD_OK) st = rtcd_last_stats(d, &stt);
-                    if (st != RTCD_OK) {
-                        d->cfg = saved;
-                        apply_launch_shape(d);
-                        fail(st, g_last_error);
-                    }
-                    ms[rep] = stt.ms_traverse;
-                }
-                std::sort(ms + 1, ms + 4);
-                if (ms[2] < best_t) {
-                    best_t = ms[2];
-                    best = d->cfg;
-                }
+                rtcd_config c = saved;
+                c.traverse_threads = t;
+                c.traverse_blocks_per_sm = per_sm;
+                time_cfg(c);
             }
+        }
+        for (uint32_t light : {16u, 32u, 64u}) {
+            rtcd_config c = best;
+            c.light_steps = light;
+            time_cfg(c);
+        }
+        if (discrete) {
+            const rtcd_config base = best;
+            for (uint32_t form : {1u, 2u})
+                for (uint32_t chunk : {1u, 16u, 64u, 256u}) {
+                    rtcd_config c = base;
+                    c.stage_b_form = form;
+                    c.stage_b_chunk = form == 2 ? std::max(1u, chunk / 16) : chunk;
+                    time_cfg(c);
+                }
         }
         d->cfg = best;
         apply_launch_shape(d);

@@ -721,7 +721,13 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
     const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
     uint32_t st[kStack];
     unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < total; c += gridDim.x * blockDim.x) {
+    // each lane takes up to W.chunk consecutive candidates in order: a pose's
+    // candidates spread over a few lanes that each stop at its first hit,
+    // instead of over many lanes that all start before any hit is known.
+    // A batch smaller than the grid keeps one candidate per lane (latency).
+    const uint32_t K = max(1u, min(W.chunk, total / (gridDim.x * blockDim.x)));
+    for (uint32_t cc = (blockIdx.x * blockDim.x + threadIdx.x) * K; cc < total; cc += gridDim.x * blockDim.x * K)
+    for (uint32_t c = cc; c < min(cc + K, total); ++c) {
         StageBCand C;
         if (!stage_b_setup<R2O>(R, S, W, W.cand[c], C, n_skip, n_rej)) continue;
         ++n_acc;
@@ -776,6 +782,121 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
     warp_count(A.stats + 4, n_leaf);
 }
 
+// Stage B, light pass in packets: a warp takes 32 consecutive candidates and
+// splits them by item (stage A emits each item's candidates in contiguous
+// runs, so a group is one item or a few).  The lanes of one item share the
+// link LBVH and the pose: they descend it together as a packet - one node
+// load per step for the whole warp, each lane testing the node against its
+// own scene primitive, the node visited when any lane needs it - and test
+// each reached leaf against their own primitives in one converged step.
+// A packet still open after 4 * W.light_steps steps hands its candidates to
+// the heavy pass.
+template <bool R2O, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, const SceneDev S, const WaveArgs W) {
+    const DiscreteArgs& A = W.d;
+    const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
+    const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
+    const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
+    const uint32_t total = min(*W.cand_count, W.cand_cap);
+    const uint32_t budget = W.light_steps ? 4u * W.light_steps : 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t n_groups = (total + 31) / 32;
+    const uint32_t warps = gridDim.x * (BLOCK / 32);
+    uint32_t st[kStack];
+    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
+    const uint32_t K = max(1u, min(W.chunk, n_groups / warps));  // consecutive groups per warp, in order
+    for (uint32_t gg = (blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5)) * K; gg < n_groups; gg += warps * K)
+    for (uint32_t g = gg; g < min(gg + K, n_groups); ++g) {
+        const uint32_t c = g * 32 + lane;
+        StageBCand C;
+        uint2 cd = make_uint2(kNone, kNone);
+        bool live = false;
+        if (c < total) {
+            cd = W.cand[c];
+            live = stage_b_setup<R2O>(R, S, W, cd, C, n_skip, n_rej) != 0;
+        }
+        if (live) ++n_acc;
+        const uint32_t same = __match_any_sync(0xffffffffu, live ? cd.x : kNone);
+        uint32_t pending = __ballot_sync(0xffffffffu, live);
+        while (pending) {
+            const int leader = __ffs(pending) - 1;
+            const uint32_t grp = __shfl_sync(0xffffffffu, same, leader) & pending;
+            pending &= ~grp;
+            const bool in = (grp >> lane) & 1u;
+            const uint32_t pose = __shfl_sync(0xffffffffu, C.pose, leader);
+            int sp = 0;
+            st[sp++] = __shfl_sync(0xffffffffu, C.lroot, leader);
+            uint32_t steps = 0, hits = 0;
+            bool spilled = false;
+            while (sp > 0) {
+                if (++steps > budget) {
+                    const uint32_t n = __popc(grp);
+                    uint32_t base = 0;
+                    if (lane == leader) base = atomicAdd(W.heavy_count, n);
+                    base = __shfl_sync(0xffffffffu, base, leader);
+                    if (base + n <= W.heavy_cap) {
+                        if (in) W.heavy[base + __popc(grp & lt)] = c;
+                        spilled = true;
+                        break;
+                    }
+                    // the heavy list is full: blank the reserved slots below the
+                    // capacity (the heavy pass reads up to it) and finish here
+                    if (in && base + __popc(grp & lt) < W.heavy_cap) W.heavy[base + __popc(grp & lt)] = kNone;
+                    steps = 0;
+                }
+                if (!A.want_counts && (steps & 15) == 0) {  // decided meanwhile by another candidate?
+                    uint32_t dec = 0;
+                    if (lane == leader) dec = ld_flag(A.pose_hit + pose);
+                    if (__shfl_sync(0xffffffffu, dec, leader)) break;
+                }
+                const uint32_t ref = st[--sp];
+                if (ref & kLeaf) {
+                    const uint32_t li = ref & ~kLeaf;
+                    bool hit = false;
+                    if (in) {
+                        ++n_leaf;
+                        hit = stage_b_leaf<R2O>(lp, wp, li, C, A.stats);
+                    }
+                    const uint32_t hm = __ballot_sync(0xffffffffu, hit);
+                    if (hm) {
+                        if (!A.want_counts) {
+                            if (lane == leader) atomicExch(A.pose_hit + pose, 1u);
+                            break;
+                        }
+                        if (lane == leader) A.pose_hit[pose] = 1u;
+                        if (hit) {
+                            if (R2O) {
+                                const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
+                                atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
+                            } else {
+                                ++hits;
+                            }
+                        }
+                    }
+                    continue;
+                }
+                Box bl, br;
+                uint32_t rl, rr;
+                load_node(ln, ref, bl, br, rl, rr);
+                const bool hr = in && stage_b_node<R2O>(C, br), hl = in && stage_b_node<R2O>(C, bl);
+                const bool any_r = __any_sync(0xffffffffu, hr), any_l = __any_sync(0xffffffffu, hl);
+                if (sp + 2 > kStack) {
+                    if (lane == leader) atomicOr(A.err, kErrStack);
+                    break;
+                }
+                if (any_r) st[sp++] = rr;
+                if (any_l) st[sp++] = rl;
+            }
+            if (hits && !spilled) atomicAdd(A.counts + pose, hits);
+        }
+    }
+    warp_count(A.stats + 1, n_acc);
+    warp_count(A.stats + 2, n_skip);
+    warp_count(A.stats + 3, n_rej);
+    warp_count(A.stats + 4, n_leaf);
+}
+
 // Stage B, heavy pass: one warp per spilled candidate.  The warp descends the
 // link LBVH through a shared LIFO frontier (up to 32 nodes a step) and tests
 // the surviving leaves 32 at a time, one per lane.
@@ -802,8 +923,10 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotD
         if (lane == 0) h = atomicAdd(W.heavy_work, 1u);
         h = __shfl_sync(0xffffffffu, h, 0);
         if (h >= n_heavy) break;
+        const uint32_t ci = W.heavy[h];
+        if (ci == kNone) continue;  // a blanked slot of a reservation that did not fit
         StageBCand C;
-        if (!stage_b_setup<R2O>(R, S, W, W.cand[W.heavy[h]], C, n_skip, n_rej, false)) continue;  // warp-uniform
+        if (!stage_b_setup<R2O>(R, S, W, W.cand[ci], C, n_skip, n_rej, false)) continue;  // warp-uniform
         if (!A.want_counts) {  // decided meanwhile? (one lane reads, all follow)
             uint32_t dec = 0;
             if (lane == 0) dec = ld_flag(A.pose_hit + C.pose);
@@ -927,7 +1050,16 @@ void launch_stage_a(bool r2o, const RobotDev& R, const SceneDev& S, const WaveAr
 
 template <bool R2O>
 static void stage_b_dispatch(const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                             uint32_t threads, cudaStream_t s) {
+                             uint32_t threads, bool packets, cudaStream_t s) {
+    if (packets) {
+        if (threads == 64)
+            k_stage_b_packet<R2O, 64><<<blocks, 64, 0, s>>>(R, S, W);
+        else if (threads == 256)
+            k_stage_b_packet<R2O, 256><<<blocks, 256, 0, s>>>(R, S, W);
+        else
+            k_stage_b_packet<R2O, 128><<<blocks, 128, 0, s>>>(R, S, W);
+        return;
+    }
     if (threads == 64)
         k_stage_b<R2O, 64><<<blocks, 64, 0, s>>>(R, S, W);
     else if (threads == 256)
@@ -937,11 +1069,11 @@ static void stage_b_dispatch(const RobotDev& R, const SceneDev& S, const WaveArg
 }
 
 void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                    uint32_t threads, uint32_t heavy_share, cudaStream_t s) {
+                    uint32_t threads, uint32_t heavy_share, bool packets, cudaStream_t s) {
     if (r2o)
-        stage_b_dispatch<true>(R, S, W, blocks, threads, s);
+        stage_b_dispatch<true>(R, S, W, blocks, threads, packets, s);
     else
-        stage_b_dispatch<false>(R, S, W, blocks, threads, s);
+        stage_b_dispatch<false>(R, S, W, blocks, threads, packets, s);
     cuda_check(cudaGetLastError(), "k_stage_b");
     if (W.light_steps) {
         static const uint32_t full_r2o = grid_for(k_stage_b_heavy<true>, kHeavyWarps * 32);

@@ -66,6 +66,7 @@ struct WaveArgs {
     uint8_t* item_overflow;    // [item word] set when its candidates overflowed; zeroed before stage A
     uint32_t* overflow_items;  // compacted overflowed items (item words, for the fused kernel)
     uint32_t* overflow_count;  // zeroed before stage A
+    uint32_t chunk;            // stage B: consecutive candidates (lanes) or 32-candidate groups (packets) per worker
     uint32_t light_steps;      // stage B visits before a candidate moves to the heavy pass; 0 = no heavy pass
     uint32_t* heavy;           // [heavy_cap] candidate indices handed to the heavy pass
     uint32_t heavy_cap;
@@ -78,10 +79,11 @@ constexpr int kFrontier = 32 * (kStack + 2);  // bound of a 32-wide LIFO frontie
 
 void launch_stage_a(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                     cudaStream_t s);
-// Stage B's light pass on `blocks` x `threads`, then (when W.light_steps) its
-// heavy pass on heavy_share percent of the full persistent grid.
+// Stage B's light pass (32-candidate packets, or one lane per candidate) on
+// `blocks` x `threads`, then (when W.light_steps) its heavy pass on
+// heavy_share percent of the full persistent grid.
 void launch_stage_b(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                    uint32_t threads, uint32_t heavy_share, cudaStream_t s);
+                    uint32_t threads, uint32_t heavy_share, bool packets, cudaStream_t s);
 uint32_t stage_a_blocks(bool robot_to_obs);
 uint32_t stage_b_blocks(bool robot_to_obs);
 uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256

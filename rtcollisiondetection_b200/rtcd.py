@@ -60,7 +60,7 @@ class RobotDesc(C.Structure):
 class Config(C.Structure):
     _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
                 ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('light_steps', C.c_uint32),
-                ('reserved', C.c_uint32 * 2)]
+                ('stage_b_form', C.c_uint32), ('stage_b_chunk', C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -268,7 +268,7 @@ class Detector:
     """One detector of one kind over a robot and a scene."""
 
     def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
-                 stream_priority=0, residency_percent=0, light_steps=0):
+                 stream_priority=0, residency_percent=0, light_steps=0, stage_b_form=0, stage_b_chunk=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -279,6 +279,8 @@ class Detector:
         cfg.stream_priority = stream_priority
         cfg.residency_percent = residency_percent
         cfg.light_steps = light_steps
+        cfg.stage_b_form = stage_b_form
+        cfg.stage_b_chunk = stage_b_chunk
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -330,7 +332,8 @@ class Detector:
         _ok(lib().rtcd_detector_autotune(self.h, _ptr(q_dev, C.c_float), _ptr(traj_off, C.c_uint32), C.c_uint32(n),
                                          C.c_void_p(stream) if stream else None, C.byref(best), C.byref(ms)))
         return {'traverse_threads': best.traverse_threads, 'traverse_blocks_per_sm': best.traverse_blocks_per_sm,
-                'light_steps': best.light_steps, 'traverse_ms': ms.value}
+                'light_steps': best.light_steps, 'stage_b_form': best.stage_b_form,
+                'stage_b_chunk': best.stage_b_chunk, 'traverse_ms': ms.value}
 
     def stats(self):
         s = Stats()
