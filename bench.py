@@ -74,7 +74,7 @@ def make_inputs(cfg, rank, scenes):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons, sampled every 20 ms."""
 
     FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
@@ -86,10 +86,14 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
-                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                          '--format=csv,noheader,nounits', '-lms', '20'],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 3.0:   # sampling is running before the timed region
+                time.sleep(0.01)
+            self.rows.clear()
         except OSError:
             self.proc = None
 
@@ -273,6 +277,42 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
     return out
 
 
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal: SMs x FP32 lanes x FMA x max SM clock
+
+
+def fp32_work(cfg, model, mesh, spheres, q, off, scene, t_trav_ms, sample=256):
+    """FP32 work of the reference algorithm for this batch, from the FP64 oracle's
+    canonical-LBVH counters on a sample (full traversal, no early exit, no OBB
+    cull - an upper bound), weighted 18 flops per node slab test, 40 per
+    segment-triangle, 45 per segment-capsule, 200 per segment-quadratic test,
+    72 per link of FK and 36 per moved edge; scaled to the batch and divided
+    by the traversal span."""
+    from oracle import oracle as O
+    robot = O.Robot(model, spheres=spheres)
+    oscene = O.Scene(mesh)
+    links = model['cos_mask'].shape[0] + 1
+    if cfg['kind'] in ('RobotToObs', 'ObsToRobot'):
+        k = O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT
+        idx = np.linspace(0, len(q) - 1, min(sample, len(q))).astype(int)
+        w = O.discrete(k, robot, oscene, q[idx], work=True)
+        edges = int(model['link_edge_off'][-1] - model['link_edge_off'][1]) if k == O.ROBOT_TO_OBS else 0
+        per_unit = (18.0 * w['node_tests'].mean() + 40.0 * w['prim_tests'].mean() + 72.0 * links + 36.0 * edges)
+        units = len(q)
+    else:
+        m = min(len(off) - 1, sample // 4)
+        w = O.sweep(cfg['kind'] == 'Quadratic', robot, oscene, q[:off[m]], off[:m + 1], work=True)
+        wpt = float(off[m]) / m
+        per_unit = (18.0 * w['node_tests'].mean() + (200.0 if cfg['kind'] == 'Quadratic' else 45.0)
+                    * w['prim_tests'].mean() + 72.0 * links * wpt)
+        units = len(off) - 1
+    tflops = per_unit * units / (t_trav_ms / 1e3) / 1e12
+    return {'rate': tflops, 'unit': 'TFLOP/s', 'flops_per_unit': per_unit,
+            'note': 'the reference algorithm (every edge ray traversed to the end) would need this many flops at '
+                    'this speed; early exit and the OBB cull skip most of it, so it can exceed the peak',
+            'sample': 'oracle counters over %d of %d units' % (len(idx) if cfg['kind'] in ('RobotToObs', 'ObsToRobot')
+                                                              else m, units)}
+
+
 def run_reference(args, cfg, rank, world):
     from rtcollisiondetection_b200 import scenes
     if rank != 0:
@@ -443,16 +483,43 @@ def main():
 
     peaks, peak_src = load_peaks()
     t_trav = float(np.mean([s['ms_traverse'] for s in trav]))
-    # algorithmic bytes of one traversal launch: poses in, flags out, the resident structures read once
+    # algorithmic bytes of one traversal span: poses in, flags out, the resident structures read once
     if sweep:
         bytes_alg = n * 4 + int(q.nbytes) + 32 * scene.n_edges * 3
     else:
         bytes_alg = n * (4 * model['cos_mask'].shape[0] + 1) + (64 + 48) * scene.n_tris + (64 + 32) * 35991
     achieved = bytes_alg / (t_trav / 1e3) / 1e9
+    form = tuned.get('stage_b_form', 0)
+    if sweep:
+        span = 'k_sweep + k_sweep_heavy'
+    elif form in (0, 3):
+        span = 'k_stage_ab + k_stage_b_heavy + k_discrete (overflow)'
+    else:
+        span = 'k_stage_a + k_stage_b%s + k_stage_b_heavy + k_discrete (overflow)' % ('_packet' if form == 2 else '')
     traffic = None
     tp = os.path.join(ROOT, 'profiles', 'traffic.json')
     if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(args.config)
+        t = json.load(open(tp)).get(args.config)
+        if t and t.get('span') == span:
+            traffic = t['bytes_per_span']
+    # FP32 work the kernels did, from their own counters (mean over the timed steps)
+    links = model['cos_mask'].shape[0] + 1
+    nodes = float(np.mean([s['node_tests'] for s in trav]))
+    leaves = float(np.mean([s['exact_tests'] for s in trav]))
+    if sweep:
+        w_ours = 18 * nodes + (200 if cfg['kind'] == 'Quadratic' else 45) * leaves + 72 * links * float(off[-1])
+    else:
+        cands = float(np.mean([s['candidates'] for s in trav]))
+        w_ours = (18 * nodes + 40 * leaves + 36 * cands + 180 * n * (links - 1) * scene.n_obstacles
+                  + 72 * links * n)
+    fp32 = {'achieved': w_ours / (t_trav / 1e3) / 1e12, 'peak': FP32_PEAK_TFLOPS, 'unit': 'TFLOP/s',
+            'frac': w_ours / (t_trav / 1e3) / 1e12 / FP32_PEAK_TFLOPS, 'flops_per_step': w_ours,
+            'node_tests': nodes, 'leaf_tests': leaves,
+            'peak_source': 'nominal (148 SMs x 128 lanes x 2 x 1.965 GHz)',
+            'weights': 'flops per op: node slab/box test 18, segment-triangle 40, segment-capsule 45, '
+                       'segment-quadratic 200, OBB SAT pair 180, FK link 72, primitive transform 36'}
+    if not args.no_check:
+        fp32['reference_work'] = fp32_work(cfg, model, mesh, spheres, q, off, scene, t_trav)
     line = {
         'metric': METRIC, 'value': value, 'unit': unit, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
@@ -462,15 +529,19 @@ def main():
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
-        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_a, k_stage_b, k_stage_b_heavy, k_discrete
-        # (overflow), k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
-        'gpu_launches': args.steps * (8 if not sweep else (5 if cfg['kind'] == 'Linear' else 6)),
+        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_ab (fused form) or k_stage_a + k_stage_b,
+        # k_stage_b_heavy, k_discrete (overflow), k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep,
+        # k_sweep_heavy, k_flags x 2
+        'gpu_launches': args.steps * ((7 if tuned.get('stage_b_form', 0) in (0, 3) else 8) if not sweep
+                                      else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in trav])),
                       'cull': float(np.mean([s['ms_cull'] for s in trav])), 'traverse': t_trav},
-        'roofline': {'bound': 'hbm', 'kernel': 'k_sweep' if sweep else 'k_discrete', 'achieved': achieved,
+        'roofline': {'bound': 'hbm', 'kernel': span, 'achieved': achieved,
                      'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved / peaks['hbm_gbs'],
-                     'traffic': traffic, 'peak_source': peak_src,
-                     'note': 'latency-bound tree traversal: HBM is not the binding resource'},
+                     'traffic': traffic, 'peak_source': peak_src, 'fp32': fp32,
+                     'note': 'latency-bound tree traversal: HBM is not the binding resource; achieved = algorithmic '
+                             'bytes / traversal span (CUDA events on the launching stream); traffic = ncu DRAM '
+                             'read+write of the span\'s kernels (profiles/traffic.json)'},
         'clocks': clocks,
     }
     if plain:

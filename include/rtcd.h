@@ -108,8 +108,9 @@ typedef struct {
                                         sphere) unit) before a whole warp takes it over; 0 = 32 (16 for
                                         the quadratic sweep), 0xFFFFFFFF = never */
     uint32_t stage_b_form;           /* discrete stage B: 1 = one lane per candidate, 2 = 32-candidate packets
-                                        that share each link-BVH node load; 0 = lanes for RobotToObs,
-                                        packets for ObsToRobot (the autotuner tries both) */
+                                        that share each link-BVH node load, 3 = stages A and B fused in one
+                                        warp per item (an item stops generating candidates once its pose
+                                        is hit); 0 = 3 (the autotuner tries all three) */
     uint32_t stage_b_chunk;          /* discrete stage B: consecutive candidates one lane takes in order (lanes
                                         form) or 32-candidate groups one warp takes (packets); a pose's
                                         candidates then spread over few workers that stop at its first hit;
@@ -179,8 +180,9 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
  * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
- * then, for the discrete kinds, both stage B forms at chunk lengths from 1 to
- * 256 candidates (coordinate descent; sweeps are timed with segment flags on)
+ * then, for the discrete kinds, the three stage B forms, the first two at
+ * chunk lengths from 1 to 256 candidates (coordinate descent; sweeps are
+ * timed with segment flags on)
  * - times the traversal with device events (median of three after a
  * warm-up run), keeps the fastest configuration in the detector and
  * writes it to best_out (optional).  The upstream picks its batch size per
@@ -215,6 +217,7 @@ typedef struct {
                               quadratic sweep: pairs that needed the root finding */
     uint64_t exact_tests;  /* primitive-pair tests run in FP32 */
     uint64_t skipped;      /* candidates dropped because their pose (trajectory) was already decided */
+    uint64_t node_tests;   /* BVH child-box tests of the traversal kernels */
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 

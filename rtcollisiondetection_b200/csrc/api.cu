@@ -341,7 +341,7 @@ static void apply_launch_shape(rtcd_detector* d) {
     uint32_t per_sm = d->cfg.traverse_blocks_per_sm ? std::min(d->cfg.traverse_blocks_per_sm, fit) : fit;
     const uint32_t pct = d->cfg.residency_percent;
     if (pct > 100) fail(RTCD_ERR_INVALID_ARGUMENT, "residency_percent must be at most 100");
-    if (d->cfg.stage_b_form > 2) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_form must be 0, 1 or 2");
+    if (d->cfg.stage_b_form > 3) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_form must be 0, 1, 2 or 3");
     if (d->cfg.stage_b_chunk > 4096) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_chunk must be at most 4096");
     const uint32_t sms = (uint32_t) device_sm_count();
     if (pct) per_sm = std::max(1u, per_sm * pct / 100);
@@ -865,7 +865,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         W.item_overflow = d->item_overflow.as<uint8_t>();
         W.overflow_items = d->overflow_items.as<uint32_t>();
         W.overflow_count = wc + 1;
-        W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (r2o ? 64u : 4u);
+        W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (d->cfg.stage_b_form == 2 ? 4u : 64u);
         W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                         : d->cfg.light_steps                ? d->cfg.light_steps
                                                                   : 32u;
@@ -878,10 +878,15 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
             W.heavy_work = d->work.as<uint32_t>() + 1;
         }
         uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
-        launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
-        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads,
-                       d->cfg.residency_percent ? d->cfg.residency_percent : 100,
-                       d->cfg.stage_b_form == 2 || (d->cfg.stage_b_form == 0 && !r2o), s);
+        const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
+        if (d->cfg.stage_b_form == 3 || d->cfg.stage_b_form == 0) {
+            const uint32_t full = stage_ab_blocks(r2o);
+            launch_stage_ab(r2o, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100), s);
+            launch_stage_b_heavy(r2o, R, d->scene->dev, W, share, s);
+        } else {
+            launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
+            launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
+        }
         DiscreteArgs F = A;
         F.items = d->overflow_items.as<uint32_t>();
         F.n_items = wc + 1;
@@ -1222,9 +1227,11 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
             cuda_check(cudaMemcpyAsync(&cand, d->wave_counts.p, 4, cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaStreamSynchronize(s), "stats sync");
         out->fp64_retests = st[0];
-        out->candidates = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) ? cand : st[5];
+        // discrete: the candidate buffer's count, or the fused form's in-warp count
+        out->candidates = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) ? (st[6] ? st[6] : cand) : st[5];
         out->exact_tests = st[4];
         out->skipped = st[2];
+        out->node_tests = st[7];
         if (d->timed) {
             cuda_check(cudaEventElapsedTime(&out->ms_prepare, d->ev[0], d->ev[1]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_cull, d->ev[1], d->ev[2]), "elapsed");
@@ -1302,8 +1309,9 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         }
         if (discrete) {
             const rtcd_config base = best;
-            for (uint32_t form : {1u, 2u})
+            for (uint32_t form : {1u, 2u, 3u})
                 for (uint32_t chunk : {1u, 16u, 64u, 256u}) {
+                    if (form == 3 && chunk != 1) continue;  // the fused form has no chunk
                     rtcd_config c = base;
                     c.stage_b_form = form;
                     c.stage_b_chunk = form == 2 ? std::max(1u, chunk / 16) : chunk;

@@ -516,6 +516,7 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
     const float4* __restrict__ wn = R2O ? S.tri_nodes : S.edge_nodes;
     const uint32_t wroot = R2O ? S.tri_root : S.edge_root;
     const uint32_t n_items = *A.n_items;
+    unsigned long long n_node = 0;
     while (true) {
         uint32_t it = 0;
         if (lane == 0) it = atomicAdd(A.work_counter, 1u);
@@ -554,6 +555,7 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
                 } else {
                     Box bl, br;
                     load_node(wn, ref, bl, br, rl, rr);
+                    n_node += 2;
                     hl = obb_aabb(bl, ob, ext);
                     hr = obb_aabb(br, ob, ext);
                 }
@@ -594,6 +596,7 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
             W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
         }
     }
+    warp_count(A.stats + 7, n_node);
 }
 
 // Stage B works on one candidate (item, scene primitive) at a time: move the
@@ -720,7 +723,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
     const uint32_t total = min(*W.cand_count, W.cand_cap);
     const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
     uint32_t st[kStack];
-    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
+    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0, n_node = 0;
     // each lane takes up to W.chunk consecutive candidates in order: a pose's
     // candidates spread over a few lanes that each stop at its first hit,
     // instead of over many lanes that all start before any hit is known.
@@ -766,6 +769,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
             Box bl, br;
             uint32_t rl, rr;
             load_node(ln, ref, bl, br, rl, rr);
+            n_node += 2;
             const bool hr = stage_b_node<R2O>(C, br), hl = stage_b_node<R2O>(C, bl);
             if (sp + 2 > kStack) {
                 atomicOr(A.err, kErrStack);
@@ -780,6 +784,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
     warp_count(A.stats + 2, n_skip);
     warp_count(A.stats + 3, n_rej);
     warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 7, n_node);
 }
 
 // Stage B, light pass in packets: a warp takes 32 consecutive candidates and
@@ -804,7 +809,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
     const uint32_t n_groups = (total + 31) / 32;
     const uint32_t warps = gridDim.x * (BLOCK / 32);
     uint32_t st[kStack];
-    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0;
+    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0, n_node = 0;
     const uint32_t K = max(1u, min(W.chunk, n_groups / warps));  // consecutive groups per warp, in order
     for (uint32_t gg = (blockIdx.x * (BLOCK / 32) + (threadIdx.x >> 5)) * K; gg < n_groups; gg += warps * K)
     for (uint32_t g = gg; g < min(gg + K, n_groups); ++g) {
@@ -879,6 +884,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
                 Box bl, br;
                 uint32_t rl, rr;
                 load_node(ln, ref, bl, br, rl, rr);
+                if (in) n_node += 2;
                 const bool hr = in && stage_b_node<R2O>(C, br), hl = in && stage_b_node<R2O>(C, bl);
                 const bool any_r = __any_sync(0xffffffffu, hr), any_l = __any_sync(0xffffffffu, hl);
                 if (sp + 2 > kStack) {
@@ -895,6 +901,186 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
     warp_count(A.stats + 2, n_skip);
     warp_count(A.stats + 3, n_rej);
     warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 7, n_node);
+}
+
+// Stages A and B in one warp per (pose, link) item.  The warp descends the
+// scene LBVH with the link's OBB through a shared frontier as stage A does,
+// but keeps the leaf survivors in a shared buffer and, 32 at a time, runs
+// them through stage B at once (one lane per candidate, bounded by the light
+// budget; longer candidates are written to the candidate buffer and handed
+// to the heavy pass).  An item whose pose is found in collision stops
+// generating candidates: most colliding items are decided after their first
+// few candidates, so most of stage A's traversal and candidate traffic is
+// never spent on them.
+constexpr int kAbWarps = 4;
+constexpr int kCandBuf = 96;  // < 32 waiting + up to 64 added by one frontier step
+
+// Capped at 5 resident blocks per SM worth of registers (a few spills, more
+// warps to hide the node-load latency; measured on the 65,536-pose workload).
+template <bool R2O>
+__global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
+    constexpr float kBoxTol = 2e-5f;
+    __shared__ uint32_t s_front[kAbWarps][kFrontier];
+    __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
+    const DiscreteArgs& A = W.d;
+    const int lane = threadIdx.x & 31;
+    uint32_t* fr = s_front[threadIdx.x >> 5];
+    uint32_t* cb = s_cand[threadIdx.x >> 5];
+    const uint32_t lt = (1u << lane) - 1u;
+    const float4* __restrict__ wn = R2O ? S.tri_nodes : S.edge_nodes;
+    const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
+    const uint32_t wroot = R2O ? S.tri_root : S.edge_root;
+    const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
+    const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
+    const uint32_t n_items = *A.n_items;
+    const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
+    uint32_t st[kStack];
+    unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0, n_cand = 0, n_node = 0;
+    while (true) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(A.work_counter, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= n_items) break;
+        const uint32_t item = A.items[it];
+        const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
+        if (pose >= A.n_poses) {
+            if (lane == 0) atomicOr(A.err, kErrRange);
+            continue;
+        }
+        uint32_t dec = 0;
+        if (lane == 0 && !A.want_counts) dec = ld_flag(A.pose_hit + pose);
+        if (wroot == kNone || __shfl_sync(0xffffffffu, dec, 0)) continue;
+        float4 T[3];
+        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
+        ObbW ob = world_obb(R.obb[link], T);
+        ob.h = mk(ob.h.x + kBoxTol, ob.h.y + kBoxTol, ob.h.z + kBoxTol);
+        const f3 ext = mk(fabsf(ob.ax[0].x) * ob.h.x + fabsf(ob.ax[1].x) * ob.h.y + fabsf(ob.ax[2].x) * ob.h.z,
+                          fabsf(ob.ax[0].y) * ob.h.x + fabsf(ob.ax[1].y) * ob.h.y + fabsf(ob.ax[2].y) * ob.h.z,
+                          fabsf(ob.ax[0].z) * ob.h.x + fabsf(ob.ax[1].z) * ob.h.y + fabsf(ob.ax[2].z) * ob.h.z);
+        int sp = 1, nc = 0;
+        if (lane == 0) fr[0] = wroot;
+        __syncwarp();
+        while (true) {
+            if (nc >= 32 || (sp == 0 && nc > 0)) {  // stage B on up to 32 buffered candidates
+                const int take = min(nc, 32);
+                nc -= take;
+                const uint32_t prim = lane < take ? cb[nc + lane] : kNone;
+                __syncwarp();
+                bool hit = false;
+                StageBCand C;
+                if (prim != kNone && stage_b_setup<R2O>(R, S, W, make_uint2(item, prim), C, n_skip, n_rej, false)) {
+                    ++n_acc;
+                    int bsp = 0;
+                    st[bsp++] = C.lroot;
+                    uint32_t steps = 0, hits = 0;
+                    bool spilled = false;
+                    while (bsp > 0) {
+                        if (++steps > budget) {
+                            const uint32_t slot = atomicAdd(W.cand_count, 1u);
+                            if (slot < W.cand_cap) {
+                                W.cand[slot] = make_uint2(item, prim);
+                                const uint32_t h = atomicAdd(W.heavy_count, 1u);
+                                if (h < W.heavy_cap) {
+                                    W.heavy[h] = slot;
+                                    spilled = true;
+                                    break;
+                                }
+                            }
+                            steps = 0;  // no room: finish the candidate here
+                        }
+                        const uint32_t ref = st[--bsp];
+                        if (ref & kLeaf) {
+                            ++n_leaf;
+                            const uint32_t li = ref & ~kLeaf;
+                            if (stage_b_leaf<R2O>(lp, wp, li, C, A.stats)) {
+                                hit = true;
+                                if (!A.want_counts) break;
+                                if (R2O) {
+                                    const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
+                                    atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
+                                } else {
+                                    ++hits;
+                                }
+                            }
+                            continue;
+                        }
+                        Box bl, br;
+                        uint32_t rl, rr;
+                        load_node(ln, ref, bl, br, rl, rr);
+                        n_node += 2;
+                        const bool hr = stage_b_node<R2O>(C, br), hl = stage_b_node<R2O>(C, bl);
+                        if (bsp + 2 > kStack) {
+                            atomicOr(A.err, kErrStack);
+                            break;
+                        }
+                        if (hr) st[bsp++] = rr;
+                        if (hl) st[bsp++] = rl;
+                    }
+                    if (hits && !spilled) atomicAdd(A.counts + pose, hits);
+                }
+                const bool any = __any_sync(0xffffffffu, hit);
+                if (any) {
+                    if (lane == 0) {
+                        if (A.want_counts) A.pose_hit[pose] = 1u;
+                        else atomicExch(A.pose_hit + pose, 1u);
+                    }
+                    if (!A.want_counts) break;
+                }
+                if (!A.want_counts) {  // decided meanwhile by another item?
+                    uint32_t d2 = 0;
+                    if (lane == 0) d2 = ld_flag(A.pose_hit + pose);
+                    if (__shfl_sync(0xffffffffu, d2, 0)) break;
+                }
+                continue;
+            }
+            if (sp == 0) break;
+            const int take = min(sp, 32);
+            sp -= take;
+            const uint32_t ref = lane < take ? fr[sp + lane] : kNone;
+            __syncwarp();
+            bool hl = false, hr = false;
+            uint32_t rl = kNone, rr = kNone;
+            if (ref != kNone) {
+                if (ref & kLeaf) {  // a one-primitive scene: the root itself is a leaf
+                    hl = true;
+                    rl = ref;
+                } else {
+                    Box bl, br;
+                    load_node(wn, ref, bl, br, rl, rr);
+                    n_node += 2;
+                    hl = obb_aabb(bl, ob, ext);
+                    hr = obb_aabb(br, ob, ext);
+                }
+            }
+            const bool pl = hl && !(rl & kLeaf), pr = hr && !(rr & kLeaf);
+            const bool el = hl && (rl & kLeaf), er = hr && (rr & kLeaf);
+            const uint32_t mpl = __ballot_sync(0xffffffffu, pl), mpr = __ballot_sync(0xffffffffu, pr);
+            const uint32_t mel = __ballot_sync(0xffffffffu, el), mer = __ballot_sync(0xffffffffu, er);
+            const int npush = __popc(mpl) + __popc(mpr);
+            if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
+                if (lane == 0) atomicOr(A.err, kErrStack);
+                break;
+            }
+            if (pl) fr[sp + __popc(mpl & lt)] = rl;
+            if (pr) fr[sp + __popc(mpl) + __popc(mpr & lt)] = rr;
+            sp += npush;
+            if (el) cb[nc + __popc(mel & lt)] = rl & ~kLeaf;
+            if (er) cb[nc + __popc(mel) + __popc(mer & lt)] = rr & ~kLeaf;
+            const int nemit = __popc(mel) + __popc(mer);
+            nc += nemit;
+            n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
+            __syncwarp();
+        }
+        __syncwarp();
+    }
+    warp_count(A.stats + 1, n_acc);
+    warp_count(A.stats + 2, n_skip);
+    warp_count(A.stats + 3, n_rej);
+    warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 7, n_node);
+    warp_count(A.stats + 6, n_cand);
 }
 
 // Stage B, heavy pass: one warp per spilled candidate.  The warp descends the
@@ -917,7 +1103,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotD
     uint32_t* lf = s_leaf[threadIdx.x >> 5];
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t n_heavy = min(*W.heavy_count, W.heavy_cap);
-    unsigned long long n_skip = 0, n_rej = 0, n_leaf = 0;
+    unsigned long long n_skip = 0, n_rej = 0, n_leaf = 0, n_node = 0;
     while (true) {
         uint32_t h = 0;
         if (lane == 0) h = atomicAdd(W.heavy_work, 1u);
@@ -984,6 +1170,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotD
                 } else {
                     Box bl, br;
                     load_node(ln, ref, bl, br, rl, rr);
+                    n_node += 2;
                     hl = stage_b_node<R2O>(C, bl);
                     hr = stage_b_node<R2O>(C, br);
                 }
@@ -1009,6 +1196,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotD
         __syncwarp();
     }
     warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 7, n_node);
 }
 
 template <class K>
@@ -1075,16 +1263,33 @@ void launch_stage_b(bool r2o, const RobotDev& R, const SceneDev& S, const WaveAr
     else
         stage_b_dispatch<false>(R, S, W, blocks, threads, packets, s);
     cuda_check(cudaGetLastError(), "k_stage_b");
-    if (W.light_steps) {
-        static const uint32_t full_r2o = grid_for(k_stage_b_heavy<true>, kHeavyWarps * 32);
-        static const uint32_t full_o2r = grid_for(k_stage_b_heavy<false>, kHeavyWarps * 32);
-        const uint32_t hb = std::max(1u, (r2o ? full_r2o : full_o2r) * heavy_share / 100);
-        if (r2o)
-            k_stage_b_heavy<true><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
-        else
-            k_stage_b_heavy<false><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
-        cuda_check(cudaGetLastError(), "k_stage_b_heavy");
-    }
+    launch_stage_b_heavy(r2o, R, S, W, heavy_share, s);
+}
+
+void launch_stage_b_heavy(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t heavy_share,
+                          cudaStream_t s) {
+    if (!W.light_steps) return;
+    static const uint32_t full_r2o = grid_for(k_stage_b_heavy<true>, kHeavyWarps * 32);
+    static const uint32_t full_o2r = grid_for(k_stage_b_heavy<false>, kHeavyWarps * 32);
+    const uint32_t hb = std::max(1u, (r2o ? full_r2o : full_o2r) * heavy_share / 100);
+    if (r2o)
+        k_stage_b_heavy<true><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
+    else
+        k_stage_b_heavy<false><<<hb, kHeavyWarps * 32, 0, s>>>(R, S, W);
+    cuda_check(cudaGetLastError(), "k_stage_b_heavy");
+}
+
+uint32_t stage_ab_blocks(bool r2o) {
+    return r2o ? grid_for(k_stage_ab<true>, kAbWarps * 32) : grid_for(k_stage_ab<false>, kAbWarps * 32);
+}
+
+void launch_stage_ab(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                     cudaStream_t s) {
+    if (r2o)
+        k_stage_ab<true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+    else
+        k_stage_ab<false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+    cuda_check(cudaGetLastError(), "k_stage_ab");
 }
 
 uint32_t discrete_persistent_blocks(bool robot_to_obs) {

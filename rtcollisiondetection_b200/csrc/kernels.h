@@ -84,6 +84,14 @@ void launch_stage_a(bool robot_to_obs, const RobotDev& R, const SceneDev& S, con
 // heavy_share percent of the full persistent grid.
 void launch_stage_b(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                     uint32_t threads, uint32_t heavy_share, bool packets, cudaStream_t s);
+// The heavy pass alone (after a light pass that spilled into W.heavy).
+void launch_stage_b_heavy(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W,
+                          uint32_t heavy_share, cudaStream_t s);
+// Stages A and B fused in one warp per item (stage_b_form 3); its spilled
+// candidates go to W.cand / W.heavy for the heavy pass.
+void launch_stage_ab(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+                     cudaStream_t s);
+uint32_t stage_ab_blocks(bool robot_to_obs);
 uint32_t stage_a_blocks(bool robot_to_obs);
 uint32_t stage_b_blocks(bool robot_to_obs);
 uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256

@@ -449,8 +449,11 @@ __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ ep, uint32_t
 // so far are set as flags, which are idempotent; its counts are dropped and
 // recounted there), so one lane never serialises a unit that meets thousands
 // of nodes.
+// The quadratic form is capped at 96 registers (5 blocks of 128 threads per
+// SM): the extra resident warps hide more load latency than the few spilled
+// registers cost (measured on the 4,096-trajectory quadratic workload).
 template <bool QUAD, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepArgs A) {
+__global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(const SceneDev S, const SweepArgs A) {
     const float4* __restrict__ en = S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
     uint32_t st[kStack];
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepAr
     U.traj = U.piece_g = 0;
     const uint32_t stride = gridDim.x * blockDim.x;
     uint32_t next = blockIdx.x * blockDim.x + threadIdx.x;  // neighbouring lanes: spheres of one piece
-    unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0;
+    unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0, n_node = 0;
     const uint32_t budget = A.light_steps ? A.light_steps : 0xFFFFFFFFu;
 
     while (true) {
@@ -500,6 +503,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepAr
             Box bl, br;
             uint32_t rl, rr;
             load_node(en, ref, bl, br, rl, rr);
+            n_node += 2;
             float tl, tr;
             bool hr = cull_box<QUAD>(c, br, tr), hl = cull_box<QUAD>(c, bl, tl);
             if (sp + 2 > kStack) {
@@ -547,6 +551,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const SceneDev S, const SweepAr
     warp_count(A.stats + 2, n_skip);
     warp_count(A.stats + 4, n_leaf);
     warp_count(A.stats + 5, n_roots);
+    warp_count(A.stats + 7, n_node);
 }
 
 // Heavy pass: one warp per spilled unit.  The warp descends the obstacle-edge
@@ -566,7 +571,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
     uint32_t* lf = s_leaf[threadIdx.x >> 5];
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t n_heavy = min(*A.heavy_count, A.heavy_cap);
-    unsigned long long n_leaf = 0, n_roots = 0;
+    unsigned long long n_leaf = 0, n_roots = 0, n_node = 0;
     while (true) {
         uint32_t h = 0;
         if (lane == 0) h = atomicAdd(A.heavy_work, 1u);
@@ -629,6 +634,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
                     Box bl, br;
                     float t;
                     load_node(S.edge_nodes, ref, bl, br, rl, rr);
+                    n_node += 2;
                     hl = cull_box<QUAD>(c, bl, t);
                     hr = cull_box<QUAD>(c, br, t);
                 }
@@ -655,6 +661,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
     }
     warp_count(A.stats + 4, n_leaf);
     warp_count(A.stats + 5, n_roots);
+    warp_count(A.stats + 7, n_node);
 }
 
 template <bool QUAD>

@@ -67,7 +67,7 @@ class Stats(C.Structure):
     _fields_ = [('work_items', C.c_uint64), ('culled_items', C.c_uint64), ('fp64_retests', C.c_uint64),
                 ('ms_prepare', C.c_float), ('ms_cull', C.c_float), ('ms_traverse', C.c_float),
                 ('ms_total', C.c_float), ('candidates', C.c_uint64), ('exact_tests', C.c_uint64),
-                ('skipped', C.c_uint64)]
+                ('skipped', C.c_uint64), ('node_tests', C.c_uint64)]
 
 
 _lib = None
@@ -340,7 +340,8 @@ class Detector:
         _ok(lib().rtcd_last_stats(self.h, C.byref(s)))
         return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests, 'ms_prepare': s.ms_prepare,
                 'ms_cull': s.ms_cull, 'ms_traverse': s.ms_traverse, 'ms_total': s.ms_total,
-                'candidates': s.candidates, 'exact_tests': s.exact_tests, 'skipped': s.skipped}
+                'candidates': s.candidates, 'exact_tests': s.exact_tests, 'skipped': s.skipped,
+                'node_tests': s.node_tests}
 
     def close(self):
         if self.h:

@@ -69,14 +69,15 @@ def test_cull_plain_and_device_paths_agree(setup, panda, name, okind):
 @pytest.mark.parametrize('name,okind', KINDS)
 @pytest.mark.parametrize('light', [1, 0, 0xFFFFFFFF])
 def test_stage_b_forms_agree(setup, panda, name, okind, light):
-    """Packet and per-lane stage B at two chunk lengths each, with every
+    """Packet and per-lane stage B at two chunk lengths each and the fused
+    stage A+B, with every
     candidate spilled to the heavy pass (budget 1), the default budget, and
     no heavy pass: identical flags and counts, and the flags agree with the
     oracle outside the band."""
     robot, scene, (orob, oscene) = setup
     q = scenes.uniform_poses(panda, 600, seed=21)
     dets = [rtcd.Detector(robot.ctx, name, robot, scene, light_steps=light, stage_b_form=f, stage_b_chunk=k)
-            for f, k in ((1, 1), (1, 64), (2, 1), (2, 4))]
+            for f, k in ((1, 1), (1, 64), (2, 1), (2, 4), (3, 0))]
     flags_only = [d.check(q) for d in dets]
     counted = [d.check(q, counts=True) for d in dets]
     for o in flags_only + counted:
