@@ -369,7 +369,8 @@ def main():
     ap.add_argument('--no-check', action='store_true')
     ap.add_argument('--ref-sample', type=int, default=8192)
     ap.add_argument('--plain-frame', type=int, default=64)
-    ap.add_argument('--fused', action='store_true', help='discrete: the single fused traversal kernel')
+    ap.add_argument('--fused', action='store_true', help='discrete: the thread-per-item traversal kernel')
+    ap.add_argument('--no-graph', action='store_true', help='launch the timed steps directly, not as a CUDA graph')
     ap.add_argument('--serve-seconds', type=float, default=5.0,
                     help='length of the served mixed stream reported under "served" (0: skip)')
     args = ap.parse_args()
@@ -410,12 +411,14 @@ def main():
 
     tuned = det.autotune(qd, n, off, stream=sp)   # untimed: picks the traversal launch shape
     base_flags = rtcd.CHECK_TIMING | (rtcd.CHECK_FUSED if args.fused else 0)
+    # the timed steps replay the launch sequence as a CUDA graph (captured in the first warm-up step)
+    graph = 0 if args.no_graph else rtcd.CHECK_GRAPH
 
     def step(extra=0):
         det.check_device(qd, n, fd, traj_off=off, seg_dev=segd, flags=base_flags | extra, stream=sp)
 
     for _ in range(max(3, args.warmup)):
-        step()
+        step(graph)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -428,9 +431,9 @@ def main():
     for k in range(args.steps):
         flush.fill_(k & 255)
         ev[k][0].record(stream)
-        step()
+        step(graph)
         ev[k][1].record(stream)
-        trav.append(det.stats())   # syncs the step; stage times come from events on the same stream
+        trav.append(det.stats())   # syncs the step; the kernels' work counters of this step
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     if dist:
@@ -482,7 +485,13 @@ def main():
                  'ms_per_step': float(np.median(pm))}
 
     peaks, peak_src = load_peaks()
-    t_trav = float(np.mean([s['ms_traverse'] for s in trav]))
+    # traversal span of the same step, timed with events around its kernels (graph replays are timed whole)
+    spans = []
+    for k in range(3):
+        flush.fill_(k & 255)
+        step()
+        spans.append(det.stats())
+    t_trav = float(np.mean([s['ms_traverse'] for s in spans]))
     # algorithmic bytes of one traversal span: poses in, flags out, the resident structures read once
     if sweep:
         bytes_alg = n * 4 + int(q.nbytes) + 32 * scene.n_edges * 3
@@ -525,7 +534,8 @@ def main():
         'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
         'data': 'synthetic',
         'config': {'workload': cfg['workload'], 'detector': cfg['kind'], 'units_per_gpu': n,
-                   'l2': 'flushed before every step (256 MiB write)', 'form': 'batched: one persistent launch per step',
+                   'l2': 'flushed before every step (256 MiB write)', 'form': 'batched: persistent traversal kernels, each step replayed as one CUDA graph'
+                   if not args.no_graph else 'batched: persistent traversal kernels, launched directly',
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
@@ -534,8 +544,8 @@ def main():
         # k_sweep_heavy, k_flags x 2
         'gpu_launches': args.steps * ((7 if tuned.get('stage_b_form', 0) in (0, 3) else 8) if not sweep
                                       else (5 if cfg['kind'] == 'Linear' else 6)),
-        'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in trav])),
-                      'cull': float(np.mean([s['ms_cull'] for s in trav])), 'traverse': t_trav},
+        'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in spans])),
+                      'cull': float(np.mean([s['ms_cull'] for s in spans])), 'traverse': t_trav},
         'roofline': {'bound': 'hbm', 'kernel': span, 'achieved': achieved,
                      'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved / peaks['hbm_gbs'],
                      'traffic': traffic, 'peak_source': peak_src, 'fp32': fp32,

@@ -65,8 +65,9 @@ typedef enum {
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
 #define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
 #define RTCD_CHECK_FUSED (1u << 6)         /* discrete: one fused traversal kernel instead of the two-stage wavefront */
-#define RTCD_CHECK_GRAPH (1u << 7)         /* discrete, device buffers: replay the launch sequence as a CUDA graph
-                                              (captured on the first call with these pointers, sizes and flags) */
+#define RTCD_CHECK_GRAPH (1u << 7)         /* device buffers: replay the launch sequence as a CUDA graph (captured on
+                                              the first call with these pointers, sizes, flags and - for sweeps -
+                                              trajectory offsets; any other call on the detector retires it) */
 
 typedef struct rtcd_ctx rtcd_ctx;
 typedef struct rtcd_robot rtcd_robot;

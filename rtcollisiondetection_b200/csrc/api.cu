@@ -273,7 +273,7 @@ struct rtcd_detector {
     cudaStream_t last_stream = nullptr;  // stream of the last check (stats read on it)
     cudaGraph_t graph = nullptr;         // captured launch sequence (RTCD_CHECK_GRAPH)
     cudaGraphExec_t graph_exec = nullptr;
-    uint64_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+    uint64_t graph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     bool timed_total_only = false;       // the last check timed only ev[0] -> ev_end (graph path)
     uint32_t blocks = 0;
     // discrete workspace
@@ -990,7 +990,12 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     if (quad) ensure_weights(d, max_wp);
     // auxiliary tables: wp_off | piece_off | ctrl_off | piece_traj
     const size_t aux_words = 3ull * (n + 1) + pieces;
-    cuda_check(cudaEventSynchronize(d->staged), "staging reuse");
+    // under graph capture the staging buffer is idle (synchronised before the
+    // capture) and replays never rewrite it, so no staging event is recorded
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cuda_check(cudaStreamIsCapturing(s, &cap), "cudaStreamIsCapturing");
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    if (!capturing) cuda_check(cudaEventSynchronize(d->staged), "staging reuse");
     d->pin_aux.ensure(4 * aux_words);
     uint32_t* a = d->pin_aux.as<uint32_t>();
     uint32_t* wp_off = a;
@@ -1016,7 +1021,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
-    cuda_check(cudaEventRecord(d->staged, s), "event");
+    if (!capturing) cuda_check(cudaEventRecord(d->staged, s), "event");
     const uint32_t* dwp = d->aux.as<uint32_t>();
     const uint32_t* dpo = dwp + (n + 1);
     const uint32_t* dco = dwp + 2 * (n + 1);
@@ -1129,16 +1134,29 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
         if (n) cuda_check(cudaMemsetAsync(d->stats.p, 0, 64, s), "stats reset");
         if (n == 0) return;
         if (flags & RTCD_CHECK_GRAPH) {
-            RTCD_REQUIRE(d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS,
-                         "graph replay is offered for the discrete detectors");
-            RTCD_REQUIRE(!(flags & (RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_PLAIN)) && !seg_flags_out,
+            const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
+            RTCD_REQUIRE(!(flags & (RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_PLAIN)),
                          "graph replay needs device buffers and the batched path");
+            RTCD_REQUIRE(!discrete || !seg_flags_out, "segment flags exist only for sweep detectors");
+            RTCD_REQUIRE(discrete || traj_offsets, "traj_offsets required for sweep detectors");
             RTCD_REQUIRE(flags_out, "graph replay needs a device flags buffer");
             // events recorded inside a graph cannot be timed: a replay is timed as a whole
             const bool want_time = (flags & RTCD_CHECK_TIMING) != 0;
             const uint32_t f = flags & ~(RTCD_CHECK_GRAPH | RTCD_CHECK_TIMING);
-            const uint64_t key[6] = {(uint64_t) q, n, (uint64_t) flags_out, (uint64_t) counts_out, f, (uint64_t) s};
-            if (d->graph_exec && std::equal(key, key + 6, d->graph_key)) {
+            // sweeps: the graph holds the trajectory tables built from traj_offsets, so
+            // their contents are part of the key (FNV-1a over the n + 1 offsets)
+            uint64_t h = 1469598103934665603ull;
+            if (!discrete)
+                for (uint32_t i = 0; i <= n; ++i) h = (h ^ traj_offsets[i]) * 1099511628211ull;
+            const uint64_t key[8] = {(uint64_t) q, n, (uint64_t) flags_out, (uint64_t) counts_out, f, (uint64_t) s,
+                                     (uint64_t) seg_flags_out, h};
+            auto run = [&] {
+                if (discrete)
+                    check_discrete(d, q, n, flags_out, counts_out, f, s);
+                else
+                    check_sweep(d, q, traj_offsets, n, flags_out, seg_flags_out, counts_out, f, s);
+            };
+            if (d->graph_exec && std::equal(key, key + 8, d->graph_key)) {
                 if (want_time) cuda_check(cudaEventRecord(d->ev[0], s), "event");
                 cuda_check(cudaGraphLaunch(d->graph_exec, s), "cudaGraphLaunch");
                 if (want_time) cuda_check(cudaEventRecord(d->ev_end, s), "event");
@@ -1148,16 +1166,17 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             // run once normally (this also sizes every workspace), then capture the
             // same sequence - which now allocates nothing - for the next calls
             if (want_time) cuda_check(cudaEventRecord(d->ev[0], s), "event");
-            check_discrete(d, q, n, flags_out, counts_out, f, s);
+            run();
             if (want_time) cuda_check(cudaEventRecord(d->ev_end, s), "event");
             d->timed_total_only = want_time;
+            cuda_check(cudaStreamSynchronize(s), "pre-capture sync");  // staging buffers idle before capture
             if (d->graph_exec) cudaGraphExecDestroy(d->graph_exec);
             if (d->graph) cudaGraphDestroy(d->graph);
             d->graph_exec = nullptr;
             d->graph = nullptr;
             cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
             try {
-                check_discrete(d, q, n, flags_out, counts_out, f, s);
+                run();
             } catch (...) {
                 cudaGraph_t g = nullptr;
                 cudaStreamEndCapture(s, &g);
@@ -1166,7 +1185,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             }
             cuda_check(cudaStreamEndCapture(s, &d->graph), "cudaStreamEndCapture");
             cuda_check(cudaGraphInstantiate(&d->graph_exec, d->graph, 0), "cudaGraphInstantiate");
-            std::copy(key, key + 6, d->graph_key);
+            std::copy(key, key + 8, d->graph_key);
             return;
         }
         if (d->graph_exec) {  // this call may grow (move) workspaces the graph points into

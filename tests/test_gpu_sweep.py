@@ -103,3 +103,33 @@ def test_sweep_rejects_bad_offsets(sweep_setup):
     qd = rtcd.Detector(robot.ctx, 'Quadratic', robot, scene)
     with pytest.raises(rtcd.RTCDError):
         qd.check(np.zeros((2, 7), np.float32), np.array([0, 2], np.uint32))
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_sweep_graph_replay_matches_direct_path(sweep_setup, panda, kind):
+    """RTCD_CHECK_GRAPH for the sweeps: the first call captures, later calls
+    with the same buffers and trajectory offsets replay; new waypoint contents
+    give the same trajectory and segment flags as the direct path, and new
+    offsets capture again."""
+    import torch
+    robot, scene, _, _ = sweep_setup
+    det = rtcd.Detector(robot.ctx, kind, robot, scene)
+    ref_det = rtcd.Detector(robot.ctx, kind, robot, scene)  # a direct call on `det` would retire its graph
+    s = torch.cuda.Stream()
+    for off_seed in (1, 2):
+        counts = scenes.log_uniform_counts(40, 8, 40, seed=off_seed)
+        off = np.zeros(41, np.uint32)
+        off[1:] = np.cumsum(counts)
+        nseg = int(rtcd.segment_offsets(det.kind, off)[-1])
+        with torch.cuda.stream(s):
+            qd = torch.zeros((int(off[-1]), 7), dtype=torch.float32, device='cuda')
+            fd = torch.zeros(40, dtype=torch.uint8, device='cuda')
+            sd = torch.zeros(nseg, dtype=torch.uint8, device='cuda')
+            for seed in (31, 32, 33):
+                q, _ = scenes.random_walk_trajectories(panda, 40, counts, seed=seed)
+                qd.copy_(torch.from_numpy(q))
+                det.check_device(qd, 40, fd, traj_off=off, seg_dev=sd, flags=rtcd.CHECK_GRAPH, stream=s.cuda_stream)
+                det.sync(s.cuda_stream)
+                ref = ref_det.check(q, off, segments=True)
+                assert np.array_equal(fd.cpu().numpy(), ref['flags']), (off_seed, seed)
+                assert np.array_equal(sd.cpu().numpy(), ref['seg_flags']), (off_seed, seed)
