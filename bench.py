@@ -153,7 +153,7 @@ def cpu_baseline(cfg, model, mesh, spheres, q, off, seconds=10.0):
             'seconds': round(dt, 3)}
 
 
-def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512):
+def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512, two_way=False, containment=False):
     """Flag mismatches outside the 1e-5 m band on a sample of the batch."""
     from oracle import oracle as O
     robot = O.Robot(model, spheres=spheres)
@@ -162,9 +162,19 @@ def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512):
         k = O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT
         idx = np.linspace(0, len(q) - 1, min(n_sample, len(q))).astype(int)
         ref = O.discrete(k, robot, scene, q[idx])
-        err = int(((flags[idx] != ref['hit']) & (ref['band'] == 0)).sum())
-        return {'flag_errors': err, 'checked': len(idx), 'in_band': int(ref['band'].sum()),
-                'collision_rate': float(ref['hit'].mean())}
+        hit, band = ref['hit'].copy(), ref['band'].copy()
+        if two_way:
+            other = O.discrete(1 - k, robot, scene, q[idx])
+            hit |= other['hit']
+            band |= other['band']
+        want = hit.astype(np.uint8)
+        if containment:
+            cont = O.containment(robot, scene, q[idx], skip=hit)
+            want |= 2 * cont['contain']
+            band |= cont['band']
+        err = int(((flags[idx] != want) & (band == 0)).sum())
+        return {'flag_errors': err, 'checked': len(idx), 'in_band': int(band.sum()),
+                'collision_rate': float((want != 0).mean())}
     m = min(len(off) - 1, n_sample // 4)
     ref = O.sweep(cfg['kind'] == 'Quadratic', robot, scene, q[:off[m]], off[:m + 1])
     err = int(((flags[:m] != ref['traj_hit']) & (ref['traj_band'] == 0)).sum())
@@ -371,6 +381,8 @@ def main():
     ap.add_argument('--plain-frame', type=int, default=64)
     ap.add_argument('--fused', action='store_true', help='discrete: the thread-per-item traversal kernel')
     ap.add_argument('--no-graph', action='store_true', help='launch the timed steps directly, not as a CUDA graph')
+    ap.add_argument('--two-way', action='store_true', help='discrete: both directions in one check (flags = union)')
+    ap.add_argument('--containment', action='store_true', help='discrete: add the containment test')
     ap.add_argument('--serve-seconds', type=float, default=5.0,
                     help='length of the served mixed stream reported under "served" (0: skip)')
     args = ap.parse_args()
@@ -410,7 +422,9 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device='cuda')
 
     tuned = det.autotune(qd, n, off, stream=sp)   # untimed: picks the traversal launch shape
-    base_flags = rtcd.CHECK_TIMING | (rtcd.CHECK_FUSED if args.fused else 0)
+    mode_flags = 0 if sweep else ((rtcd.CHECK_TWO_WAY if args.two_way else 0) |
+                                  (rtcd.CHECK_CONTAINMENT if args.containment else 0))
+    base_flags = rtcd.CHECK_TIMING | (rtcd.CHECK_FUSED if args.fused else 0) | mode_flags
     # the timed steps replay the launch sequence as a CUDA graph (captured in the first warm-up step)
     graph = 0 if args.no_graph else rtcd.CHECK_GRAPH
 
@@ -458,7 +472,7 @@ def main():
         flush.fill_(k & 255)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        out = det.check(q, off, segments=sweep)
+        out = det.check(q, off, segments=sweep, flags=mode_flags)
         dt = (time.perf_counter() - t0) * 1e3
         if k >= 2:
             e2e_ms.append(dt)
@@ -477,7 +491,7 @@ def main():
             flush.fill_(k & 255)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            det.check_device(qd, n, fd, flags=rtcd.CHECK_PLAIN, stream=sp)
+            det.check_device(qd, n, fd, flags=rtcd.CHECK_PLAIN | mode_flags, stream=sp)
             torch.cuda.synchronize()
             pm.append((time.perf_counter() - t0) * 1e3)
         assert np.array_equal(fd.cpu().numpy(), flags), 'plain path disagrees'
@@ -533,8 +547,11 @@ def main():
         'metric': METRIC, 'value': value, 'unit': unit, 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32',
         'data': 'synthetic',
-        'config': {'workload': cfg['workload'], 'detector': cfg['kind'], 'units_per_gpu': n,
-                   'l2': 'flushed before every step (256 MiB write)', 'form': 'batched: persistent traversal kernels, each step replayed as one CUDA graph'
+        'config': {'workload': cfg['workload'] + (' (two-way: both directions)' if args.two_way and not sweep else '')
+                   + (' + containment' if args.containment and not sweep else ''),
+                   'detector': cfg['kind'], 'units_per_gpu': n,
+                   'l2': 'flushed before every step (256 MiB write)',
+                   'form': 'batched: persistent traversal kernels, each step replayed as one CUDA graph'
                    if not args.no_graph else 'batched: persistent traversal kernels, launched directly',
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
@@ -558,7 +575,8 @@ def main():
         line['plain'] = plain
         line['batched_over_plain'] = value / plain['value']
     if not args.no_check and rank == 0:
-        line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags)
+        line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags, two_way=args.two_way,
+                                      containment=args.containment)
         line['fp64_retests'] = st['fp64_retests']
     if args.serve_seconds > 0 and rank == 0 and args.config == 'c2':
         line['served'] = served_stream(ctx, args.serve_seconds)

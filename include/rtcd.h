@@ -65,6 +65,12 @@ typedef enum {
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
 #define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
 #define RTCD_CHECK_FUSED (1u << 6)         /* discrete: one fused traversal kernel instead of the two-stage wavefront */
+#define RTCD_CHECK_CONTAINMENT (1u << 8)   /* discrete: also flag poses with no surface crossing where a link lies
+                                              inside an obstacle or an obstacle inside a link (ray parity);
+                                              such poses get flag value 2, surface crossings 1 */
+#define RTCD_CHECK_TWO_WAY (1u << 9)       /* discrete: run both directions (ObsToRobot and RobotToObs) in one check
+                                              over the same FK, cull and items: flags are the union, counts the
+                                              sum of the two upstream counts */
 #define RTCD_CHECK_GRAPH (1u << 7)         /* device buffers: replay the launch sequence as a CUDA graph (captured on
                                               the first call with these pointers, sizes, flags and - for sweeps -
                                               trajectory offsets; any other call on the detector retires it) */

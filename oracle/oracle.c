@@ -703,6 +703,166 @@ int orc_discrete(int kind, const orc_robot* R, const orc_scene* S, const float* 
     return 0;
 }
 
+/* ------------------------------------------------------------- containment
+ * No upstream counterpart: the reference's rays follow surface crossings only,
+ * so a link wholly inside an obstacle (or an obstacle inside a link) is never
+ * seen.  For a pose with no surface crossing (skip[pose] == 0), every checked
+ * link l and obstacle o: (a) the link's first vertex inside o, or (b) o's
+ * first vertex (first vertex of its first triangle) inside the link, decided
+ * by the parity of the crossings of the segment from the point along
+ * (0.48, 0.6, 0.64) to beyond the other mesh's box, with that mesh's
+ * triangles (closed segment vs closed triangle).  A crossing within eps of
+ * flipping puts the pose in band.  Both meshes must be closed.
+ */
+typedef struct {
+    const orc_robot* R;
+    const orc_scene* S;
+    const u32* ooff;
+    int n_obs;
+    const float* q;
+    double eps;
+    const unsigned char* skip;
+    unsigned char *contain, *band;
+    bvh_t scene_tri;
+    bvh_t* link_tri;
+    u32* tri_obs;
+    double* obox;  /* [o][6] lo, hi */
+    double* lbox;  /* [l][6] link-frame lo, hi */
+} cont_ctx;
+
+typedef struct {
+    d3 p, q;
+    const float* tv; const u32* tt;
+    const u32* tag; u32 want;  /* count only triangles with tag[t] == want (tag NULL: all) */
+    double eps;
+    u32 crossings;
+    int marginal;
+} ray_query;
+
+static int visit_cross(void* vctx, u32 t) {
+    ray_query* r = (ray_query*) vctx;
+    if (r->tag && r->tag[t] != r->want) return 0;
+    d3 a = fv(r->tv + r->tt[t * 3] * 3), b = fv(r->tv + r->tt[t * 3 + 1] * 3), c = fv(r->tv + r->tt[t * 3 + 2] * 3);
+    double m;
+    int h = seg_tri(r->p, r->q, a, b, c, &m);
+    if (h) r->crossings++;
+    if (m <= r->eps) r->marginal = 1;
+    return 0;
+}
+
+/* exit parameter of p + t d from the box [lo, hi] */
+static double box_exit_d(d3 p, d3 d, const double* lo, const double* hi) {
+    double pc[3] = {p.x, p.y, p.z}, dc[3] = {d.x, d.y, d.z}, t = INFINITY;
+    for (int k = 0; k < 3; ++k) {
+        double tk = dc[k] > 0 ? (hi[k] - pc[k]) / dc[k] : (dc[k] < 0 ? (lo[k] - pc[k]) / dc[k] : INFINITY);
+        if (tk < t) t = tk;
+    }
+    return t < 0 ? 0 : t;
+}
+
+static int in_box(d3 p, const double* b, double pad) {
+    return p.x >= b[0] - pad && p.x <= b[3] + pad && p.y >= b[1] - pad && p.y <= b[4] + pad && p.z >= b[2] - pad &&
+           p.z <= b[5] + pad;
+}
+
+/* crossings parity of the ray from p (direction dir) through a mesh held in box b */
+static int ray_parity(const bvh_t* bvh, d3 p, const double* b, const float* tv, const u32* tt, const u32* tag, u32 want,
+                      double eps, int* marginal) {
+    const d3 dir = v3(0.48, 0.6, 0.64);
+    double t = box_exit_d(p, dir, b, b + 3) + 1e-2;
+    ray_query r;
+    memset(&r, 0, sizeof(r));
+    r.p = p; r.q = add(p, mul(dir, t)); r.tv = tv; r.tt = tt; r.tag = tag; r.want = want; r.eps = eps;
+    double qlo[3] = {fmin(r.p.x, r.q.x) - eps, fmin(r.p.y, r.q.y) - eps, fmin(r.p.z, r.q.z) - eps};
+    double qhi[3] = {fmax(r.p.x, r.q.x) + eps, fmax(r.p.y, r.q.y) + eps, fmax(r.p.z, r.q.z) + eps};
+    bvh_query(bvh, qlo, qhi, visit_cross, &r);
+    if (r.marginal) *marginal = 1;
+    return (int) (r.crossings & 1u);
+}
+
+static void cont_pose(void* vctx, int pose, void* scratch) {
+    (void) scratch;
+    cont_ctx* C = (cont_ctx*) vctx;
+    const orc_robot* R = C->R;
+    const orc_scene* S = C->S;
+    C->contain[pose] = 0;
+    if (C->band) C->band[pose] = 0;
+    if (C->skip && C->skip[pose]) return;
+    double T[9 * 12];
+    double* Tp = (R->dof + 1) * 12 <= 9 * 12 ? T : (double*) malloc(sizeof(double) * (size_t) (R->dof + 1) * 12);
+    orc_fk_pose(R->dof, R->cos_mask, R->sin_mask, R->one_mask, R->base_tf, C->q + (size_t) pose * R->dof, Tp);
+    int inside = 0, marginal = 0;
+    for (int l = R->skip_base ? 1 : 0; l < R->n_links && !inside; ++l) {
+        if (R->link_vert_off[l + 1] == R->link_vert_off[l]) continue;
+        const double* TL = Tp + l * 12;
+        const float* lv = R->link_verts + (size_t) R->link_vert_off[l] * 3;
+        const u32* lt = R->link_tris + (size_t) R->link_tri_off[l] * 3;
+        d3 p = xform(TL, fv(lv));
+        for (int o = 0; o < C->n_obs && !inside; ++o) {
+            const double* ob = C->obox + 6 * o;
+            if (in_box(p, ob, 1e-4) &&
+                ray_parity(&C->scene_tri, p, ob, S->verts, S->tris, C->tri_obs, (u32) o, C->eps, &marginal))
+                inside = 1;
+            if (inside || C->ooff[o + 1] == C->ooff[o]) continue;
+            d3 qo = xform_inv(TL, fv(S->verts + S->tris[(size_t) C->ooff[o] * 3] * 3));
+            const double* lb = C->lbox + 6 * l;
+            if (in_box(qo, lb, 1e-4) && ray_parity(&C->link_tri[l], qo, lb, lv, lt, NULL, 0, C->eps, &marginal))
+                inside = 1;
+        }
+    }
+    if (Tp != T) free(Tp);
+    C->contain[pose] = (unsigned char) inside;
+    if (C->band) C->band[pose] = (unsigned char) marginal;
+}
+
+int orc_containment(const orc_robot* R, const orc_scene* S, const u32* obstacle_tri_off, int n_obs, const float* q,
+                    int n, double eps, int threads, const unsigned char* skip, unsigned char* contain,
+                    unsigned char* band) {
+    cont_ctx C;
+    memset(&C, 0, sizeof(C));
+    C.R = R; C.S = S; C.ooff = obstacle_tri_off; C.n_obs = n_obs; C.q = q; C.eps = eps; C.skip = skip;
+    C.contain = contain; C.band = band;
+    float *lo, *hi;
+    tri_boxes(S->verts, S->tris, S->n_tris, &lo, &hi);
+    bvh_make(&C.scene_tri, S->n_tris, lo, hi);
+    C.tri_obs = (u32*) malloc(sizeof(u32) * (size_t) (S->n_tris ? S->n_tris : 1));
+    C.obox = (double*) malloc(sizeof(double) * 6 * (size_t) (n_obs ? n_obs : 1));
+    for (int o = 0; o < n_obs; ++o) {
+        double* b = C.obox + 6 * o;
+        b[0] = b[1] = b[2] = INFINITY; b[3] = b[4] = b[5] = -INFINITY;
+        for (u32 t = obstacle_tri_off[o]; t < obstacle_tri_off[o + 1]; ++t) {
+            C.tri_obs[t] = (u32) o;
+            for (int k = 0; k < 3; ++k)
+                for (int a = 0; a < 3; ++a) {
+                    double v = S->verts[S->tris[t * 3 + k] * 3 + a];
+                    if (v < b[a]) b[a] = v;
+                    if (v > b[3 + a]) b[3 + a] = v;
+                }
+        }
+    }
+    C.link_tri = (bvh_t*) calloc((size_t) R->n_links, sizeof(bvh_t));
+    C.lbox = (double*) malloc(sizeof(double) * 6 * (size_t) R->n_links);
+    for (int l = 0; l < R->n_links; ++l) {
+        int nt = (int) (R->link_tri_off[l + 1] - R->link_tri_off[l]);
+        const float* lv = R->link_verts + (size_t) R->link_vert_off[l] * 3;
+        tri_boxes(lv, R->link_tris + (size_t) R->link_tri_off[l] * 3, nt, &lo, &hi);
+        bvh_make(&C.link_tri[l], nt, lo, hi);
+        double* b = C.lbox + 6 * l;
+        b[0] = b[1] = b[2] = INFINITY; b[3] = b[4] = b[5] = -INFINITY;
+        for (u32 v = 0; v < R->link_vert_off[l + 1] - R->link_vert_off[l]; ++v)
+            for (int a = 0; a < 3; ++a) {
+                double x = lv[v * 3 + a];
+                if (x < b[a]) b[a] = x;
+                if (x > b[3 + a]) b[3 + a] = x;
+            }
+    }
+    run_pool(n, threads, cont_pose, &C, 16);
+    bvh_free(&C.scene_tri);
+    for (int l = 0; l < R->n_links; ++l) bvh_free(&C.link_tri[l]);
+    free(C.link_tri); free(C.lbox); free(C.obox); free(C.tri_obs);
+    return 0;
+}
+
 /* ------------------------------------------------------------- sweep checks */
 typedef struct {
     d3 a, b;        /* capsule axis (linear) */

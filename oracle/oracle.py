@@ -93,6 +93,8 @@ class Scene:
     def __init__(self, mesh):
         self.verts = _c(mesh.verts, np.float32)
         self.tris = _c(mesh.tris, np.uint32)
+        off = getattr(mesh, 'obstacle_tri_off', None)
+        self.obstacle_tri_off = _c(off if off is not None else [0, len(self.tris)], np.uint32)
         self.edges = unique_edges(self.tris)
         self.s = OrcScene(len(self.verts), _p(self.verts, F), len(self.tris), _p(self.tris, U), len(self.edges),
                           _p(self.edges, U))
@@ -144,6 +146,21 @@ def discrete(kind, robot, scene, q, eps=1e-5, threads=None, work=False):
         out['node_tests'] = arr['node_tests'].copy()
         out['prim_tests'] = arr['prim_tests'].copy()
     return out
+
+
+def containment(robot, scene, q, skip=None, eps=1e-5, threads=None):
+    """Containment of poses without a surface crossing (skip[pose] != 0 skips
+    a pose): dict(contain, band) - a link vertex inside an obstacle or an
+    obstacle vertex inside a link, by ray parity (no upstream counterpart)."""
+    q = _c(q, np.float32)
+    n = len(q)
+    contain = np.zeros(n, np.uint8)
+    band = np.zeros(n, np.uint8)
+    sk = None if skip is None else _c(np.asarray(skip) != 0, np.uint8)
+    off = scene.obstacle_tri_off
+    lib().orc_containment(C.byref(robot.s), C.byref(scene.s), _p(off, U), C.c_int(len(off) - 1), _p(q, F), C.c_int(n),
+                          D(eps), C.c_int(threads or threads_default()), _p(sk, B), _p(contain, B), _p(band, B))
+    return {'contain': contain, 'band': band}
 
 
 class PreparedDiscrete:

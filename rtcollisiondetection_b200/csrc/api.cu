@@ -193,7 +193,8 @@ struct GroupedBvh {
 };
 
 static void build_grouped(bool tris, const float* d_verts, const std::vector<uint32_t>& vert_off, const uint32_t* d_idx,
-                          const std::vector<uint32_t>& prim_off, uint32_t* d_err, cudaStream_t s, GroupedBvh& out) {
+                          const std::vector<uint32_t>& prim_off, uint32_t* d_err, cudaStream_t s, GroupedBvh& out,
+                          const uint32_t* d_tag = nullptr) {
     size_t groups = prim_off.size() - 1;
     uint32_t total = prim_off.back();
     size_t total_nodes = 0;
@@ -223,7 +224,8 @@ static void build_grouped(bool tris, const float* d_verts, const std::vector<uin
         out.roots[g] = r.root;
         out.max_depth = std::max(out.max_depth, r.depth);
         if (tris)
-            gather_tris(v, ix, perm.as<uint32_t>() + p0, n, p0, (uint32_t) g, out.prims.as<float4>() + 3ull * p0, s);
+            gather_tris(v, ix, perm.as<uint32_t>() + p0, n, p0, (uint32_t) g, d_tag ? d_tag + p0 : nullptr,
+                        out.prims.as<float4>() + 3ull * p0, s);
         else
             gather_edges(v, ix, perm.as<uint32_t>() + p0, n, p0, (uint32_t) g, out.prims.as<float4>() + 2ull * p0, s);
         node_off += n > 1 ? n - 1 : 0;
@@ -254,7 +256,7 @@ struct rtcd_scene {
     rtcd_ctx* ctx = nullptr;
     SceneDev dev{};
     GroupedBvh tri, edge;
-    DevBuf verts, tris, edges, obbs;
+    DevBuf verts, tris, edges, obbs, tri_obs, obs_box, obs_point;
     uint32_t n_tris = 0, n_edges = 0, n_obs = 0;
 };
 
@@ -277,7 +279,7 @@ struct rtcd_detector {
     bool timed_total_only = false;       // the last check timed only ev[0] -> ev_end (graph path)
     uint32_t blocks = 0;
     // discrete workspace
-    DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats;
+    DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats, contain;
     DevBuf cand, item_overflow, overflow_items, wave_counts;  // wavefront traversal
     uint32_t blocks_a = 0, blocks_b = 0, blocks_a_full = 0;
     uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
@@ -465,6 +467,10 @@ rtcd_status rtcd_robot_create(rtcd_ctx* ctx, const rtcd_robot_desc* d, rtcd_robo
         std::memcpy(ch.om, d->one_mask, 12ull * d->dof * sizeof(float));
         r->dev.n_links = L;
         r->dev.first_link = d->skip_base ? 1 : 0;
+        for (uint32_t l = 0; l < L; ++l) {  // the containment test's ray start: the link's first vertex
+            const float* v = d->link_verts + 3ull * voff[l];
+            r->dev.link_point[l] = voff[l + 1] > voff[l] ? make_float4(v[0], v[1], v[2], 0.f) : make_float4(0, 0, 0, 0);
+        }
         // OBBs (link frames)
         for (uint32_t l = 0; l < L; ++l) {
             float* o = r->dev.obb[l];
@@ -561,14 +567,40 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
             fit_obb(verts, idx, 1e-5f, obbs.data() + 16ull * o);
         }
         sc->n_obs = nob;
+        // per obstacle: the exact box of its vertices and one of its vertices (the
+        // containment test's ray start); per triangle: its obstacle
+        std::vector<uint32_t> tri_obs(std::max<uint32_t>(n_tris, 1), 0);
+        std::vector<float> obs_box(8ull * std::max<uint32_t>(nob, 1), 0.f), obs_point(4ull * std::max<uint32_t>(nob, 1), 0.f);
+        for (uint32_t o = 0; o < nob; ++o) {
+            float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+            for (uint32_t t = off[o]; t < off[o + 1]; ++t) {
+                tri_obs[t] = o;
+                for (int k = 0; k < 3; ++k)
+                    for (int a = 0; a < 3; ++a) {
+                        const float v = verts[3ull * tris[3ull * t + k] + a];
+                        lo[a] = std::min(lo[a], v);
+                        hi[a] = std::max(hi[a], v);
+                    }
+            }
+            for (int a = 0; a < 3; ++a) {
+                obs_box[8ull * o + a] = lo[a];
+                obs_box[8ull * o + 4 + a] = hi[a];
+            }
+            if (off[o + 1] > off[o])
+                for (int a = 0; a < 3; ++a) obs_point[4ull * o + a] = verts[3ull * tris[3ull * off[o]] + a];
+        }
         cudaStream_t s = ctx->stream;
         upload(sc->verts, verts, 3ull * n_verts, s);
         upload(sc->tris, tris, 3ull * n_tris, s);
         upload(sc->edges, edges.data(), edges.size(), s);
         upload(sc->obbs, obbs.data(), obbs.size(), s);
+        upload(sc->tri_obs, tri_obs.data(), tri_obs.size(), s);
+        upload(sc->obs_box, obs_box.data(), obs_box.size(), s);
+        upload(sc->obs_point, obs_point.data(), obs_point.size(), s);
         std::vector<uint32_t> v0 = {0, 0};
         std::vector<uint32_t> toff = {0, n_tris}, eoff = {0, sc->n_edges};
-        build_grouped(true, sc->verts.as<float>(), v0, sc->tris.as<uint32_t>(), toff, ctx->err.as<uint32_t>(), s, sc->tri);
+        build_grouped(true, sc->verts.as<float>(), v0, sc->tris.as<uint32_t>(), toff, ctx->err.as<uint32_t>(), s, sc->tri,
+                      sc->tri_obs.as<uint32_t>());
         build_grouped(false, sc->verts.as<float>(), v0, sc->edges.as<uint32_t>(), eoff, ctx->err.as<uint32_t>(), s,
                       sc->edge);
         SceneDev& dv = sc->dev;
@@ -581,6 +613,8 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
         dv.edge_root = sc->edge.roots[0];
         dv.n_edges = sc->n_edges;
         dv.obbs = sc->obbs.as<float>();
+        dv.obs_box = sc->obs_box.as<float4>();
+        dv.obs_point = sc->obs_point.as<float4>();
         dv.n_obs = nob;
         cuda_check(cudaStreamSynchronize(s), "scene upload");
         *out = sc.release();
@@ -799,12 +833,75 @@ void check_device_errors(rtcd_detector* d, cudaStream_t s) {
 
 // One discrete pass over poses [0, n) of d_q.  When `plain`, the item count
 // is read back and the traversal grid sized to it (the upstream shape).
-void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_hit, uint32_t* d_counts,
-                   uint32_t* d_bits, uint32_t flags, bool plain, cudaStream_t s) {
+// The traversal of one direction over the items of the current pass.
+static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t n, bool plain, uint32_t blocks,
+                     uint32_t flags, cudaStream_t s) {
     RobotDev& R = d->robot->dev;
     const uint32_t L = R.n_links;
-    const bool r2o = d->kind == RTCD_ROBOT_TO_OBS;
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 8, s), "memset");
+    if (flags & RTCD_CHECK_FUSED) {
+        launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+        return;
+    }
+    // stage A (+ B) -> heavy pass -> the thread-per-item kernel over items whose candidates overflowed
+    const size_t items_max = (size_t) n * L;
+    const uint32_t cap = (uint32_t) std::min<size_t>(std::max<size_t>(items_max * 128, 1u << 16), 1u << 26);
+    d->cand.ensure(8ull * cap);
+    d->item_overflow.ensure(items_max);
+    d->overflow_items.ensure(4ull * items_max);
+    d->wave_counts.ensure(4 * 4);
+    cuda_check(cudaMemsetAsync(d->item_overflow.p, 0, items_max, s), "memset");
+    cuda_check(cudaMemsetAsync(d->wave_counts.p, 0, 16, s), "memset");
+    uint32_t* wc = d->wave_counts.as<uint32_t>();  // [0] candidates, [1] overflowed items, [2] fallback work, [3] heavy
+    WaveArgs W{};
+    W.d = A;
+    W.cand = d->cand.as<uint2>();
+    W.cand_count = wc;
+    W.cand_cap = cap;
+    W.item_overflow = d->item_overflow.as<uint8_t>();
+    W.overflow_items = d->overflow_items.as<uint32_t>();
+    W.overflow_count = wc + 1;
+    W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (d->cfg.stage_b_form == 2 ? 4u : 64u);
+    W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
+                    : d->cfg.light_steps                ? d->cfg.light_steps
+                                                              : 32u;
+    if (W.light_steps) {
+        const uint32_t hcap = std::min<uint32_t>(cap, 1u << 24);
+        d->heavy.ensure(4ull * hcap);
+        W.heavy = d->heavy.as<uint32_t>();
+        W.heavy_cap = hcap;
+        W.heavy_count = wc + 3;
+        W.heavy_work = d->work.as<uint32_t>() + 1;
+    }
+    uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
+    const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
+    if (d->cfg.stage_b_form == 3 || d->cfg.stage_b_form == 0) {
+        const uint32_t full = stage_ab_blocks(r2o);
+        launch_stage_ab(r2o, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100), s);
+        launch_stage_b_heavy(r2o, R, d->scene->dev, W, share, s);
+    } else {
+        launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
+        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
+    }
+    DiscreteArgs F = A;
+    F.items = d->overflow_items.as<uint32_t>();
+    F.n_items = wc + 1;
+    F.work_counter = wc + 2;
+    launch_discrete(r2o, R, d->scene->dev, F, d->blocks, s);
+}
+
+// One discrete pass over poses [0, n) of d_q.  When `plain`, the item count
+// is read back and the traversal grid sized to it (the upstream shape).  With
+// RTCD_CHECK_TWO_WAY both directions run over the same items (ObsToRobot
+// first, so RobotToObs skips the poses it decided; with counts RobotToObs
+// first, its edge counts then ObsToRobot's hits added); with
+// RTCD_CHECK_CONTAINMENT the containment test runs over the poses left.
+void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_hit, uint32_t* d_counts,
+                   uint32_t* d_bits, uint32_t* d_contain, uint32_t flags, bool plain, cudaStream_t s) {
+    RobotDev& R = d->robot->dev;
+    const uint32_t L = R.n_links;
     const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
+    const bool two_way = (flags & RTCD_CHECK_TWO_WAY) != 0;
     d->T.ensure(48ull * n * L);
     d->mask.ensure((size_t) n * L);
     d->items.ensure(4ull * n * L);
@@ -828,74 +925,38 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         if (!cnt) return;
         blocks = (cnt + kTravThreads - 1) / kTravThreads;
     }
-    cuda_check(cudaMemsetAsync(d->work.p, 0, 8, s), "memset");
-    const bool fused = (flags & RTCD_CHECK_FUSED) != 0;
     DiscreteArgs A{};
     A.T = d->T.as<float4>();
     A.items = d->items.as<uint32_t>();
     A.n_items = d->count.as<uint32_t>();
     A.n_poses = n;
     A.pose_hit = d_hit;
-    A.counts = (counts && !r2o) ? d_counts : nullptr;
-    A.edge_bits = (counts && r2o) ? d_bits : nullptr;
     A.edge_words = (R.n_edges_total + 31) / 32;
     A.work_counter = d->work.as<uint32_t>();
     A.err = d->err.as<uint32_t>();
     A.stats = d->stats.as<unsigned long long>();
     A.want_counts = counts ? 1 : 0;
     if (timed) cuda_check(cudaEventRecord(d->ev[2], s), "event");
-    if (fused) {
-        launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
-    } else {
-        // stage A -> stage B -> the fused kernel over items whose candidates overflowed
-        const size_t items_max = (size_t) n * L;
-        const uint32_t cap = (uint32_t) std::min<size_t>(std::max<size_t>(items_max * 128, 1u << 16), 1u << 26);
-        d->cand.ensure(8ull * cap);
-        d->item_overflow.ensure(items_max);
-        d->overflow_items.ensure(4ull * items_max);
-        d->wave_counts.ensure(4 * 4);
-        cuda_check(cudaMemsetAsync(d->item_overflow.p, 0, items_max, s), "memset");
-        cuda_check(cudaMemsetAsync(d->wave_counts.p, 0, 16, s), "memset");
-        uint32_t* wc = d->wave_counts.as<uint32_t>();  // [0] candidates, [1] overflowed items, [2] fallback work
-        WaveArgs W{};
-        W.d = A;
-        W.cand = d->cand.as<uint2>();
-        W.cand_count = wc;
-        W.cand_cap = cap;
-        W.item_overflow = d->item_overflow.as<uint8_t>();
-        W.overflow_items = d->overflow_items.as<uint32_t>();
-        W.overflow_count = wc + 1;
-        W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (d->cfg.stage_b_form == 2 ? 4u : 64u);
-        W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
-                        : d->cfg.light_steps                ? d->cfg.light_steps
-                                                                  : 32u;
-        if (W.light_steps) {
-            const uint32_t hcap = std::min<uint32_t>(cap, 1u << 24);
-            d->heavy.ensure(4ull * hcap);
-            W.heavy = d->heavy.as<uint32_t>();
-            W.heavy_cap = hcap;
-            W.heavy_count = wc + 3;
-            W.heavy_work = d->work.as<uint32_t>() + 1;
-        }
-        uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
-        const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
-        if (d->cfg.stage_b_form == 3 || d->cfg.stage_b_form == 0) {
-            const uint32_t full = stage_ab_blocks(r2o);
-            launch_stage_ab(r2o, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100), s);
-            launch_stage_b_heavy(r2o, R, d->scene->dev, W, share, s);
-        } else {
-            launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
-            launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
-        }
-        DiscreteArgs F = A;
-        F.items = d->overflow_items.as<uint32_t>();
-        F.n_items = wc + 1;
-        F.work_counter = wc + 2;
-        launch_discrete(r2o, R, d->scene->dev, F, d->blocks, s);
+    const bool own_r2o = d->kind == RTCD_ROBOT_TO_OBS;
+    // the directions to run, in order
+    bool dirs[2] = {own_r2o, !own_r2o};
+    int n_dirs = 1;
+    if (two_way) {
+        n_dirs = 2;
+        dirs[0] = counts;  // counts: RobotToObs first (its popcount writes the counts), else ObsToRobot first
+        dirs[1] = !counts;
     }
+    for (int k = 0; k < n_dirs; ++k) {
+        const bool r2o = dirs[k];
+        DiscreteArgs Ad = A;
+        Ad.counts = (counts && !r2o) ? d_counts : nullptr;
+        Ad.edge_bits = (counts && r2o) ? d_bits : nullptr;
+        traverse(d, r2o, Ad, n, plain, blocks, flags, s);
+        if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);
+    }
+    if (d_contain) launch_contain(R, d->scene->dev, A, d_contain, s);
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     d->timed = timed;
-    if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);
 }
 
 void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags_out, uint32_t* counts_out,
@@ -925,11 +986,17 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
             d_counts = counts_out;
         }
         cuda_check(cudaMemsetAsync(d_counts, 0, 4ull * n, s), "memset");
-        if (d->kind == RTCD_ROBOT_TO_OBS) {
+        if (d->kind == RTCD_ROBOT_TO_OBS || (flags & RTCD_CHECK_TWO_WAY)) {
             d->edge_bits.ensure(4ull * n * words);
             d_bits = d->edge_bits.as<uint32_t>();
             cuda_check(cudaMemsetAsync(d_bits, 0, 4ull * n * words, s), "memset");
         }
+    }
+    uint32_t* d_contain = nullptr;
+    if (flags & RTCD_CHECK_CONTAINMENT) {
+        d->contain.ensure(4ull * n);
+        d_contain = d->contain.as<uint32_t>();
+        cuda_check(cudaMemsetAsync(d_contain, 0, 4ull * n, s), "memset");
     }
     d->last_items = 0;
     if (flags & RTCD_CHECK_PLAIN) {
@@ -938,17 +1005,17 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
             uint32_t m = std::min(fs, n - start);
             discrete_pass(d, d_q + (size_t) start * dof, m, d->pose_hit.as<uint32_t>() + start,
                           d_counts ? d_counts + start : nullptr, d_bits ? d_bits + (size_t) start * words : nullptr,
-                          flags, true, s);
+                          d_contain ? d_contain + start : nullptr, flags, true, s);
         }
     } else {
-        discrete_pass(d, d_q, n, d->pose_hit.as<uint32_t>(), d_counts, d_bits, flags, false, s);
+        discrete_pass(d, d_q, n, d->pose_hit.as<uint32_t>(), d_counts, d_bits, d_contain, flags, false, s);
     }
     uint8_t* d_flags = flags_out;
     if (host || !flags_out) {
         d->flags.ensure(n);
         d_flags = d->flags.as<uint8_t>();
     }
-    launch_flags(d->pose_hit.as<uint32_t>(), n, d_flags, s);
+    launch_flags(d->pose_hit.as<uint32_t>(), n, d_flags, s, d_contain);
     if (host) {
         d->pin_out.ensure(5ull * n + 16);
         uint8_t* pf = d->pin_out.as<uint8_t>();
@@ -967,6 +1034,8 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
 void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uint32_t n, uint8_t* flags_out,
                  uint8_t* seg_out, uint32_t* counts_out, uint32_t flags, cudaStream_t s) {
     RTCD_REQUIRE(traj_off, "traj_offsets required for sweep detectors");
+    RTCD_REQUIRE(!(flags & (RTCD_CHECK_CONTAINMENT | RTCD_CHECK_TWO_WAY)),
+                 "containment and two-way checks are for the discrete detectors");
     const bool host = (flags & RTCD_CHECK_HOST_BUFFERS) != 0;
     const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
     const bool quad = d->kind == RTCD_QUAD_SWEEP;

@@ -1333,14 +1333,134 @@ void launch_popcount_rows(const uint32_t* d_bits, uint32_t words, uint32_t rows,
     cuda_check(cudaGetLastError(), "k_popcount_rows");
 }
 
-__global__ void k_flags(const uint32_t* __restrict__ hit, uint32_t n, uint8_t* __restrict__ flags) {
+__global__ void k_flags(const uint32_t* __restrict__ hit, const uint32_t* __restrict__ contain, uint32_t n,
+                        uint8_t* __restrict__ flags) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) flags[i] = hit[i] ? 1 : 0;
+    if (i < n) flags[i] = (hit[i] ? 1 : 0) | (contain && contain[i] ? 2 : 0);
 }
 
-void launch_flags(const uint32_t* d_hit, uint32_t n, uint8_t* d_flags, cudaStream_t s) {
+// ---------------------------------------------------------------- containment
+// A pose whose meshes cross nowhere can still collide: a link inside an
+// obstacle, or an obstacle inside a link.  The reference's ray tests cannot
+// see that (they only follow surface crossings).  For every item of a pose
+// not yet hit and every obstacle whose OBB overlaps the link's (the cull's
+// SAT), a ray from one vertex of the link (of the obstacle) in a fixed
+// direction is clipped beyond the obstacle's box (the link's OBB) and its
+// crossings with that obstacle's triangles (the link's triangles) are
+// counted: an odd count means the vertex, and with no surface crossing the
+// whole mesh, is inside.  Both meshes are closed.
+__device__ __forceinline__ f3 contain_dir() { return mk(0.48f, 0.6f, 0.64f); }
+
+// Crossings of the segment p -> q with the triangles of one tree whose tag
+// (third float4's w) equals `tag` (any tag when tag == kNone).
+__device__ uint32_t count_crossings(const float4* __restrict__ nodes, const float4* __restrict__ prims, uint32_t root,
+                                    f3 p, f3 q, uint32_t tag, uint32_t* err) {
+    constexpr float kBoxTol = 2e-5f;
+    if (root == kNone) return 0;
+    const f3 d = q - p;
+    const f3 inv = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    uint32_t st[kStack];
+    int sp = 0;
+    st[sp++] = root;
+    uint32_t n = 0;
+    while (sp > 0) {
+        const uint32_t ref = st[--sp];
+        if (ref & kLeaf) {
+            const float4* t = prims + 3ull * (ref & ~kLeaf);
+            const float4 a = __ldg(t), b = __ldg(t + 1), c = __ldg(t + 2);
+            if (tag != kNone && __float_as_uint(c.w) != tag) continue;
+            int r = seg_tri_f32(p, q, f3of(a), f3of(b), f3of(c));
+            if (r == 2) r = seg_tri_f64(d3of(p), d3of(q), d3of(f3of(a)), d3of(f3of(b)), d3of(f3of(c))) ? 1 : 0;
+            n += (uint32_t) r;
+            continue;
+        }
+        Box bl, br;
+        uint32_t rl, rr;
+        load_node(nodes, ref, bl, br, rl, rr);
+        const bool hr = seg_box(p, inv, br, kBoxTol), hl = seg_box(p, inv, bl, kBoxTol);
+        if (sp + 2 > kStack) {
+            atomicOr(err, kErrStack);
+            break;
+        }
+        if (hr) st[sp++] = rr;
+        if (hl) st[sp++] = rl;
+    }
+    return n;
+}
+
+// Exit parameter of the ray p + t d from the box [lo, hi] (p inside it).
+__device__ __forceinline__ float box_exit(f3 p, f3 d, float4 lo, float4 hi) {
+    const float tx = d.x > 0 ? (hi.x - p.x) / d.x : (d.x < 0 ? (lo.x - p.x) / d.x : 3e38f);
+    const float ty = d.y > 0 ? (hi.y - p.y) / d.y : (d.y < 0 ? (lo.y - p.y) / d.y : 3e38f);
+    const float tz = d.z > 0 ? (hi.z - p.z) / d.z : (d.z < 0 ? (lo.z - p.z) / d.z : 3e38f);
+    return fminf(tx, fminf(ty, tz));
+}
+
+__global__ void __launch_bounds__(128) k_contain(const RobotDev R, const SceneDev S, const DiscreteArgs A,
+                                                 uint32_t* __restrict__ contain) {
+    constexpr float kPad = 1e-4f;  // the segments run this far past the boxes that hold the meshes
+    const uint32_t n_items = *A.n_items;
+    const f3 dir = contain_dir();
+    for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x) {
+        const uint32_t item = A.items[it];
+        const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
+        if (pose >= A.n_poses) {
+            atomicOr(A.err, kErrRange);
+            continue;
+        }
+        if (ld_flag(A.pose_hit + pose) || ld_flag(contain + pose)) continue;
+        float4 T[3];
+        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
+        const ObbW ob = world_obb(R.obb[link], T);
+        const float arad = sqrtf(dot(ob.h, ob.h)) + 2e-5f;
+        const f3 lp = xf(T, f3of(R.link_point[link]));
+        const float* lo = R.obb[link];
+        const f3 oc = mk(lo[0], lo[1], lo[2]);
+        const float lrad = sqrtf(lo[3] * lo[3] + lo[4] * lo[4] + lo[5] * lo[5]);
+        bool inside = false;
+        for (uint32_t o = 0; o < S.n_obs && !inside; ++o) {
+            const float* B = S.obbs + 16ull * o;
+            const f3 dc = mk(B[0], B[1], B[2]) - ob.c;
+            const float rr = arad + B[15];
+            if (dot(dc, dc) > rr * rr || !obb_overlap(ob, B)) continue;
+            // (a) the link's vertex inside obstacle o
+            const float4 blo = S.obs_box[2ull * o], bhi = S.obs_box[2ull * o + 1];
+            if (lp.x >= blo.x - kPad && lp.x <= bhi.x + kPad && lp.y >= blo.y - kPad && lp.y <= bhi.y + kPad &&
+                lp.z >= blo.z - kPad && lp.z <= bhi.z + kPad) {
+                const float t = fmaxf(box_exit(lp, dir, blo, bhi), 0.f) + 10.f * kPad;
+                const f3 q = lp + dir * t;
+                if (count_crossings(S.tri_nodes, S.tri_prims, S.tri_root, lp, q, o, A.err) & 1u) inside = true;
+            }
+            // (b) obstacle o's vertex inside the link
+            if (!inside) {
+                const f3 op = xf_inv(T, f3of(S.obs_point[o]));
+                const f3 r = op - oc;
+                const float len = sqrtf(dot(r, r));
+                if (len <= lrad + kPad) {
+                    const f3 q = op + dir * (len + lrad + 10.f * kPad);
+                    if (count_crossings(R.tri_nodes, R.tri_prims, R.tri_root[link], op, q, kNone, A.err) & 1u)
+                        inside = true;
+                }
+            }
+        }
+        if (inside) atomicExch(contain + pose, 1u);
+    }
+}
+
+void launch_contain(const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t* d_contain, cudaStream_t s) {
+    static const uint32_t blocks = [] {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contain, 128, 0);
+        return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
+    }();
+    k_contain<<<blocks, 128, 0, s>>>(R, S, A, d_contain);
+    cuda_check(cudaGetLastError(), "k_contain");
+}
+
+void launch_flags(const uint32_t* d_hit, uint32_t n, uint8_t* d_flags, cudaStream_t s, const uint32_t* d_contain) {
     if (!n) return;
-    k_flags<<<(n + 255) / 256, 256, 0, s>>>(d_hit, n, d_flags);
+    k_flags<<<(n + 255) / 256, 256, 0, s>>>(d_hit, d_contain, n, d_flags);
     cuda_check(cudaGetLastError(), "k_flags");
 }
 

@@ -93,8 +93,9 @@ LbvhResult build_lbvh(const float4* d_lo, const float4* d_hi, uint32_t n, float4
 void tri_boxes(const float* d_verts, const uint32_t* d_tris, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s);
 void edge_boxes(const float* d_verts, const uint32_t* d_edges, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s);
 // Sorted triangles: 3 float4 per triangle (v0 | id, v1 | group, v2 | 0).
+// Triangles in tree order: 3 float4, w = original index, group, tag[index] (0 without tags).
 void gather_tris(const float* d_verts, const uint32_t* d_tris, const uint32_t* d_perm, uint32_t n, uint32_t id_base,
-                 uint32_t group, float4* d_out, cudaStream_t s);
+                 uint32_t group, const uint32_t* d_tag, float4* d_out, cudaStream_t s);
 // Sorted edges: 2 float4 per edge (a | id, b | group).
 void gather_edges(const float* d_verts, const uint32_t* d_edges, const uint32_t* d_perm, uint32_t n, uint32_t id_base,
                   uint32_t group, float4* d_out, cudaStream_t s);

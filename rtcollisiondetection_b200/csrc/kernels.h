@@ -17,6 +17,7 @@ struct RobotDev {
     const float4* edge_prims;       // 2 float4 per edge; w of the first = global edge id
     uint32_t edge_root[kMaxLinks];
     uint32_t n_edges_total;
+    float4 link_point[kMaxLinks];   // one vertex of each link mesh (link frame)
     const float4* spheres;          // local centre xyz, radius w
     const uint32_t* sphere_link;
     uint32_t n_spheres;
@@ -33,7 +34,9 @@ struct SceneDev {
     uint32_t edge_root;
     uint32_t n_edges;
     const float* obbs;  // 16 floats per obstacle: centre(3), half(3), axes(9), bounding radius
-    uint32_t n_obs;
+    const float4* obs_box;    // [obstacle][2]: exact box of its vertices (lo, hi)
+    const float4* obs_point;  // [obstacle]: one of its vertices
+    uint32_t n_obs;           // scene triangles carry their obstacle in the third float4's w
 };
 
 struct DiscreteArgs {
@@ -102,7 +105,11 @@ void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t
 void launch_discrete(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t blocks,
                      cudaStream_t s);
 void launch_popcount_rows(const uint32_t* d_bits, uint32_t words, uint32_t rows, uint32_t* d_out, cudaStream_t s);
-void launch_flags(const uint32_t* d_hit, uint32_t n, uint8_t* d_flags, cudaStream_t s);
+// flags[i] = (hit[i] != 0) | 2 * (contain[i] != 0); contain may be NULL.
+void launch_flags(const uint32_t* d_hit, uint32_t n, uint8_t* d_flags, cudaStream_t s,
+                  const uint32_t* d_contain = nullptr);
+// Containment of the items' poses not yet hit (sets contain[pose] = 1).
+void launch_contain(const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t* d_contain, cudaStream_t s);
 uint32_t discrete_persistent_blocks(bool robot_to_obs);
 
 // ---- sweeps

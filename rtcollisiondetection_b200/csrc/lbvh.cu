@@ -87,7 +87,7 @@ void edge_boxes(const float* d_verts, const uint32_t* d_edges, uint32_t n, float
 
 __global__ void k_gather_tris(const float* __restrict__ v, const uint32_t* __restrict__ t,
                               const uint32_t* __restrict__ perm, uint32_t n, uint32_t id_base, uint32_t group,
-                              float4* out) {
+                              const uint32_t* __restrict__ tag, float4* out) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t p = perm[i];
@@ -96,7 +96,7 @@ __global__ void k_gather_tris(const float* __restrict__ v, const uint32_t* __res
     const float* c = v + 3ull * t[3ull * p + 2];
     out[3ull * i] = make_float4(a[0], a[1], a[2], __uint_as_float(id_base + p));
     out[3ull * i + 1] = make_float4(b[0], b[1], b[2], __uint_as_float(group));
-    out[3ull * i + 2] = make_float4(c[0], c[1], c[2], 0.f);
+    out[3ull * i + 2] = make_float4(c[0], c[1], c[2], __uint_as_float(tag ? tag[p] : 0u));
 }
 
 __global__ void k_gather_edges(const float* __restrict__ v, const uint32_t* __restrict__ e,
@@ -112,9 +112,9 @@ __global__ void k_gather_edges(const float* __restrict__ v, const uint32_t* __re
 }
 
 void gather_tris(const float* d_verts, const uint32_t* d_tris, const uint32_t* d_perm, uint32_t n, uint32_t id_base,
-                 uint32_t group, float4* d_out, cudaStream_t s) {
+                 uint32_t group, const uint32_t* d_tag, float4* d_out, cudaStream_t s) {
     if (!n) return;
-    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_tris, d_perm, n, id_base, group, d_out);
+    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_verts, d_tris, d_perm, n, id_base, group, d_tag, d_out);
     cuda_check(cudaGetLastError(), "k_gather_tris");
 }
 

@@ -28,6 +28,8 @@ CHECK_NO_ENDPOINTS = 1 << 4
 CHECK_TIMING = 1 << 5
 CHECK_FUSED = 1 << 6
 CHECK_GRAPH = 1 << 7
+CHECK_CONTAINMENT = 1 << 8
+CHECK_TWO_WAY = 1 << 9
 
 STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
           4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}

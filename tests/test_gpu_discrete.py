@@ -162,3 +162,75 @@ def test_graph_replay_matches_direct_path(setup, panda, name):
             ref = ref_det.check(q, counts=True)
             assert np.array_equal(fd.cpu().numpy(), ref['flags']), seed
             assert np.array_equal(cd.cpu().numpy().astype(np.uint32), ref['counts']), seed
+
+
+def _tiny_box_scene(n_boxes, seed, extent=0.012):
+    """Small cubes scattered over the robot's reach, plus the small shelf scene."""
+    rng = np.random.default_rng(seed)
+    base = scenes.discrete_small()
+    verts, tris, off = [base.verts], [base.tris], list(base.obstacle_tri_off)
+    nv = len(base.verts)
+    for _ in range(n_boxes):
+        c = rng.uniform([-0.6, -0.6, 0.0], [0.6, 0.6, 1.0])
+        v, t = scenes.box_mesh(c, [extent] * 3)
+        verts.append(v.astype(np.float32))
+        tris.append(t + nv)
+        nv += len(v)
+        off.append(off[-1] + len(t))
+    return scenes.Mesh(np.concatenate(verts), np.concatenate(tris), off)
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_containment_matches_oracle(ctx, panda, name, okind):
+    """RTCD_CHECK_CONTAINMENT: flag 1 where a surface crossing exists, 2 where
+    the oracle finds a link inside an obstacle or an obstacle inside a link
+    (ray parity) and no crossing; compared outside both bands."""
+    mesh = _tiny_box_scene(400, seed=7)
+    robot = rtcd.Robot(ctx, panda)
+    sc = rtcd.Scene.from_mesh(ctx, mesh)
+    q = scenes.uniform_poses(panda, 512, seed=8)
+    det = rtcd.Detector(ctx, name, robot, sc)
+    out = det.check(q, flags=rtcd.CHECK_CONTAINMENT)['flags']
+    plain = det.check(q)['flags']
+    assert np.array_equal(out & 1, plain)                      # the surface flags are unchanged
+    orob, osc = O.Robot(panda), O.Scene(mesh)
+    ref = O.discrete(okind, orob, osc, q)
+    cont = O.containment(orob, osc, q, skip=ref['hit'])
+    ok = (ref['band'] == 0) & (cont['band'] == 0)
+    assert np.array_equal(out[ok] & 1, ref['hit'][ok])
+    assert np.array_equal((out[ok] >> 1) & 1, cont['contain'][ok])
+    assert cont['contain'][ok].sum() >= 3                       # the case is exercised
+    assert ok.mean() > 0.95
+
+
+def test_containment_enclosing_box(ctx, panda):
+    robot = rtcd.Robot(ctx, panda)
+    v, t = scenes.box_mesh([0, 0, 0.5], [6, 6, 6])
+    sc = rtcd.Scene.from_mesh(ctx, scenes.Mesh(v, t, [0, 12]))
+    q = scenes.uniform_poses(panda, 64, seed=9)
+    for name in ('ObsToRobot', 'RobotToObs'):
+        det = rtcd.Detector(ctx, name, robot, sc)
+        assert det.check(q)['flags'].sum() == 0
+        assert (det.check(q, flags=rtcd.CHECK_CONTAINMENT)['flags'] == 2).all()
+        assert (det.check(q, flags=rtcd.CHECK_CONTAINMENT | rtcd.CHECK_TWO_WAY)['flags'] == 2).all()
+
+
+@pytest.mark.parametrize('name', ['ObsToRobot', 'RobotToObs'])
+def test_two_way_is_union_of_directions(setup, panda, name):
+    """RTCD_CHECK_TWO_WAY: flags = ObsToRobot | RobotToObs, counts = their sum,
+    from either detector kind and through the graph path."""
+    robot, scene, (orob, oscene) = setup
+    q = scenes.uniform_poses(panda, 700, seed=12)
+    o2r = rtcd.Detector(robot.ctx, 'ObsToRobot', robot, scene).check(q, counts=True)
+    r2o = rtcd.Detector(robot.ctx, 'RobotToObs', robot, scene).check(q, counts=True)
+    det = rtcd.Detector(robot.ctx, name, robot, scene)
+    both = det.check(q, counts=True, flags=rtcd.CHECK_TWO_WAY)
+    assert np.array_equal(both['flags'], o2r['flags'] | r2o['flags'])
+    assert np.array_equal(both['counts'], o2r['counts'] + r2o['counts'])
+    assert np.array_equal(det.check(q, flags=rtcd.CHECK_TWO_WAY)['flags'], both['flags'])
+    assert np.array_equal(det.check(q, flags=rtcd.CHECK_TWO_WAY | rtcd.CHECK_PLAIN)['flags'], both['flags'])
+    ref_h = O.discrete(O.OBS_TO_ROBOT, orob, oscene, q)
+    ref_r = O.discrete(O.ROBOT_TO_OBS, orob, oscene, q)
+    ok = (ref_h['band'] == 0) & (ref_r['band'] == 0)
+    assert np.array_equal(both['flags'][ok], (ref_h['hit'] | ref_r['hit'])[ok])
+    assert (both['flags'] > o2r['flags']).sum() + (both['flags'] > r2o['flags']).sum() > 0

@@ -219,3 +219,74 @@ def test_sweep_quad_oracle_segments_and_endpoints(panda):
     assert a['seg_off'][-1] == b['seg_off'][-1] + 8
     # dropping the end spheres can only remove hits
     assert np.all(b['traj_hit'] <= a['traj_hit'])
+
+
+def _winding(p, tri):
+    """Generalised winding number of a closed triangle mesh at p (solid angles,
+    Van Oosterom & Strackee): about 1 inside, 0 outside - independent of ray
+    parity."""
+    a, b, c = tri[:, 0] - p, tri[:, 1] - p, tri[:, 2] - p
+    la, lb, lc = (np.linalg.norm(x, axis=1) for x in (a, b, c))
+    num = np.einsum('ij,ij->i', a, np.cross(b, c))
+    den = la * lb * lc + np.einsum('ij,ij->i', a, b) * lc + np.einsum('ij,ij->i', b, c) * la + \
+        np.einsum('ij,ij->i', c, a) * lb
+    return float(2.0 * np.arctan2(num, den).sum() / (4 * np.pi))
+
+
+def test_containment_oracle_against_winding_numbers(panda):
+    """A 1 mm box whose first vertex is a link's vertex-mean point (or a point
+    pushed out from it): the oracle's
+    ray-parity containment equals the winding-number truth (inside some
+    checked link), for every pose without a surface crossing."""
+    q = scenes.uniform_poses(panda, 40, seed=5)
+    T = O.fk(panda, q)
+    R = O.Robot(panda)
+    checked = inside_seen = 0
+    for i in range(len(q)):
+        l = 1 + i % 7
+        lv = panda['link_verts'][panda['link_vert_off'][l]:panda['link_vert_off'][l + 1]].astype(np.float64)
+        Tl = T[i, l].reshape(3, 4)
+        P = lv.mean(axis=0) @ Tl[:, :3].T + Tl[:, 3]
+        if i % 2:  # half the points pushed out to 3-12 cm from the link's centre
+            d = np.random.default_rng(i).normal(size=3)
+            P = P + (0.03 + 0.09 * (i % 4) / 3) * d / np.linalg.norm(d)
+        v, t = scenes.box_mesh(P + 0.0005, [0.001] * 3)
+        mesh = scenes.Mesh(v, t, [0, 12])
+        assert np.allclose(mesh.verts[0], P, atol=1e-6)
+        S = O.Scene(mesh)
+        hit = O.discrete(O.ROBOT_TO_OBS, R, S, q[i:i + 1])['hit'] | O.discrete(O.OBS_TO_ROBOT, R, S, q[i:i + 1])['hit']
+        if hit[0]:
+            continue
+        w = []
+        P32 = mesh.verts[0].astype(np.float64)
+        for k in range(1, 8):
+            Tk = T[i, k].reshape(3, 4)
+            kv = panda['link_verts'][panda['link_vert_off'][k]:panda['link_vert_off'][k + 1]].astype(np.float64)
+            kt = panda['link_tris'][panda['link_tri_off'][k]:panda['link_tri_off'][k + 1]]
+            w.append(_winding(P32, (kv @ Tk[:, :3].T + Tk[:, 3])[kt]))
+        w = np.abs(np.array(w))
+        if np.any(np.abs(w - 0.5) < 0.2):
+            continue  # too close to a surface for either method to be sharp
+        out = O.containment(R, S, q[i:i + 1])
+        if out['band'][0]:
+            continue
+        assert out['contain'][0] == int(np.any(w > 0.5)), (i, w)
+        checked += 1
+        inside_seen += int(out['contain'][0])
+    assert checked >= 20 and 0 < inside_seen < checked
+
+
+def test_containment_oracle_enclosing_box(panda):
+    """The robot inside one large box: no surface crossing, every pose contained;
+    far away: nothing."""
+    q = scenes.uniform_poses(panda, 16, seed=6)
+    R = O.Robot(panda)
+    v, t = scenes.box_mesh([0, 0, 0.5], [6, 6, 6])
+    S = O.Scene(scenes.Mesh(v, t, [0, 12]))
+    assert O.discrete(O.ROBOT_TO_OBS, R, S, q)['hit'].sum() == 0
+    out = O.containment(R, S, q)
+    assert out['contain'].all() and not out['band'].any()
+    v, t = scenes.box_mesh([20, 0, 0], [1, 1, 1])
+    S = O.Scene(scenes.Mesh(v, t, [0, 12]))
+    assert O.containment(R, S, q)['contain'].sum() == 0
+    assert O.containment(R, S, q, skip=np.ones(16))['contain'].sum() == 0
