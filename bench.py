@@ -57,12 +57,30 @@ CONFIGS = {
     'c4': dict(kind='Quadratic', n=4096, scene='sweep', wp=(8, 64),
                workload='Quadratic sweep, 4,096 trajectories of 8-64 waypoints (log-uniform), 64 spheres, '
                         '49,744-tri scene'),
+    # the reference's own benchmark shelves (models/curobo, placements of its scene headers), batch 4096
+    'ref_simple_r2o': dict(kind='RobotToObs', n=4096, scene='ref_simple',
+                           workload='RobotToObs, 4,096 uniform poses, reference simple shelf (15,008 tris)'),
+    'ref_simple_o2r': dict(kind='ObsToRobot', n=4096, scene='ref_simple',
+                           workload='ObsToRobot, 4,096 uniform poses, reference simple shelf (15,008 tris)'),
+    'ref_dense_r2o': dict(kind='RobotToObs', n=4096, scene='ref_dense',
+                          workload='RobotToObs, 4,096 uniform poses, reference dense shelf (202,330 tris)'),
+    'ref_dense_o2r': dict(kind='ObsToRobot', n=4096, scene='ref_dense',
+                          workload='ObsToRobot, 4,096 uniform poses, reference dense shelf (202,330 tris)'),
+    'ref_dense_linear': dict(kind='Linear', n=4096, scene='ref_dense', wp=16,
+                             workload='Linear sweep, 4,096 trajectories x 16 waypoints, reference dense shelf'),
+    'ref_dense_quad': dict(kind='Quadratic', n=4096, scene='ref_dense', wp=(8, 16),
+                           workload='Quadratic sweep, 4,096 trajectories of 8-16 waypoints (4-8 control points), '
+                                    'reference dense shelf'),
 }
 
 
 def make_inputs(cfg, rank, scenes):
     model = scenes.load_panda()
-    mesh = {'dense': scenes.discrete_dense, 'small': scenes.discrete_small, 'sweep': scenes.sweep_scene}[cfg['scene']]()
+    if cfg['scene'].startswith('ref_'):
+        mesh = scenes.reference_scene(cfg['scene'][4:])
+    else:
+        mesh = {'dense': scenes.discrete_dense, 'small': scenes.discrete_small,
+                'sweep': scenes.sweep_scene}[cfg['scene']]()
     spheres = scenes.synth_spheres(model) if cfg['kind'] in ('Linear', 'Quadratic') else None
     if cfg['kind'] in ('Linear', 'Quadratic'):
         wp = cfg['wp']
@@ -515,8 +533,8 @@ def main():
     form = tuned.get('stage_b_form', 0)
     if sweep:
         span = 'k_sweep + k_sweep_heavy'
-    elif form in (0, 3):
-        span = 'k_stage_ab + k_stage_b_heavy + k_discrete (overflow)'
+    elif form in (0, 3, 4):
+        span = 'k_stage_ab + k_stage_b (deferred) + k_stage_b_heavy + k_discrete (overflow)'
     else:
         span = 'k_stage_a + k_stage_b%s + k_stage_b_heavy + k_discrete (overflow)' % ('_packet' if form == 2 else '')
     traffic = None
@@ -556,10 +574,11 @@ def main():
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
-        # discrete: k_fk_poses, k_cull, k_select_u8, k_stage_ab (fused form) or k_stage_a + k_stage_b,
-        # k_stage_b_heavy, k_discrete (overflow), k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep,
-        # k_sweep_heavy, k_flags x 2
-        'gpu_launches': args.steps * ((7 if tuned.get('stage_b_form', 0) in (0, 3) else 8) if not sweep
+        # discrete: k_fk_poses, k_cull, k_select_u8, then per direction k_stage_ab + k_stage_b (deferred
+        # candidates) or k_stage_a + k_stage_b, k_stage_b_heavy, k_discrete (overflow); (k_contain), k_flags;
+        # sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
+        'gpu_launches': args.steps * ((3 + (2 if args.two_way else 1) * 4
+                                       + (1 if args.containment else 0) + 1) if not sweep
                                       else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in spans])),
                       'cull': float(np.mean([s['ms_cull'] for s in spans])), 'traverse': t_trav},

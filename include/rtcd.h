@@ -117,11 +117,14 @@ typedef struct {
     uint32_t stage_b_form;           /* discrete stage B: 1 = one lane per candidate, 2 = 32-candidate packets
                                         that share each link-BVH node load, 3 = stages A and B fused in one
                                         warp per item (an item stops generating candidates once its pose
-                                        is hit); 0 = 3 (the autotuner tries all three) */
+                                        is hit), 4 = 3 with packet descents of the link tree; 0 = 3 (the
+                                        autotuner tries all four) */
     uint32_t stage_b_chunk;          /* discrete stage B: consecutive candidates one lane takes in order (lanes
-                                        form) or 32-candidate groups one warp takes (packets); a pose's
-                                        candidates then spread over few workers that stop at its first hit;
-                                        0 = 64 lanes / 4 packets; at most 4096 */
+                                        form) or 32-candidate groups one warp takes (packets), so a pose's
+                                        candidates spread over few workers that stop at its first hit; for
+                                        the fused forms, the stage-B steps (32 candidates each) an item runs
+                                        in its warp before its further candidates go to a one-lane pass over
+                                        the whole GPU; 0 = 64 lanes / 4 packets / 8 steps; at most 4096 */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -187,7 +190,7 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
  * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
- * then, for the discrete kinds, the three stage B forms, the first two at
+ * then, for the discrete kinds, the four stage B forms, the first two at
  * chunk lengths from 1 to 256 candidates (coordinate descent; sweeps are
  * timed with segment flags on)
  * - times the traversal with device events (median of three after a

@@ -343,7 +343,7 @@ static void apply_launch_shape(rtcd_detector* d) {
     uint32_t per_sm = d->cfg.traverse_blocks_per_sm ? std::min(d->cfg.traverse_blocks_per_sm, fit) : fit;
     const uint32_t pct = d->cfg.residency_percent;
     if (pct > 100) fail(RTCD_ERR_INVALID_ARGUMENT, "residency_percent must be at most 100");
-    if (d->cfg.stage_b_form > 3) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_form must be 0, 1, 2 or 3");
+    if (d->cfg.stage_b_form > 4) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_form must be 0 to 4");
     if (d->cfg.stage_b_chunk > 4096) fail(RTCD_ERR_INVALID_ARGUMENT, "stage_b_chunk must be at most 4096");
     const uint32_t sms = (uint32_t) device_sm_count();
     if (pct) per_sm = std::max(1u, per_sm * pct / 100);
@@ -861,24 +861,30 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
     W.item_overflow = d->item_overflow.as<uint8_t>();
     W.overflow_items = d->overflow_items.as<uint32_t>();
     W.overflow_count = wc + 1;
-    W.chunk = d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : (d->cfg.stage_b_form == 2 ? 4u : 64u);
+    const bool fused_form = d->cfg.stage_b_form == 0 || d->cfg.stage_b_form >= 3;
+    // lanes / packets: the chunk; fused forms: stage_b_chunk is the item's stage-B step budget
+    W.chunk = (!fused_form && d->cfg.stage_b_chunk) ? d->cfg.stage_b_chunk : (d->cfg.stage_b_form == 2 ? 4u : 64u);
+    W.item_steps = fused_form ? (d->cfg.stage_b_chunk ? d->cfg.stage_b_chunk : 8u) : 0xFFFFFFFFu;
     W.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                     : d->cfg.light_steps                ? d->cfg.light_steps
                                                               : 32u;
     if (W.light_steps) {
         const uint32_t hcap = std::min<uint32_t>(cap, 1u << 24);
-        d->heavy.ensure(4ull * hcap);
-        W.heavy = d->heavy.as<uint32_t>();
+        d->heavy.ensure(8ull * hcap);
+        W.heavy = d->heavy.as<uint2>();
         W.heavy_cap = hcap;
         W.heavy_count = wc + 3;
         W.heavy_work = d->work.as<uint32_t>() + 1;
     }
     uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
     const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
-    if (d->cfg.stage_b_form == 3 || d->cfg.stage_b_form == 0) {
-        const uint32_t full = stage_ab_blocks(r2o);
-        launch_stage_ab(r2o, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100), s);
-        launch_stage_b_heavy(r2o, R, d->scene->dev, W, share, s);
+    if (fused_form) {
+        const bool packets = d->cfg.stage_b_form == 4;
+        const uint32_t full = stage_ab_blocks(r2o, packets);
+        launch_stage_ab(r2o, packets, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100),
+                        s);
+        // the one-lane pass over the candidates crowded items deferred, then the heavy pass
+        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, false, s);
     } else {
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
         launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
@@ -1397,12 +1403,13 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         }
         if (discrete) {
             const rtcd_config base = best;
-            for (uint32_t form : {1u, 2u, 3u})
+            for (uint32_t form : {1u, 2u, 3u, 4u})
                 for (uint32_t chunk : {1u, 16u, 64u, 256u}) {
-                    if (form == 3 && chunk != 1) continue;  // the fused form has no chunk
                     rtcd_config c = base;
                     c.stage_b_form = form;
-                    c.stage_b_chunk = form == 2 ? std::max(1u, chunk / 16) : chunk;
+                    // lanes: candidates per lane; packets: groups per warp; fused: the item's
+                    // stage-B step budget (1, 4, 16, 64)
+                    c.stage_b_chunk = form == 2 ? std::max(1u, chunk / 16) : (form >= 3 ? std::max(1u, chunk / 4) : chunk);
                     time_cfg(c);
                 }
         }

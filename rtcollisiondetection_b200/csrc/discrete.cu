@@ -732,7 +732,8 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
     for (uint32_t cc = (blockIdx.x * blockDim.x + threadIdx.x) * K; cc < total; cc += gridDim.x * blockDim.x * K)
     for (uint32_t c = cc; c < min(cc + K, total); ++c) {
         StageBCand C;
-        if (!stage_b_setup<R2O>(R, S, W, W.cand[c], C, n_skip, n_rej)) continue;
+        const uint2 cd = W.cand[c];
+        if (!stage_b_setup<R2O>(R, S, W, cd, C, n_skip, n_rej)) continue;
         ++n_acc;
         int sp = 0;
         st[sp++] = C.lroot;
@@ -741,7 +742,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
             if (++steps > budget) {
                 const uint32_t slot = atomicAdd(W.heavy_count, 1u);
                 if (slot < W.heavy_cap) {
-                    W.heavy[slot] = c;
+                    W.heavy[slot] = cd;
                     hits = 0;
                     break;
                 }
@@ -841,13 +842,14 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
                     if (lane == leader) base = atomicAdd(W.heavy_count, n);
                     base = __shfl_sync(0xffffffffu, base, leader);
                     if (base + n <= W.heavy_cap) {
-                        if (in) W.heavy[base + __popc(grp & lt)] = c;
+                        if (in) W.heavy[base + __popc(grp & lt)] = cd;
                         spilled = true;
                         break;
                     }
                     // the heavy list is full: blank the reserved slots below the
                     // capacity (the heavy pass reads up to it) and finish here
-                    if (in && base + __popc(grp & lt) < W.heavy_cap) W.heavy[base + __popc(grp & lt)] = kNone;
+                    if (in && base + __popc(grp & lt) < W.heavy_cap)
+                        W.heavy[base + __popc(grp & lt)] = make_uint2(kNone, kNone);
                     steps = 0;
                 }
                 if (!A.want_counts && (steps & 15) == 0) {  // decided meanwhile by another candidate?
@@ -912,13 +914,16 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
 // to the heavy pass).  An item whose pose is found in collision stops
 // generating candidates: most colliding items are decided after their first
 // few candidates, so most of stage A's traversal and candidate traffic is
-// never spent on them.
+// never spent on them.  PACKET: the 32 buffered candidates (one item, so one
+// link tree) descend the link LBVH together - one node load per step for the
+// warp, each lane testing its own primitive - which shares the top levels of
+// the link tree when many small scene primitives crowd one link.
 constexpr int kAbWarps = 4;
 constexpr int kCandBuf = 96;  // < 32 waiting + up to 64 added by one frontier step
 
 // Capped at 5 resident blocks per SM worth of registers (a few spills, more
 // warps to hide the node-load latency; measured on the 65,536-pose workload).
-template <bool R2O>
+template <bool R2O, bool PACKET>
 __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
     constexpr float kBoxTol = 2e-5f;
     __shared__ uint32_t s_front[kAbWarps][kFrontier];
@@ -960,6 +965,8 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                           fabsf(ob.ax[0].y) * ob.h.x + fabsf(ob.ax[1].y) * ob.h.y + fabsf(ob.ax[2].y) * ob.h.z,
                           fabsf(ob.ax[0].z) * ob.h.x + fabsf(ob.ax[1].z) * ob.h.y + fabsf(ob.ax[2].z) * ob.h.z);
         int sp = 1, nc = 0;
+        uint32_t nbs = 0;  // stage-B steps this item ran in its warp
+        bool overflow = false;
         if (lane == 0) fr[0] = wroot;
         __syncwarp();
         while (true) {
@@ -968,9 +975,91 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 nc -= take;
                 const uint32_t prim = lane < take ? cb[nc + lane] : kNone;
                 __syncwarp();
+                if (!A.want_counts && nbs >= W.item_steps) {
+                    // a crowded item: its further candidates go to the one-lane pass, which
+                    // spreads them over the whole GPU instead of this warp's serial steps
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(W.cand_count, (uint32_t) take);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (base + (uint32_t) take <= W.cand_cap) {
+                        if (prim != kNone) W.cand[base + lane] = make_uint2(item, prim);
+                        continue;
+                    }
+                    // no room: blank the reserved slots below the capacity and hand the whole
+                    // item to the thread-per-item kernel (flags only, so re-running is safe)
+                    if (prim != kNone && base + lane < W.cand_cap) W.cand[base + lane] = make_uint2(kNone, kNone);
+                    overflow = true;
+                    break;
+                }
+                ++nbs;
                 bool hit = false;
                 StageBCand C;
-                if (prim != kNone && stage_b_setup<R2O>(R, S, W, make_uint2(item, prim), C, n_skip, n_rej, false)) {
+                if (PACKET) {
+                    const bool live =
+                        prim != kNone && stage_b_setup<R2O>(R, S, W, make_uint2(item, prim), C, n_skip, n_rej, false);
+                    const uint32_t grp = __ballot_sync(0xffffffffu, live);
+                    if (live) ++n_acc;
+                    if (grp) {
+                        int bsp = 0;
+                        st[bsp++] = R2O ? R.edge_root[link] : R.tri_root[link];
+                        uint32_t steps = 0, hits = 0;
+                        bool spilled = false;
+                        const uint32_t rank = __popc(grp & lt), np = __popc(grp);
+                        while (bsp > 0) {
+                            if (++steps > 4u * budget) {  // hand the packet's candidates to the heavy pass
+                                uint32_t hbase = 0;
+                                if (lane == 0) hbase = atomicAdd(W.heavy_count, np);
+                                hbase = __shfl_sync(0xffffffffu, hbase, 0);
+                                const bool fits = hbase + np <= W.heavy_cap;
+                                // heavy slots below the capacity are always written (blank when the
+                                // packet stays here), since the heavy pass reads up to it
+                                if (live && hbase + rank < W.heavy_cap)
+                                    W.heavy[hbase + rank] = fits ? make_uint2(item, prim) : make_uint2(kNone, kNone);
+                                if (fits) {
+                                    spilled = true;
+                                    break;
+                                }
+                                steps = 0;  // no room: finish the packet here
+                            }
+                            const uint32_t ref = st[--bsp];
+                            if (ref & kLeaf) {
+                                const uint32_t li = ref & ~kLeaf;
+                                bool h = false;
+                                if (live) {
+                                    ++n_leaf;
+                                    h = stage_b_leaf<R2O>(lp, wp, li, C, A.stats);
+                                }
+                                if (__any_sync(0xffffffffu, h)) {
+                                    hit = true;
+                                    if (!A.want_counts) break;
+                                    if (h) {
+                                        if (R2O) {
+                                            const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
+                                            atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5),
+                                                     1u << (eid & 31));
+                                        } else {
+                                            ++hits;
+                                        }
+                                    }
+                                }
+                                continue;
+                            }
+                            Box bl, br;
+                            uint32_t rl, rr;
+                            load_node(ln, ref, bl, br, rl, rr);
+                            if (live) n_node += 2;
+                            const bool hr = live && stage_b_node<R2O>(C, br), hl = live && stage_b_node<R2O>(C, bl);
+                            const bool any_r = __any_sync(0xffffffffu, hr), any_l = __any_sync(0xffffffffu, hl);
+                            if (bsp + 2 > kStack) {
+                                if (lane == 0) atomicOr(A.err, kErrStack);
+                                break;
+                            }
+                            if (any_r) st[bsp++] = rr;
+                            if (any_l) st[bsp++] = rl;
+                        }
+                        if (hits && !spilled) atomicAdd(A.counts + pose, hits);
+                    }
+                } else if (prim != kNone && stage_b_setup<R2O>(R, S, W, make_uint2(item, prim), C, n_skip, n_rej, false)) {
                     ++n_acc;
                     int bsp = 0;
                     st[bsp++] = C.lroot;
@@ -978,15 +1067,11 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                     bool spilled = false;
                     while (bsp > 0) {
                         if (++steps > budget) {
-                            const uint32_t slot = atomicAdd(W.cand_count, 1u);
-                            if (slot < W.cand_cap) {
-                                W.cand[slot] = make_uint2(item, prim);
-                                const uint32_t h = atomicAdd(W.heavy_count, 1u);
-                                if (h < W.heavy_cap) {
-                                    W.heavy[h] = slot;
-                                    spilled = true;
-                                    break;
-                                }
+                            const uint32_t h = atomicAdd(W.heavy_count, 1u);
+                            if (h < W.heavy_cap) {
+                                W.heavy[h] = make_uint2(item, prim);
+                                spilled = true;
+                                break;
                             }
                             steps = 0;  // no room: finish the candidate here
                         }
@@ -1073,6 +1158,10 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
             n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
             __syncwarp();
         }
+        if (overflow && lane == 0) {
+            W.item_overflow[item] = 1;
+            W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
+        }
         __syncwarp();
     }
     warp_count(A.stats + 1, n_acc);
@@ -1109,10 +1198,10 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_stage_b_heavy(const RobotD
         if (lane == 0) h = atomicAdd(W.heavy_work, 1u);
         h = __shfl_sync(0xffffffffu, h, 0);
         if (h >= n_heavy) break;
-        const uint32_t ci = W.heavy[h];
-        if (ci == kNone) continue;  // a blanked slot of a reservation that did not fit
+        const uint2 cd = W.heavy[h];
+        if (cd.x == kNone) continue;  // a blanked slot of a reservation that did not fit
         StageBCand C;
-        if (!stage_b_setup<R2O>(R, S, W, W.cand[ci], C, n_skip, n_rej, false)) continue;  // warp-uniform
+        if (!stage_b_setup<R2O>(R, S, W, cd, C, n_skip, n_rej, false)) continue;  // warp-uniform
         if (!A.want_counts) {  // decided meanwhile? (one lane reads, all follow)
             uint32_t dec = 0;
             if (lane == 0) dec = ld_flag(A.pose_hit + C.pose);
@@ -1279,16 +1368,25 @@ void launch_stage_b_heavy(bool r2o, const RobotDev& R, const SceneDev& S, const 
     cuda_check(cudaGetLastError(), "k_stage_b_heavy");
 }
 
-uint32_t stage_ab_blocks(bool r2o) {
-    return r2o ? grid_for(k_stage_ab<true>, kAbWarps * 32) : grid_for(k_stage_ab<false>, kAbWarps * 32);
+uint32_t stage_ab_blocks(bool r2o, bool packets) {
+    if (packets)
+        return r2o ? grid_for(k_stage_ab<true, true>, kAbWarps * 32) : grid_for(k_stage_ab<false, true>, kAbWarps * 32);
+    return r2o ? grid_for(k_stage_ab<true, false>, kAbWarps * 32) : grid_for(k_stage_ab<false, false>, kAbWarps * 32);
 }
 
-void launch_stage_ab(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
+void launch_stage_ab(bool r2o, bool packets, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                      cudaStream_t s) {
-    if (r2o)
-        k_stage_ab<true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
-    else
-        k_stage_ab<false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+    if (packets) {
+        if (r2o)
+            k_stage_ab<true, true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+        else
+            k_stage_ab<false, true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+    } else {
+        if (r2o)
+            k_stage_ab<true, false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+        else
+            k_stage_ab<false, false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+    }
     cuda_check(cudaGetLastError(), "k_stage_ab");
 }
 

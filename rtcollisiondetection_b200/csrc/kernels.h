@@ -70,8 +70,9 @@ struct WaveArgs {
     uint32_t* overflow_items;  // compacted overflowed items (item words, for the fused kernel)
     uint32_t* overflow_count;  // zeroed before stage A
     uint32_t chunk;            // stage B: consecutive candidates (lanes) or 32-candidate groups (packets) per worker
+    uint32_t item_steps;       // fused forms: stage-B steps an item runs in its warp before deferring the rest
     uint32_t light_steps;      // stage B visits before a candidate moves to the heavy pass; 0 = no heavy pass
-    uint32_t* heavy;           // [heavy_cap] candidate indices handed to the heavy pass
+    uint2* heavy;              // [heavy_cap] candidates (item word, primitive) handed to the heavy pass
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // appended (may exceed heavy_cap: those stayed in the light pass); zeroed
     uint32_t* heavy_work;      // heavy-pass work counter; zeroed
@@ -90,11 +91,11 @@ void launch_stage_b(bool robot_to_obs, const RobotDev& R, const SceneDev& S, con
 // The heavy pass alone (after a light pass that spilled into W.heavy).
 void launch_stage_b_heavy(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W,
                           uint32_t heavy_share, cudaStream_t s);
-// Stages A and B fused in one warp per item (stage_b_form 3); its spilled
-// candidates go to W.cand / W.heavy for the heavy pass.
-void launch_stage_ab(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
-                     cudaStream_t s);
-uint32_t stage_ab_blocks(bool robot_to_obs);
+// Stages A and B fused in one warp per item (stage_b_form 3; 4 with packet
+// descents of the link tree); spilled candidates go to W.cand / W.heavy.
+void launch_stage_ab(bool robot_to_obs, bool packets, const RobotDev& R, const SceneDev& S, const WaveArgs& W,
+                     uint32_t blocks, cudaStream_t s);
+uint32_t stage_ab_blocks(bool robot_to_obs, bool packets);
 uint32_t stage_a_blocks(bool robot_to_obs);
 uint32_t stage_b_blocks(bool robot_to_obs);
 uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256

@@ -185,6 +185,21 @@ def served_large_scene(seed=0):
     return Mesh(v, t, off)
 
 
+def reference_scene(name):
+    """The reference's benchmark shelves ('simple', 'medium', 'dense': 15,008 /
+    71,746 / 202,330 triangles), one obstacle per placed model, from
+    ``data/ref_scenes.npz`` (see ``data/make_ref_scenes.py``)."""
+    d = np.load(os.path.join(DATA_DIR, 'ref_scenes.npz'))
+    verts, tris, off, nv = [], [], [0], 0
+    for m, t in zip(d['scene_%s_models' % name], d['scene_%s_offsets' % name]):
+        v = d['model_%s_verts' % m] + t.astype(np.float32)   # identity pose translated, in float
+        verts.append(v)
+        tris.append(d['model_%s_tris' % m] + np.uint32(nv))
+        nv += len(v)
+        off.append(off[-1] + len(d['model_%s_tris' % m]))
+    return Mesh(np.concatenate(verts), np.concatenate(tris), off)
+
+
 # --------------------------------------------------------------------------- queries
 def uniform_poses(robot, n, seed=0):
     rng = np.random.default_rng(seed)

@@ -77,7 +77,7 @@ def test_stage_b_forms_agree(setup, panda, name, okind, light):
     robot, scene, (orob, oscene) = setup
     q = scenes.uniform_poses(panda, 600, seed=21)
     dets = [rtcd.Detector(robot.ctx, name, robot, scene, light_steps=light, stage_b_form=f, stage_b_chunk=k)
-            for f, k in ((1, 1), (1, 64), (2, 1), (2, 4), (3, 0))]
+            for f, k in ((1, 1), (1, 64), (2, 1), (2, 4), (3, 0), (3, 1), (4, 0), (4, 1))]
     flags_only = [d.check(q) for d in dets]
     counted = [d.check(q, counts=True) for d in dets]
     for o in flags_only + counted:
