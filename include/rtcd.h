@@ -132,6 +132,41 @@ typedef struct {
 RTCD_API rtcd_status rtcd_context_create(int device, rtcd_ctx** out);
 RTCD_API rtcd_status rtcd_context_destroy(rtcd_ctx* ctx);
 
+/* Robot input at run time.  The reference generates a header of joint masks
+ * from a URDF offline (scripts/URDFParser/urdfParserUtils.py:527-605 ->
+ * RTCD/Robot/models/panda.h) and loads link meshes with tinyobjloader
+ * (RTCD/Meshes/mesh.h:311-360); these two calls do both inside the library.
+ *
+ * rtcd_urdf_chain_parse reads URDF text (len bytes) describing a serial chain
+ * from its root link: every revolute (or continuous) joint adds a link and its
+ * masks L(q) = cos q C + sin q S + O = origin * Rot(axis, q) (values within
+ * 1e-5 of 0 or +-1 set to them, as the reference does); fixed joints fold
+ * into the next joint's origin (links they attach are not separate links:
+ * merge their meshes beforehand, as the reference's parser does); the base
+ * transform is the identity.  Branching chains, prismatic joints and more
+ * than RTCD_URDF_MAX_LINKS links are rejected. */
+#define RTCD_URDF_MAX_LINKS 16
+#define RTCD_URDF_NAME 128
+typedef struct {
+    uint32_t dof;
+    uint32_t n_links;                                  /* dof + 1: the root, then each joint's child */
+    float base_tf[12];
+    float cos_mask[(RTCD_URDF_MAX_LINKS - 1) * 12];   /* dof * 12 used, as rtcd_robot_desc wants them */
+    float sin_mask[(RTCD_URDF_MAX_LINKS - 1) * 12];
+    float one_mask[(RTCD_URDF_MAX_LINKS - 1) * 12];
+    float lower[RTCD_URDF_MAX_LINKS - 1];
+    float upper[RTCD_URDF_MAX_LINKS - 1];
+    char link_name[RTCD_URDF_MAX_LINKS][RTCD_URDF_NAME];
+    char link_mesh[RTCD_URDF_MAX_LINKS][2 * RTCD_URDF_NAME]; /* the link's visual mesh file name, "" if none */
+} rtcd_urdf_chain;
+RTCD_API rtcd_status rtcd_urdf_chain_parse(const char* urdf, size_t len, rtcd_urdf_chain* out);
+
+/* Loads an OBJ mesh: vertices deduplicated by exact float position (first
+ * occurrence wins, faces in file order), polygons fan-triangulated, only
+ * vertices that faces use.  Call with NULL outputs to learn the sizes. */
+RTCD_API rtcd_status rtcd_obj_load(const char* path, float* verts_out, uint32_t max_verts, uint32_t* n_verts,
+                                   uint32_t* tris_out, uint32_t max_tris, uint32_t* n_tris);
+
 /* Replaces robot<DOF>(robotConfig) and the link GAS builds
  * (RTCD/Robot/robot.h:91-124, RTCD/Robot/batchIASRobot.h:310-365): uploads
  * the chain and builds one triangle and one edge LBVH per link. */

@@ -40,7 +40,7 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
            'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
-           'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights']
+           'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights', 'rtcd_urdf_chain_parse', 'rtcd_obj_load']
 
 
 class RTCDError(RuntimeError):
@@ -148,6 +148,63 @@ def quad_fit_weights(n_ctrl, n_wp):
     out = np.zeros((n_ctrl, n_wp), np.float32)
     _ok(lib().rtcd_quad_fit_weights(C.c_uint32(n_ctrl), C.c_uint32(n_wp), _ptr(out, C.c_float)))
     return out
+
+
+URDF_MAX_LINKS, URDF_NAME = 16, 128
+
+
+class UrdfChain(C.Structure):
+    _fields_ = [('dof', C.c_uint32), ('n_links', C.c_uint32), ('base_tf', C.c_float * 12),
+                ('cos_mask', C.c_float * ((URDF_MAX_LINKS - 1) * 12)),
+                ('sin_mask', C.c_float * ((URDF_MAX_LINKS - 1) * 12)),
+                ('one_mask', C.c_float * ((URDF_MAX_LINKS - 1) * 12)),
+                ('lower', C.c_float * (URDF_MAX_LINKS - 1)), ('upper', C.c_float * (URDF_MAX_LINKS - 1)),
+                ('link_name', (C.c_char * URDF_NAME) * URDF_MAX_LINKS),
+                ('link_mesh', (C.c_char * (2 * URDF_NAME)) * URDF_MAX_LINKS)]
+
+
+def urdf_chain(text):
+    """Parse URDF text (rtcd_urdf_chain_parse): masks, limits, link names and mesh files."""
+    raw = text.encode() if isinstance(text, str) else bytes(text)
+    c = UrdfChain()
+    _ok(lib().rtcd_urdf_chain_parse(C.c_char_p(raw), C.c_size_t(len(raw)), C.byref(c)))
+    d = c.dof
+    return {'dof': d, 'base_tf': np.array(c.base_tf, np.float32),
+            'cos_mask': np.array(c.cos_mask, np.float32)[:12 * d].reshape(d, 12),
+            'sin_mask': np.array(c.sin_mask, np.float32)[:12 * d].reshape(d, 12),
+            'one_mask': np.array(c.one_mask, np.float32)[:12 * d].reshape(d, 12),
+            'lower': np.array(c.lower, np.float32)[:d], 'upper': np.array(c.upper, np.float32)[:d],
+            'link_names': [c.link_name[i].value.decode() for i in range(c.n_links)],
+            'link_meshes': [c.link_mesh[i].value.decode() for i in range(c.n_links)]}
+
+
+def obj_load(path):
+    """Load an OBJ (rtcd_obj_load): deduplicated float32 vertices [n, 3], uint32 triangles [m, 3]."""
+    nv, nt = C.c_uint32(), C.c_uint32()
+    p = os.fsencode(path)
+    _ok(lib().rtcd_obj_load(C.c_char_p(p), None, 0, C.byref(nv), None, 0, C.byref(nt)))
+    v = np.zeros((max(nv.value, 1), 3), np.float32)
+    t = np.zeros((max(nt.value, 1), 3), np.uint32)
+    _ok(lib().rtcd_obj_load(C.c_char_p(p), _ptr(v, C.c_float), nv, C.byref(nv), _ptr(t, C.c_uint32), nt, C.byref(nt)))
+    return v[:nv.value], t[:nt.value]
+
+
+def model_from_urdf(text, mesh_root):
+    """A robot model dict (as Robot takes) from URDF text and the directory its
+    mesh file names are relative to; links without a visual mesh get none."""
+    ch = urdf_chain(text)
+    V, T, voff, toff = [], [], [0], [0]
+    for m in ch['link_meshes']:
+        if m:
+            v, t = obj_load(os.path.join(mesh_root, m))
+        else:
+            v, t = np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32)
+        V.append(v); T.append(t)
+        voff.append(voff[-1] + len(v)); toff.append(toff[-1] + len(t))
+    model = {k: ch[k] for k in ('cos_mask', 'sin_mask', 'one_mask', 'base_tf', 'lower', 'upper')}
+    model.update(link_verts=np.concatenate(V), link_vert_off=np.asarray(voff, np.uint32),
+                 link_tris=np.concatenate(T), link_tri_off=np.asarray(toff, np.uint32), link_names=ch['link_names'])
+    return model
 
 
 def robot_fk(robot, q_dev, n, T_dev, stream=None):

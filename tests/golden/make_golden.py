@@ -13,6 +13,10 @@ Writes
 * ``panda_mesh_stats.json`` - per-link vertex/triangle/unique-edge counts of
   the merged visual meshes, counted here with a direct text scan of the OBJ
   files (independent of the package loader).
+* ``panda_chain.json`` - the kinematic chain of the Panda URDF
+  (``models/franka_description/modified_panda.urdf``): per joint its parent,
+  child, type, origin (rpy, xyz), axis and limits, per link its visual mesh
+  file name; the tests rebuild a URDF from it for the C++ URDF reader.
 """
 import json
 import os
@@ -56,6 +60,28 @@ def mesh_stats(root):
     return stats
 
 
+def panda_chain(urdf):
+    import xml.etree.ElementTree as ET
+    r = ET.parse(urdf).getroot()
+    links = []
+    for l in r.findall('link'):
+        m = l.find('visual/geometry/mesh')
+        links.append({'name': l.get('name'), 'mesh': m.get('filename') if m is not None else ''})
+    joints = []
+    for j in r.findall('joint'):
+        o = j.find('origin')
+        lim = j.find('limit')
+        ax = j.find('axis')
+        joints.append({'name': j.get('name'), 'type': j.get('type'), 'parent': j.find('parent').get('link'),
+                       'child': j.find('child').get('link'),
+                       'rpy': o.get('rpy', '0 0 0') if o is not None else '0 0 0',
+                       'xyz': o.get('xyz', '0 0 0') if o is not None else '0 0 0',
+                       'axis': ax.get('xyz') if ax is not None else '1 0 0',
+                       'lower': lim.get('lower') if lim is not None else None,
+                       'upper': lim.get('upper') if lim is not None else None})
+    return {'links': links, 'joints': joints}
+
+
 def main(root):
     hdr = header_arrays(os.path.join(root, 'RTCD/Robot/models/panda.h'))
     json.dump(hdr, open(os.path.join(HERE, 'panda_header.json'), 'w'), indent=1)
@@ -66,6 +92,8 @@ def main(root):
         w['w_' + key] = np.loadtxt(f, dtype=np.float32).reshape(nc, nt)
     np.savez_compressed(os.path.join(HERE, 'quad_weights.npz'), **w)
     json.dump(mesh_stats(root), open(os.path.join(HERE, 'panda_mesh_stats.json'), 'w'), indent=1)
+    json.dump(panda_chain(os.path.join(root, 'models/franka_description/modified_panda.urdf')),
+              open(os.path.join(HERE, 'panda_chain.json'), 'w'), indent=1)
 
 
 if __name__ == '__main__':
