@@ -324,6 +324,37 @@ RTCD_API rtcd_status rtcd_server_wait(rtcd_server* server, uint64_t ticket, int3
 RTCD_API rtcd_status rtcd_server_get_stats(rtcd_server* server, rtcd_server_stats* out);
 RTCD_API rtcd_status rtcd_server_reset_stats(rtcd_server* server);
 
+/* ---- planner side: roadmap samples, neighbour edges, batched edge checks ----
+ *
+ * The reference's planner tooling samples the configuration space with a
+ * Halton sequence (RTCD/Planner/sampler/sampler.h:11-82), links samples to
+ * their K weighted nearest neighbours on the GPU (RTCD/Planner/KNN/knn.h,
+ * knnCUDA.cu) and checks each edge as a straight line of evenly spaced
+ * configurations (RTCD/Utils/Test/poseUtils.h:115-141). */
+
+/* Host only: n samples of dimension dim, sample i, coordinate d =
+ * halton(i, prime[d + skip]) * (upper[d] - lower[d]) + lower[d], with the
+ * reference's float arithmetic; out is n x dim row-major. */
+RTCD_API rtcd_status rtcd_halton_samples(uint32_t n, uint32_t dim, uint32_t skip, const float* lower,
+                                         const float* upper, float* out);
+/* For every point (device, n x dim, dim <= 16) its k (<= 32) nearest others
+ * by the weighted distance sqrt(sum_d (w_d (a_d - b_d))^2) (weights on the
+ * host, NULL = 1); points with mask_dev[i] != 0 (optional) take no part.
+ * idx_dev / dist_dev: n x k, nearest first, ties to the lower index; rows
+ * with fewer than k candidates end with index 0xFFFFFFFF, distance FLT_MAX. */
+RTCD_API rtcd_status rtcd_knn(rtcd_ctx* ctx, const float* points_dev, uint32_t n, uint32_t dim, const float* weights,
+                              uint32_t k, const uint8_t* mask_dev, uint32_t* idx_dev, float* dist_dev, void* stream);
+/* Checks n_edges straight-line edges between configurations: nodes_dev
+ * (device, n_nodes x dof), edges_dev (device, n_edges x 2 node indices).
+ * Each edge becomes n_wp evenly spaced configurations a + (b - a)/(n_wp-1) i,
+ * built on the device; sweep detectors check them as one trajectory each,
+ * discrete detectors check every configuration.  flags_dev[e] != 0 when the
+ * edge collides.  flags may carry RTCD_CHECK_NO_ENDPOINTS (sweeps),
+ * RTCD_CHECK_TWO_WAY and RTCD_CHECK_CONTAINMENT (discrete). */
+RTCD_API rtcd_status rtcd_check_edges(rtcd_detector* det, const float* nodes_dev, uint32_t n_nodes,
+                                      const uint32_t* edges_dev, uint32_t n_edges, uint32_t n_wp, uint8_t* flags_dev,
+                                      uint32_t flags, void* stream);
+
 /* ---- building blocks, exposed for callers that compose their own pipelines ---- */
 
 /* Batched forward kinematics (upstream batchFkineAdj, RTCD/Robot/robot.cu:202-241;

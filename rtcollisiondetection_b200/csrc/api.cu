@@ -241,6 +241,8 @@ struct rtcd_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     DevBuf err;
+    DevBuf knn_w2;  // squared neighbour-search weights
+    std::mutex mu;  // guards knn_w2
 };
 
 struct rtcd_robot {
@@ -286,6 +288,8 @@ struct rtcd_detector {
     ScanScratch scan;
     // sweep workspace
     DevBuf centers, ctrl, aux, piece_hit, W, W_off, heavy;
+    DevBuf edge_q, edge_pose_flags;  // edge checks: interpolated configurations, per-configuration flags
+    std::vector<uint32_t> edge_off;
     std::vector<float> W_host;
     std::vector<uint32_t> W_off_host;
     uint32_t W_max = 0;
@@ -1426,6 +1430,69 @@ rtcd_status rtcd_quad_fit_weights(uint32_t n_ctrl, uint32_t n_wp, float* W_out) 
         RTCD_REQUIRE(n_ctrl >= 3 && n_wp >= n_ctrl, "need 3 <= n_ctrl <= n_wp");
         const std::vector<double> W = fit_weights(n_ctrl, n_wp);
         for (size_t i = 0; i < W.size(); ++i) W_out[i] = (float) W[i];
+    });
+}
+
+rtcd_status rtcd_knn(rtcd_ctx* ctx, const float* points_dev, uint32_t n, uint32_t dim, const float* weights,
+                     uint32_t k, const uint8_t* mask_dev, uint32_t* idx_dev, float* dist_dev, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && (n == 0 || (points_dev && idx_dev && dist_dev)), "NULL argument");
+        RTCD_REQUIRE(dim >= 1 && dim <= kKnnMaxDim, "dim must be 1..16");
+        RTCD_REQUIRE(k >= 1 && k <= kKnnMaxK, "k must be 1..32");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : ctx->stream;
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        float w2[kKnnMaxDim];
+        for (uint32_t d = 0; d < dim; ++d) w2[d] = weights ? weights[d] * weights[d] : 1.0f;
+        ctx->knn_w2.ensure(sizeof(w2));
+        cuda_check(cudaStreamSynchronize(s), "knn weights");  // the previous call's kernel may still read them
+        cuda_check(cudaMemcpy(ctx->knn_w2.p, w2, dim * sizeof(float), cudaMemcpyHostToDevice), "knn weights");
+        launch_knn(points_dev, n, dim, ctx->knn_w2.as<float>(), k, mask_dev, idx_dev, dist_dev, s);
+    });
+}
+
+rtcd_status rtcd_check_edges(rtcd_detector* d, const float* nodes_dev, uint32_t n_nodes, const uint32_t* edges_dev,
+                             uint32_t n_edges, uint32_t n_wp, uint8_t* flags_dev, uint32_t flags, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(d && (n_edges == 0 || (nodes_dev && edges_dev && flags_dev)), "NULL argument");
+        RTCD_REQUIRE(n_wp >= 2, "an edge needs at least 2 configurations");
+        RTCD_REQUIRE(!(flags & ~(uint32_t) (RTCD_CHECK_NO_ENDPOINTS | RTCD_CHECK_TWO_WAY | RTCD_CHECK_CONTAINMENT)),
+                     "edge checks accept RTCD_CHECK_NO_ENDPOINTS, RTCD_CHECK_TWO_WAY and RTCD_CHECK_CONTAINMENT");
+        const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
+        RTCD_REQUIRE(discrete || !(flags & (RTCD_CHECK_TWO_WAY | RTCD_CHECK_CONTAINMENT)),
+                     "two-way and containment are for the discrete detectors");
+        RTCD_REQUIRE(d->kind != RTCD_QUAD_SWEEP || n_wp >= 3, "quadratic edges need at least 3 configurations");
+        RTCD_REQUIRE((uint64_t) n_edges * n_wp < (1ull << 32), "too many configurations in one call");
+        if (!n_edges) return;
+        // one critical section: the interpolated configurations live in the detector's workspace
+        std::lock_guard<std::mutex> lock(d->mu);
+        DeviceScope ds(d->ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : d->stream;
+        d->timed = false;
+        d->timed_total_only = false;
+        d->last_stream = s;
+        if (d->graph_exec) {  // this call may grow (move) workspaces the graph points into
+            cuda_check(cudaStreamSynchronize(s), "graph retire");
+            cudaGraphExecDestroy(d->graph_exec);
+            cudaGraphDestroy(d->graph);
+            d->graph_exec = nullptr;
+            d->graph = nullptr;
+        }
+        cuda_check(cudaMemsetAsync(d->stats.p, 0, 64, s), "stats reset");
+        const uint32_t dof = d->robot->dof;
+        const uint32_t total = n_edges * n_wp;
+        d->edge_q.ensure(4ull * total * dof);
+        launch_interp_edges(nodes_dev, n_nodes, dof, edges_dev, n_edges, n_wp, d->edge_q.as<float>(),
+                            d->err.as<uint32_t>(), s);
+        if (discrete) {
+            d->edge_pose_flags.ensure(total);
+            check_discrete(d, d->edge_q.as<float>(), total, d->edge_pose_flags.as<uint8_t>(), nullptr, flags, s);
+            launch_or_rows(d->edge_pose_flags.as<uint8_t>(), n_edges, n_wp, flags_dev, s);
+        } else {
+            d->edge_off.resize(n_edges + 1);
+            for (uint32_t e = 0; e <= n_edges; ++e) d->edge_off[e] = e * n_wp;
+            check_sweep(d, d->edge_q.as<float>(), d->edge_off.data(), n_edges, flags_dev, nullptr, nullptr, flags, s);
+        }
     });
 }
 

@@ -151,4 +151,13 @@ void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32
 uint32_t sweep_persistent_blocks(bool quad);
 uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads);  // threads: 64, 128 or 256
 
+// planner side (planner.cu)
+constexpr uint32_t kKnnMaxK = 32;
+constexpr uint32_t kKnnMaxDim = 16;
+void launch_knn(const float* pts, uint32_t n, uint32_t dim, const float* w2_dev, uint32_t k, const uint8_t* mask,
+                uint32_t* idx, float* dist, cudaStream_t s);
+void launch_interp_edges(const float* nodes, uint32_t n_nodes, uint32_t dof, const uint32_t* edges, uint32_t n_edges,
+                         uint32_t n_wp, float* q, uint32_t* err, cudaStream_t s);
+void launch_or_rows(const uint8_t* pose_flags, uint32_t n_edges, uint32_t n_wp, uint8_t* flags, cudaStream_t s);
+
 }  // namespace rtcd

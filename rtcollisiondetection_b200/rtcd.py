@@ -40,7 +40,8 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_robot_fk', 'rtcd_exclusive_scan_u32', 'rtcd_select_flags_u8', 'rtcd_lbvh_build',
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
            'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
-           'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights', 'rtcd_urdf_chain_parse', 'rtcd_obj_load']
+           'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights', 'rtcd_urdf_chain_parse', 'rtcd_obj_load',
+           'rtcd_halton_samples', 'rtcd_knn', 'rtcd_check_edges']
 
 
 class RTCDError(RuntimeError):
@@ -205,6 +206,23 @@ def model_from_urdf(text, mesh_root):
     model.update(link_verts=np.concatenate(V), link_vert_off=np.asarray(voff, np.uint32),
                  link_tris=np.concatenate(T), link_tri_off=np.asarray(toff, np.uint32), link_names=ch['link_names'])
     return model
+
+
+def halton_samples(n, lower, upper, skip=0):
+    """Halton roadmap samples (host): n x dim float32 in [lower, upper]."""
+    lo, hi = _arr(lower, np.float32), _arr(upper, np.float32)
+    out = np.zeros((max(n, 1), len(lo)), np.float32)
+    _ok(lib().rtcd_halton_samples(C.c_uint32(n), C.c_uint32(len(lo)), C.c_uint32(skip), _ptr(lo, C.c_float),
+                                  _ptr(hi, C.c_float), _ptr(out, C.c_float)))
+    return out[:n]
+
+
+def knn(ctx, points_dev, n, dim, k, idx_dev, dist_dev, weights=None, mask_dev=None, stream=None):
+    """Weighted k nearest neighbours of every point (device buffers, rtcd_knn)."""
+    w = _arr(weights, np.float32)
+    _ok(lib().rtcd_knn(ctx.h, _ptr(points_dev, C.c_float), C.c_uint32(n), C.c_uint32(dim), _ptr(w, C.c_float),
+                       C.c_uint32(k), _ptr(mask_dev, C.c_uint8), _ptr(idx_dev, C.c_uint32), _ptr(dist_dev, C.c_float),
+                       C.c_void_p(stream) if stream else None))
 
 
 def robot_fk(robot, q_dev, n, T_dev, stream=None):
@@ -382,6 +400,12 @@ class Detector:
 
     def sync(self, stream=None):
         _ok(lib().rtcd_sync(self.h, C.c_void_p(stream) if stream else None))
+
+    def check_edges(self, nodes_dev, n_nodes, edges_dev, n_edges, n_wp, flags_dev, flags=0, stream=None):
+        """Straight-line edges between configurations, interpolated on the device (rtcd_check_edges)."""
+        _ok(lib().rtcd_check_edges(self.h, _ptr(nodes_dev, C.c_float), C.c_uint32(n_nodes), _ptr(edges_dev, C.c_uint32),
+                                   C.c_uint32(n_edges), C.c_uint32(n_wp), _ptr(flags_dev, C.c_uint8), C.c_uint32(flags),
+                                   C.c_void_p(stream) if stream else None))
 
     def autotune(self, q_dev, n, traj_off=None, stream=None):
         """Pick the fastest traversal launch shape on this device-resident batch."""

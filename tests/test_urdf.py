@@ -135,3 +135,27 @@ def test_obj_loader_matches_upstream_dedupe(tmp_path):
     assert len(v) == 6  # vertex 6 repeats vertex 2's position
     with pytest.raises(rtcd.RTCDError):
         rtcd.obj_load(str(tmp_path / 'missing.obj'))
+
+
+def test_halton_samples_restate_reference_arithmetic():
+    """Host only: the reference's float radical inverse, scaled into the bounds."""
+    lo = np.array([-1.0, 0.0, 2.0], np.float32)
+    hi = np.array([1.0, 0.5, 3.0], np.float32)
+    got = rtcd.halton_samples(200, lo, hi, skip=2)
+    primes = [5, 7, 11]
+
+    def radical(n, b):
+        hn, n0, f = np.float32(0), n, np.float32(1) / np.float32(b)
+        while n0 > 0:
+            n1 = np.float32(n0 // b)
+            r = n0 - int(n1 * np.float32(b))
+            hn = np.float32(hn + f * np.float32(r))
+            f = np.float32(f / np.float32(b))
+            n0 = int(n1)
+        return hn
+    ref = np.array([[np.float32(radical(i, primes[d]) * (hi[d] - lo[d]) + lo[d]) for d in range(3)]
+                    for i in range(200)], np.float32)
+    assert np.array_equal(got, ref)
+    assert got[0].tolist() == lo.tolist()
+    with pytest.raises(rtcd.RTCDError):
+        rtcd.halton_samples(4, np.zeros(20), np.ones(20), skip=10)
