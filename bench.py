@@ -534,7 +534,7 @@ def main():
     if sweep:
         span = 'k_sweep + k_sweep_heavy'
     elif form in (0, 3, 4):
-        span = 'k_stage_ab + k_stage_b (deferred) + k_stage_b_heavy + k_discrete (overflow)'
+        span = 'k_stage_ab + k_subtree x 2 + k_stage_b (deferred) + k_stage_b_heavy + k_discrete (overflow)'
     else:
         span = 'k_stage_a + k_stage_b%s + k_stage_b_heavy + k_discrete (overflow)' % ('_packet' if form == 2 else '')
     traffic = None
@@ -574,10 +574,10 @@ def main():
                    'launch_shape': tuned},
         'e2e': {'value': units_all / (e2e_step / 1e3), 'unit': unit, 'ms_per_step': e2e_step,
                 'h2d_bytes_per_step': int(h2d), 'd2h_bytes_per_step': int(d2h)},
-        # discrete: k_fk_poses, k_cull, k_select_u8, then per direction k_stage_ab + k_stage_b (deferred
-        # candidates) or k_stage_a + k_stage_b, k_stage_b_heavy, k_discrete (overflow); (k_contain), k_flags;
-        # sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
-        'gpu_launches': args.steps * ((3 + (2 if args.two_way else 1) * 4
+        # discrete: k_fk_poses, k_cull, k_select_u8, then per direction k_stage_ab + k_subtree x 2 + k_stage_b
+        # (deferred candidates) or k_stage_a + k_stage_b, k_stage_b_heavy, k_discrete (overflow); (k_contain),
+        # k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
+        'gpu_launches': args.steps * ((3 + (2 if args.two_way else 1) * (6 if form in (0, 3, 4) else 4)
                                        + (1 if args.containment else 0) + 1) if not sweep
                                       else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in spans])),

@@ -259,6 +259,7 @@ struct rtcd_scene {
     SceneDev dev{};
     GroupedBvh tri, edge;
     DevBuf verts, tris, edges, obbs, tri_obs, obs_box, obs_point;
+    DevBuf tri_wide, edge_wide;  // 4-wide copies of the two scene trees (the fused kernel's descent)
     uint32_t n_tris = 0, n_edges = 0, n_obs = 0;
 };
 
@@ -282,7 +283,7 @@ struct rtcd_detector {
     uint32_t blocks = 0;
     // discrete workspace
     DevBuf q, T, mask, items, count, pose_hit, counts, edge_bits, flags, seg_flags, work, err, stats, contain;
-    DevBuf cand, item_overflow, overflow_items, wave_counts;  // wavefront traversal
+    DevBuf cand, item_overflow, overflow_items, wave_counts, sub;  // wavefront traversal
     uint32_t blocks_a = 0, blocks_b = 0, blocks_a_full = 0;
     uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
     ScanScratch scan;
@@ -607,7 +608,16 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
                       sc->tri_obs.as<uint32_t>());
         build_grouped(false, sc->verts.as<float>(), v0, sc->edges.as<uint32_t>(), eoff, ctx->err.as<uint32_t>(), s,
                       sc->edge);
+        const auto node_count = [](uint32_t n) { return n > 1 ? n - 1 : 0u; };
+        const WideResult wt = build_wide(sc->tri.nodes.as<float4>(), node_count(n_tris), sc->tri.roots[0], sc->tri_wide, s);
+        const WideResult we =
+            build_wide(sc->edge.nodes.as<float4>(), node_count(sc->n_edges), sc->edge.roots[0], sc->edge_wide, s);
         SceneDev& dv = sc->dev;
+        dv.tri_wide = sc->tri_wide.as<float4>();
+        dv.tri_wide_root = wt.root;
+        dv.edge_wide = sc->edge_wide.as<float4>();
+        dv.edge_wide_root = we.root;
+        dv.wide_front = wide_frontier(std::max(wt.depth, we.depth));
         dv.tri_nodes = sc->tri.nodes.as<float4>();
         dv.tri_prims = sc->tri.prims.as<float4>();
         dv.tri_root = sc->tri.roots[0];
@@ -851,12 +861,13 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
     const size_t items_max = (size_t) n * L;
     const uint32_t cap = (uint32_t) std::min<size_t>(std::max<size_t>(items_max * 128, 1u << 16), 1u << 26);
     d->cand.ensure(8ull * cap);
-    d->item_overflow.ensure(items_max);
+    d->item_overflow.ensure(items_max + 4);  // marked a word at a time
     d->overflow_items.ensure(4ull * items_max);
-    d->wave_counts.ensure(4 * 4);
-    cuda_check(cudaMemsetAsync(d->item_overflow.p, 0, items_max, s), "memset");
-    cuda_check(cudaMemsetAsync(d->wave_counts.p, 0, 16, s), "memset");
-    uint32_t* wc = d->wave_counts.as<uint32_t>();  // [0] candidates, [1] overflowed items, [2] fallback work, [3] heavy
+    d->wave_counts.ensure(8 * 4);
+    cuda_check(cudaMemsetAsync(d->item_overflow.p, 0, items_max + 4, s), "memset");
+    cuda_check(cudaMemsetAsync(d->wave_counts.p, 0, 32, s), "memset");
+    // [0] candidates, [1] overflowed items, [2] fallback work, [3] heavy, [4..7] subtree pass
+    uint32_t* wc = d->wave_counts.as<uint32_t>();
     WaveArgs W{};
     W.d = A;
     W.cand = d->cand.as<uint2>();
@@ -880,14 +891,23 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
         W.heavy_count = wc + 3;
         W.heavy_work = d->work.as<uint32_t>() + 1;
     }
+    if (fused_form) {
+        const uint32_t scap = (uint32_t) std::min<size_t>(std::max<size_t>(items_max * 8, 1u << 16), 1u << 24);
+        d->sub.ensure(2 * 8ull * scap);
+        W.sub = d->sub.as<uint2>();
+        W.sub_cap = scap;
+        W.sub_count = wc + 4;
+    }
     uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
     const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
     if (fused_form) {
         const bool packets = d->cfg.stage_b_form == 4;
-        const uint32_t full = stage_ab_blocks(r2o, packets);
+        const uint32_t full = stage_ab_blocks(r2o, packets, d->scene->dev);
         launch_stage_ab(r2o, packets, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100),
                         s);
-        // the one-lane pass over the candidates crowded items deferred, then the heavy pass
+        // the rest of the crowded items' descents, the one-lane pass over the candidates they
+        // deferred, then the heavy pass
+        launch_subtree(r2o, R, d->scene->dev, W, share, s);
         launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, false, s);
     } else {
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);

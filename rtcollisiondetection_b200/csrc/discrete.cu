@@ -907,8 +907,12 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
 }
 
 // Stages A and B in one warp per (pose, link) item.  The warp descends the
-// scene LBVH with the link's OBB through a shared frontier as stage A does,
-// but keeps the leaf survivors in a shared buffer and, 32 at a time, runs
+// scene's 4-wide tree with the link's OBB through a shared LIFO frontier
+// (each step pops up to 32 nodes and spreads their children over the lanes:
+// 4 lanes per node when at most 8 are waiting, 2 when at most 16, else one
+// lane tests all four children of its node, so a step costs about one box
+// test per lane and the descent half the dependent node loads of a binary
+// tree), keeps the leaf survivors in a shared buffer and, 32 at a time, runs
 // them through stage B at once (one lane per candidate, bounded by the light
 // budget; longer candidates are written to the candidate buffer and handed
 // to the heavy pass).  An item whose pose is found in collision stops
@@ -919,23 +923,110 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b_packet(const RobotDev R, cons
 // warp, each lane testing its own primitive - which shares the top levels of
 // the link tree when many small scene primitives crowd one link.
 constexpr int kAbWarps = 4;
-constexpr int kCandBuf = 96;  // < 32 waiting + up to 64 added by one frontier step
+constexpr int kCandBuf = 32 + 32 * kWide;  // < 32 waiting + up to 32 * kWide added by one frontier step
+
+// The link OBB of an item in the world frame, padded by the box tolerance,
+// and its world-axis half extents.
+__device__ __forceinline__ void item_box(const RobotDev& R, const DiscreteArgs& A, uint32_t pose, uint32_t link,
+                                         ObbW& ob, f3& ext) {
+    constexpr float kBoxTol = 2e-5f;
+    float4 T[3];
+    const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
+    T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
+    ob = world_obb(R.obb[link], T);
+    ob.h = mk(ob.h.x + kBoxTol, ob.h.y + kBoxTol, ob.h.z + kBoxTol);
+    ext = mk(fabsf(ob.ax[0].x) * ob.h.x + fabsf(ob.ax[1].x) * ob.h.y + fabsf(ob.ax[2].x) * ob.h.z,
+             fabsf(ob.ax[0].y) * ob.h.x + fabsf(ob.ax[1].y) * ob.h.y + fabsf(ob.ax[2].y) * ob.h.z,
+             fabsf(ob.ax[0].z) * ob.h.x + fabsf(ob.ax[1].z) * ob.h.y + fabsf(ob.ax[2].z) * ob.h.z);
+}
+
+// Marks an item for the thread-per-item fallback once, however many warps
+// give up on it (one byte per item in a word-aligned buffer with 3 spare bytes).
+__device__ __forceinline__ void mark_overflow(const WaveArgs& W, uint32_t item) {
+    unsigned* word = reinterpret_cast<unsigned*>(W.item_overflow + (item & ~3u));
+    const unsigned bit = 1u << (8 * (item & 3u));
+    if (!(atomicOr(word, bit) & bit)) W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
+}
+
+// One step of a warp's descent of a scene wide tree through its shared LIFO
+// frontier fr[0, sp): pops up to 32 nodes and spreads their children over
+// the lanes (4 lanes per node when at most 8 are waiting, 2 when at most 16,
+// else one lane tests all four children of its node, so a step costs about
+// one box test per lane); internal children that overlap the OBB are pushed,
+// leaf children appended to cb[nc, ...) (at most 32 * kWide per step).
+// Returns false, with the error flag set, if the frontier would overflow
+// (which the frontier's size, derived from the tree depth, rules out).
+__device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_t* fr, int& sp, uint32_t* cb, int& nc,
+                                          const ObbW& ob, const f3& ext, uint32_t front_cap, uint32_t* err,
+                                          unsigned long long& n_node, unsigned long long& n_cand) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const int lg = sp <= 8 ? 2 : (sp <= 16 ? 1 : 0), g = 1 << lg;
+    const int take = min(sp, 32 >> lg);
+    sp -= take;
+    const int j = lane >> lg;
+    const uint32_t node = j < take ? fr[sp + j] : kNone;
+    __syncwarp();
+    // this lane's kWide / g child records, all loads issued before the first test (the
+    // records of one node share a 128-byte line, but each is its own sector)
+    const int c0 = lane & (g - 1), rounds = kWide >> lg;
+    float4 ra[kWide], rb[kWide];
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) {
+        ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+        rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
+        if (r < rounds && node != kNone) {
+            const float4* rec = wn + 2ull * (kWide * (size_t) node + c0 + r * g);
+            ra[r] = __ldg(rec);
+            rb[r] = __ldg(rec + 1);
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int r = 0; r < kWide; ++r) {
+        if (r >= rounds) break;  // warp-uniform
+        const uint32_t ref = __float_as_uint(rb[r].z);
+        bool h = false;
+        if (ref != kNone) {
+            ++n_node;
+            Box bx;
+            bx.lo[0] = ra[r].x; bx.lo[1] = ra[r].y; bx.lo[2] = ra[r].z;
+            bx.hi[0] = ra[r].w; bx.hi[1] = rb[r].x; bx.hi[2] = rb[r].y;
+            h = obb_aabb(bx, ob, ext);
+        }
+        const bool push = h && !(ref & kLeaf), emit = h && (ref & kLeaf);
+        const uint32_t mp = __ballot_sync(0xffffffffu, push), me = __ballot_sync(0xffffffffu, emit);
+        const int npush = __popc(mp);
+        if (sp + npush > (int) front_cap) {
+            if (lane == 0) atomicOr(err, kErrStack);
+            ok = false;
+            break;
+        }
+        if (push) fr[sp + __popc(mp & lt)] = ref;
+        if (emit) cb[nc + __popc(me & lt)] = ref & ~kLeaf;
+        sp += npush;
+        const int nemit = __popc(me);
+        nc += nemit;
+        n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
+    }
+    __syncwarp();
+    return ok;
+}
 
 // Capped at 5 resident blocks per SM worth of registers (a few spills, more
 // warps to hide the node-load latency; measured on the 65,536-pose workload).
 template <bool R2O, bool PACKET>
 __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
-    constexpr float kBoxTol = 2e-5f;
-    __shared__ uint32_t s_front[kAbWarps][kFrontier];
+    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front]
     __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
     const DiscreteArgs& A = W.d;
     const int lane = threadIdx.x & 31;
-    uint32_t* fr = s_front[threadIdx.x >> 5];
+    uint32_t* fr = s_front + (threadIdx.x >> 5) * S.wide_front;
     uint32_t* cb = s_cand[threadIdx.x >> 5];
     const uint32_t lt = (1u << lane) - 1u;
-    const float4* __restrict__ wn = R2O ? S.tri_nodes : S.edge_nodes;
+    const float4* __restrict__ wn = R2O ? S.tri_wide : S.edge_wide;
     const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
-    const uint32_t wroot = R2O ? S.tri_root : S.edge_root;
+    const uint32_t wroot = R2O ? S.tri_wide_root : S.edge_wide_root;
     const float4* __restrict__ ln = R2O ? R.edge_nodes : R.tri_nodes;
     const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
     const uint32_t n_items = *A.n_items;
@@ -956,18 +1047,17 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
         uint32_t dec = 0;
         if (lane == 0 && !A.want_counts) dec = ld_flag(A.pose_hit + pose);
         if (wroot == kNone || __shfl_sync(0xffffffffu, dec, 0)) continue;
-        float4 T[3];
-        const float4* tp = A.T + ((size_t) pose * R.n_links + link) * 3;
-        T[0] = tp[0]; T[1] = tp[1]; T[2] = tp[2];
-        ObbW ob = world_obb(R.obb[link], T);
-        ob.h = mk(ob.h.x + kBoxTol, ob.h.y + kBoxTol, ob.h.z + kBoxTol);
-        const f3 ext = mk(fabsf(ob.ax[0].x) * ob.h.x + fabsf(ob.ax[1].x) * ob.h.y + fabsf(ob.ax[2].x) * ob.h.z,
-                          fabsf(ob.ax[0].y) * ob.h.x + fabsf(ob.ax[1].y) * ob.h.y + fabsf(ob.ax[2].y) * ob.h.z,
-                          fabsf(ob.ax[0].z) * ob.h.x + fabsf(ob.ax[1].z) * ob.h.y + fabsf(ob.ax[2].z) * ob.h.z);
-        int sp = 1, nc = 0;
+        ObbW ob;
+        f3 ext;
+        item_box(R, A, pose, link, ob, ext);
+        // a one-primitive scene: its root is the only candidate
+        int sp = (wroot & kLeaf) ? 0 : 1, nc = (wroot & kLeaf) ? 1 : 0;
         uint32_t nbs = 0;  // stage-B steps this item ran in its warp
         bool overflow = false;
-        if (lane == 0) fr[0] = wroot;
+        if (lane == 0) {
+            if (sp) fr[0] = wroot;
+            else cb[0] = wroot & ~kLeaf;
+        }
         __syncwarp();
         while (true) {
             if (nc >= 32 || (sp == 0 && nc > 0)) {  // stage B on up to 32 buffered candidates
@@ -978,11 +1068,31 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 if (!A.want_counts && nbs >= W.item_steps) {
                     // a crowded item: its further candidates go to the one-lane pass, which
                     // spreads them over the whole GPU instead of this warp's serial steps
-                    uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(W.cand_count, (uint32_t) take);
+                    uint32_t base = 0, d2 = 0;
+                    if (lane == 0) {
+                        d2 = ld_flag(A.pose_hit + pose);  // decided by another item: stop enumerating
+                        if (!d2) base = atomicAdd(W.cand_count, (uint32_t) take);
+                    }
+                    if (__shfl_sync(0xffffffffu, d2, 0)) break;
                     base = __shfl_sync(0xffffffffu, base, 0);
                     if (base + (uint32_t) take <= W.cand_cap) {
                         if (prim != kNone) W.cand[base + lane] = make_uint2(item, prim);
+                        if (sp > 0) {
+                            // and the rest of its descent to the subtree pass, one warp per frontier
+                            // node, so no single warp walks a crowded item's whole overlap
+                            uint32_t sb = 0;
+                            if (lane == 0) sb = atomicAdd(W.sub_count, (uint32_t) sp);
+                            sb = __shfl_sync(0xffffffffu, sb, 0);
+                            const bool fits = sb + (uint32_t) sp <= W.sub_cap;
+                            for (int i = lane; i < sp; i += 32)  // slots below the capacity are always written
+                                if (sb + i < W.sub_cap) W.sub[sb + i] = fits ? make_uint2(item, fr[i]) : make_uint2(kNone, kNone);
+                            __syncwarp();
+                            if (!fits) {
+                                overflow = true;
+                                break;
+                            }
+                            sp = 0;
+                        }
                         continue;
                     }
                     // no room: blank the reserved slots below the capacity and hand the whole
@@ -1121,53 +1231,103 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 continue;
             }
             if (sp == 0) break;
-            const int take = min(sp, 32);
-            sp -= take;
-            const uint32_t ref = lane < take ? fr[sp + lane] : kNone;
-            __syncwarp();
-            bool hl = false, hr = false;
-            uint32_t rl = kNone, rr = kNone;
-            if (ref != kNone) {
-                if (ref & kLeaf) {  // a one-primitive scene: the root itself is a leaf
-                    hl = true;
-                    rl = ref;
-                } else {
-                    Box bl, br;
-                    load_node(wn, ref, bl, br, rl, rr);
-                    n_node += 2;
-                    hl = obb_aabb(bl, ob, ext);
-                    hr = obb_aabb(br, ob, ext);
-                }
-            }
-            const bool pl = hl && !(rl & kLeaf), pr = hr && !(rr & kLeaf);
-            const bool el = hl && (rl & kLeaf), er = hr && (rr & kLeaf);
-            const uint32_t mpl = __ballot_sync(0xffffffffu, pl), mpr = __ballot_sync(0xffffffffu, pr);
-            const uint32_t mel = __ballot_sync(0xffffffffu, el), mer = __ballot_sync(0xffffffffu, er);
-            const int npush = __popc(mpl) + __popc(mpr);
-            if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
-                if (lane == 0) atomicOr(A.err, kErrStack);
-                break;
-            }
-            if (pl) fr[sp + __popc(mpl & lt)] = rl;
-            if (pr) fr[sp + __popc(mpl) + __popc(mpr & lt)] = rr;
-            sp += npush;
-            if (el) cb[nc + __popc(mel & lt)] = rl & ~kLeaf;
-            if (er) cb[nc + __popc(mel) + __popc(mer & lt)] = rr & ~kLeaf;
-            const int nemit = __popc(mel) + __popc(mer);
-            nc += nemit;
-            n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
-            __syncwarp();
+            if (!wide_step(wn, fr, sp, cb, nc, ob, ext, S.wide_front, A.err, n_node, n_cand)) break;
         }
-        if (overflow && lane == 0) {
-            W.item_overflow[item] = 1;
-            W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
-        }
+        if (overflow && lane == 0) mark_overflow(W, item);
         __syncwarp();
     }
     warp_count(A.stats + 1, n_acc);
     warp_count(A.stats + 2, n_skip);
     warp_count(A.stats + 3, n_rej);
     warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 7, n_node);
+    warp_count(A.stats + 6, n_cand);
+}
+
+// The subtree pass: the rest of a crowded item's scene descent, one warp
+// per frontier node the fused kernel handed over.  Every leaf that overlaps
+// the item's OBB is appended to the candidate buffer for the one-lane pass
+// (32 or more at a time); a subtree stops when its pose is decided.  When the
+// buffer is full the item goes to the thread-per-item fallback (flags only,
+// like every deferral).  It runs twice.  The first launch (SPLIT) takes the
+// fused kernel's nodes and descends breadth-first - while at most 32 nodes
+// wait, every step pops them all, so the frontier holds one level - and as
+// soon as a level is wider than 32 nodes hands those nodes to the second
+// launch, which descends each to the end: a large subtree becomes many
+// pieces of equal depth on as many warps instead of one warp's serial walk.
+template <bool R2O, bool SPLIT>
+__global__ void __launch_bounds__(kAbWarps * 32) k_subtree(const RobotDev R, const SceneDev S, const WaveArgs W) {
+    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front]
+    __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
+    const DiscreteArgs& A = W.d;
+    const int lane = threadIdx.x & 31;
+    uint32_t* fr = s_front + (threadIdx.x >> 5) * S.wide_front;
+    uint32_t* cb = s_cand[threadIdx.x >> 5];
+    const float4* __restrict__ wn = R2O ? S.tri_wide : S.edge_wide;
+    const uint2* src = SPLIT ? W.sub : W.sub + W.sub_cap;  // the second half holds the split pieces
+    const uint32_t n_sub = min(SPLIT ? W.sub_count[0] : W.sub_count[2], W.sub_cap);
+    uint32_t* work = SPLIT ? W.sub_count + 1 : W.sub_count + 3;
+    unsigned long long n_node = 0, n_cand = 0;
+    while (true) {
+        uint32_t h = 0;
+        if (lane == 0) h = atomicAdd(work, 1u);
+        h = __shfl_sync(0xffffffffu, h, 0);
+        if (h >= n_sub) break;
+        const uint2 pr = src[h];
+        if (pr.x == kNone) continue;  // a blanked slot of a reservation that did not fit
+        const uint32_t item = pr.x, pose = item / R.n_links, link = item - pose * R.n_links;
+        if (pose >= A.n_poses) {
+            if (lane == 0) atomicOr(A.err, kErrRange);
+            continue;
+        }
+        uint32_t skip = 0;
+        if (lane == 0) skip = W.item_overflow[item] | ld_flag(A.pose_hit + pose);
+        if (__shfl_sync(0xffffffffu, skip, 0)) continue;  // re-run whole by the fallback, or decided
+        ObbW ob;
+        f3 ext;
+        item_box(R, A, pose, link, ob, ext);
+        int sp = 1, nc = 0;
+        if (lane == 0) fr[0] = pr.y;
+        __syncwarp();
+        while (true) {
+            if (nc >= 32 || (sp == 0 && nc > 0)) {  // flush every buffered candidate
+                uint32_t base = 0, dec = 0;
+                if (lane == 0) {
+                    dec = ld_flag(A.pose_hit + pose);
+                    if (!dec) base = atomicAdd(W.cand_count, (uint32_t) nc);
+                }
+                if (__shfl_sync(0xffffffffu, dec, 0)) break;
+                base = __shfl_sync(0xffffffffu, base, 0);
+                const bool fits = base + (uint32_t) nc <= W.cand_cap;
+                for (int i = lane; i < nc; i += 32)  // slots below the capacity are always written
+                    if (base + i < W.cand_cap) W.cand[base + i] = fits ? make_uint2(item, cb[i]) : make_uint2(kNone, kNone);
+                __syncwarp();
+                nc = 0;
+                if (!fits) {
+                    if (lane == 0) mark_overflow(W, item);
+                    break;
+                }
+                continue;
+            }
+            if (sp == 0) break;
+            if (SPLIT && sp > 32) {  // one level wider than a step: hand its nodes to the second launch
+                uint32_t sb = 0;
+                if (lane == 0) sb = atomicAdd(W.sub_count + 2, (uint32_t) sp);
+                sb = __shfl_sync(0xffffffffu, sb, 0);
+                const bool fits = sb + (uint32_t) sp <= W.sub_cap;
+                uint2* dst = W.sub + W.sub_cap;
+                for (int i = lane; i < sp; i += 32)  // slots below the capacity are always written
+                    if (sb + i < W.sub_cap) dst[sb + i] = fits ? make_uint2(item, fr[i]) : make_uint2(kNone, kNone);
+                __syncwarp();
+                if (!fits && lane == 0) mark_overflow(W, item);
+                sp = 0;
+                if (!fits) break;
+                continue;  // flush what is buffered, then the item is done here
+            }
+            if (!wide_step(wn, fr, sp, cb, nc, ob, ext, S.wide_front, A.err, n_node, n_cand)) break;
+        }
+        __syncwarp();
+    }
     warp_count(A.stats + 7, n_node);
     warp_count(A.stats + 6, n_cand);
 }
@@ -1368,24 +1528,58 @@ void launch_stage_b_heavy(bool r2o, const RobotDev& R, const SceneDev& S, const 
     cuda_check(cudaGetLastError(), "k_stage_b_heavy");
 }
 
-uint32_t stage_ab_blocks(bool r2o, bool packets) {
-    if (packets)
-        return r2o ? grid_for(k_stage_ab<true, true>, kAbWarps * 32) : grid_for(k_stage_ab<false, true>, kAbWarps * 32);
-    return r2o ? grid_for(k_stage_ab<true, false>, kAbWarps * 32) : grid_for(k_stage_ab<false, false>, kAbWarps * 32);
+// The fused kernel's frontier lives in dynamic shared memory, sized from the
+// scene's wide-tree depth.
+static size_t stage_ab_smem(const SceneDev& S) { return sizeof(uint32_t) * kAbWarps * (size_t) S.wide_front; }
+
+template <class K>
+static uint32_t stage_ab_grid(K kernel, size_t smem) {
+    // beyond the default 48 KB a block needs the opt-in (trees deeper than ~44 wide levels;
+    // the deepest accepted tree needs about 96 KB)
+    if (smem + sizeof(uint32_t) * kAbWarps * kCandBuf > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem),
+                   "k_stage_ab shared memory");
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kAbWarps * 32, smem);
+    return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
+}
+
+uint32_t stage_ab_blocks(bool r2o, bool packets, const SceneDev& S) {
+    const size_t smem = stage_ab_smem(S);
+    if (packets) return r2o ? stage_ab_grid(k_stage_ab<true, true>, smem) : stage_ab_grid(k_stage_ab<false, true>, smem);
+    return r2o ? stage_ab_grid(k_stage_ab<true, false>, smem) : stage_ab_grid(k_stage_ab<false, false>, smem);
+}
+
+void launch_subtree(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t share, cudaStream_t s) {
+    const size_t smem = stage_ab_smem(S);
+    const uint32_t full = r2o ? stage_ab_grid(k_subtree<true, true>, smem) : stage_ab_grid(k_subtree<false, true>, smem);
+    const uint32_t blocks = std::max(1u, full * share / 100);
+    if (r2o) {
+        stage_ab_grid(k_subtree<true, false>, smem);
+        k_subtree<true, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
+        k_subtree<true, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
+    } else {
+        stage_ab_grid(k_subtree<false, false>, smem);
+        k_subtree<false, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
+        k_subtree<false, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
+    }
+    cuda_check(cudaGetLastError(), "k_subtree");
 }
 
 void launch_stage_ab(bool r2o, bool packets, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                      cudaStream_t s) {
+    stage_ab_blocks(r2o, packets, S);  // sets the shared-memory limit before the first launch
+    const size_t smem = stage_ab_smem(S);
     if (packets) {
         if (r2o)
-            k_stage_ab<true, true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+            k_stage_ab<true, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
         else
-            k_stage_ab<false, true><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+            k_stage_ab<false, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
     } else {
         if (r2o)
-            k_stage_ab<true, false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+            k_stage_ab<true, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
         else
-            k_stage_ab<false, false><<<blocks, kAbWarps * 32, 0, s>>>(R, S, W);
+            k_stage_ab<false, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
     }
     cuda_check(cudaGetLastError(), "k_stage_ab");
 }

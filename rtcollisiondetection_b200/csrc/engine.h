@@ -89,6 +89,17 @@ LbvhResult build_lbvh(const float4* d_lo, const float4* d_hi, uint32_t n, float4
                       uint32_t node_offset, uint32_t prim_offset, uint32_t* d_err, cudaStream_t s,
                       std::vector<uint32_t>* codes_out = nullptr, std::vector<uint32_t>* child_out = nullptr);
 
+// A 4-wide tree collapsed from a binary one (lbvh.cu).  Node i is 8 float4 =
+// 4 child records of 32 bytes: (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z,
+// bits(ref), 0); ref = wide node index, kLeaf | sorted primitive (the binary
+// tree's leaf reference), or kNone in an empty slot (whose box is inverted).
+struct WideResult {
+    uint32_t root = kNone;  // 0, or the binary root when it is empty or a single leaf
+    uint32_t depth = 0;     // depth of the deepest wide node (root = 0)
+    uint32_t nodes = 0;
+};
+WideResult build_wide(const float4* d_nodes, uint32_t n_nodes, uint32_t root, DevBuf& out, cudaStream_t s);
+
 // Primitive boxes and gathers (lbvh.cu).
 void tri_boxes(const float* d_verts, const uint32_t* d_tris, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s);
 void edge_boxes(const float* d_verts, const uint32_t* d_edges, uint32_t n, float4* d_lo, float4* d_hi, cudaStream_t s);

@@ -37,6 +37,11 @@ struct SceneDev {
     const float4* obs_box;    // [obstacle][2]: exact box of its vertices (lo, hi)
     const float4* obs_point;  // [obstacle]: one of its vertices
     uint32_t n_obs;           // scene triangles carry their obstacle in the third float4's w
+    const float4* tri_wide;   // 4-wide copies of the two trees (8 float4 per node), same leaf references
+    uint32_t tri_wide_root;   // 0, or the binary root when that is kNone or a leaf
+    const float4* edge_wide;
+    uint32_t edge_wide_root;
+    uint32_t wide_front;      // frontier entries a warp needs over either wide tree
 };
 
 struct DiscreteArgs {
@@ -76,6 +81,10 @@ struct WaveArgs {
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // appended (may exceed heavy_cap: those stayed in the light pass); zeroed
     uint32_t* heavy_work;      // heavy-pass work counter; zeroed
+    uint2* sub;                // [2][sub_cap] (item word, wide node): crowded items' frontiers, then the split pieces
+    uint32_t sub_cap;
+    uint32_t* sub_count;       // [4] zeroed: frontier nodes appended, their work counter, pieces appended, their work
+                               // counter (appends may exceed sub_cap: those items went to the fallback)
 };
 
 constexpr int kStageAWarps = 4;
@@ -95,7 +104,12 @@ void launch_stage_b_heavy(bool robot_to_obs, const RobotDev& R, const SceneDev& 
 // descents of the link tree); spilled candidates go to W.cand / W.heavy.
 void launch_stage_ab(bool robot_to_obs, bool packets, const RobotDev& R, const SceneDev& S, const WaveArgs& W,
                      uint32_t blocks, cudaStream_t s);
-uint32_t stage_ab_blocks(bool robot_to_obs, bool packets);
+uint32_t stage_ab_blocks(bool robot_to_obs, bool packets, const SceneDev& S);
+// The subtree pass over the frontiers crowded items handed over (after the
+// fused kernel, before the one-lane pass over the candidates), on share
+// percent of its full persistent grid.
+void launch_subtree(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t share,
+                    cudaStream_t s);
 uint32_t stage_a_blocks(bool robot_to_obs);
 uint32_t stage_b_blocks(bool robot_to_obs);
 uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256
