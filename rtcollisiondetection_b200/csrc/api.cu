@@ -259,7 +259,7 @@ struct rtcd_scene {
     SceneDev dev{};
     GroupedBvh tri, edge;
     DevBuf verts, tris, edges, obbs, tri_obs, obs_box, obs_point;
-    DevBuf tri_wide, edge_wide;  // 4-wide copies of the two scene trees (the fused kernel's descent)
+    DevBuf tri_wide, edge_wide, tri_cut, edge_cut;  // 4-wide copies of the two scene trees and their top cuts
     uint32_t n_tris = 0, n_edges = 0, n_obs = 0;
 };
 
@@ -618,6 +618,12 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
         dv.edge_wide = sc->edge_wide.as<float4>();
         dv.edge_wide_root = we.root;
         dv.wide_front = wide_frontier(std::max(wt.depth, we.depth));
+        upload(sc->tri_cut, wt.cut.data(), wt.cut.size(), s);
+        upload(sc->edge_cut, we.cut.data(), we.cut.size(), s);
+        dv.tri_cut = sc->tri_cut.as<float4>();
+        dv.edge_cut = sc->edge_cut.as<float4>();
+        dv.n_tri_cut = (uint32_t) wt.cut.size() / 2;
+        dv.n_edge_cut = (uint32_t) we.cut.size() / 2;
         dv.tri_nodes = sc->tri.nodes.as<float4>();
         dv.tri_prims = sc->tri.prims.as<float4>();
         dv.tri_root = sc->tri.roots[0];

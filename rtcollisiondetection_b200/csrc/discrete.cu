@@ -948,19 +948,51 @@ __device__ __forceinline__ void mark_overflow(const WaveArgs& W, uint32_t item) 
     if (!(atomicOr(word, bit) & bit)) W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
 }
 
+// One round of a wide descent: every lane tests one child record (a, b) -
+// (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, bits(ref), 0); ref kNone in an empty
+// slot or a lane without a record - against the OBB; overlapping internal
+// children are pushed on the frontier fr[0, sp), leaves appended to cb[nc,
+// ...).  Returns false, with the error flag set, if the frontier would
+// overflow (which its size, derived from the tree depth, rules out).
+__device__ __forceinline__ bool wide_round(const float4& a, const float4& b, uint32_t* fr, int& sp, uint32_t* cb,
+                                           int& nc, const ObbW& ob, const f3& ext, uint32_t front_cap, uint32_t* err,
+                                           unsigned long long& n_node, unsigned long long& n_cand) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t ref = __float_as_uint(b.z);
+    bool h = false;
+    if (ref != kNone) {
+        ++n_node;
+        Box bx;
+        bx.lo[0] = a.x; bx.lo[1] = a.y; bx.lo[2] = a.z;
+        bx.hi[0] = a.w; bx.hi[1] = b.x; bx.hi[2] = b.y;
+        h = obb_aabb(bx, ob, ext);
+    }
+    const bool push = h && !(ref & kLeaf), emit = h && (ref & kLeaf);
+    const uint32_t mp = __ballot_sync(0xffffffffu, push), me = __ballot_sync(0xffffffffu, emit);
+    const int npush = __popc(mp);
+    if (sp + npush > (int) front_cap) {
+        if (lane == 0) atomicOr(err, kErrStack);
+        return false;
+    }
+    if (push) fr[sp + __popc(mp & lt)] = ref;
+    if (emit) cb[nc + __popc(me & lt)] = ref & ~kLeaf;
+    sp += npush;
+    const int nemit = __popc(me);
+    nc += nemit;
+    n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
+    return true;
+}
+
 // One step of a warp's descent of a scene wide tree through its shared LIFO
 // frontier fr[0, sp): pops up to 32 nodes and spreads their children over
 // the lanes (4 lanes per node when at most 8 are waiting, 2 when at most 16,
 // else one lane tests all four children of its node, so a step costs about
-// one box test per lane); internal children that overlap the OBB are pushed,
-// leaf children appended to cb[nc, ...) (at most 32 * kWide per step).
-// Returns false, with the error flag set, if the frontier would overflow
-// (which the frontier's size, derived from the tree depth, rules out).
+// one box test per lane); at most 32 * kWide leaves are appended per step.
 __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_t* fr, int& sp, uint32_t* cb, int& nc,
                                           const ObbW& ob, const f3& ext, uint32_t front_cap, uint32_t* err,
                                           unsigned long long& n_node, unsigned long long& n_cand) {
     const int lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1u;
     const int lg = sp <= 8 ? 2 : (sp <= 16 ? 1 : 0), g = 1 << lg;
     const int take = min(sp, 32 >> lg);
     sp -= take;
@@ -985,29 +1017,40 @@ __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_
 #pragma unroll
     for (int r = 0; r < kWide; ++r) {
         if (r >= rounds) break;  // warp-uniform
-        const uint32_t ref = __float_as_uint(rb[r].z);
-        bool h = false;
-        if (ref != kNone) {
-            ++n_node;
-            Box bx;
-            bx.lo[0] = ra[r].x; bx.lo[1] = ra[r].y; bx.lo[2] = ra[r].z;
-            bx.hi[0] = ra[r].w; bx.hi[1] = rb[r].x; bx.hi[2] = rb[r].y;
-            h = obb_aabb(bx, ob, ext);
-        }
-        const bool push = h && !(ref & kLeaf), emit = h && (ref & kLeaf);
-        const uint32_t mp = __ballot_sync(0xffffffffu, push), me = __ballot_sync(0xffffffffu, emit);
-        const int npush = __popc(mp);
-        if (sp + npush > (int) front_cap) {
-            if (lane == 0) atomicOr(err, kErrStack);
+        if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, ob, ext, front_cap, err, n_node, n_cand)) {
             ok = false;
             break;
         }
-        if (push) fr[sp + __popc(mp & lt)] = ref;
-        if (emit) cb[nc + __popc(me & lt)] = ref & ~kLeaf;
-        sp += npush;
-        const int nemit = __popc(me);
-        nc += nemit;
-        n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
+    }
+    __syncwarp();
+    return ok;
+}
+
+// The first step of a descent: the tree's top cut (at most kWideCut child
+// records that cover every root-leaf path), one record per lane.
+__device__ __forceinline__ bool cut_step(const float4* __restrict__ cut, uint32_t n_cut, uint32_t* fr, int& sp,
+                                         uint32_t* cb, int& nc, const ObbW& ob, const f3& ext, uint32_t front_cap,
+                                         uint32_t* err, unsigned long long& n_node, unsigned long long& n_cand) {
+    const int lane = threadIdx.x & 31;
+    float4 ra[kWideCut / 32], rb[kWideCut / 32];
+#pragma unroll
+    for (int r = 0; r < kWideCut / 32; ++r) {
+        const uint32_t i = 32u * r + lane;
+        ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+        rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
+        if (i < n_cut) {
+            ra[r] = __ldg(cut + 2ull * i);
+            rb[r] = __ldg(cut + 2ull * i + 1);
+        }
+    }
+    bool ok = true;
+#pragma unroll
+    for (int r = 0; r < kWideCut / 32; ++r) {
+        if (32u * r >= n_cut) break;  // warp-uniform
+        if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, ob, ext, front_cap, err, n_node, n_cand)) {
+            ok = false;
+            break;
+        }
     }
     __syncwarp();
     return ok;
@@ -1050,15 +1093,18 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
         ObbW ob;
         f3 ext;
         item_box(R, A, pose, link, ob, ext);
-        // a one-primitive scene: its root is the only candidate
-        int sp = (wroot & kLeaf) ? 0 : 1, nc = (wroot & kLeaf) ? 1 : 0;
+        // the descent starts with the tree's top cut; a one-primitive scene's root is its only candidate
+        int sp = 0, nc = 0;
         uint32_t nbs = 0;  // stage-B steps this item ran in its warp
         bool overflow = false;
-        if (lane == 0) {
-            if (sp) fr[0] = wroot;
-            else cb[0] = wroot & ~kLeaf;
+        if (wroot & kLeaf) {
+            if (lane == 0) cb[0] = wroot & ~kLeaf;
+            nc = 1;
+            __syncwarp();
+        } else if (!cut_step(R2O ? S.tri_cut : S.edge_cut, R2O ? S.n_tri_cut : S.n_edge_cut, fr, sp, cb, nc, ob, ext,
+                             S.wide_front, A.err, n_node, n_cand)) {
+            continue;
         }
-        __syncwarp();
         while (true) {
             if (nc >= 32 || (sp == 0 && nc > 0)) {  // stage B on up to 32 buffered candidates
                 const int take = min(nc, 32);

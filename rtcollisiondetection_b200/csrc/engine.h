@@ -97,6 +97,10 @@ struct WideResult {
     uint32_t root = kNone;  // 0, or the binary root when it is empty or a single leaf
     uint32_t depth = 0;     // depth of the deepest wide node (root = 0)
     uint32_t nodes = 0;
+    // The top cut: at most kWideCut child records (2 float4 each) that cover
+    // every root-leaf path - the root's records, opened level by level while
+    // they fit; a descent starts by testing these instead of the root.
+    std::vector<float4> cut;
 };
 WideResult build_wide(const float4* d_nodes, uint32_t n_nodes, uint32_t root, DevBuf& out, cudaStream_t s);
 

@@ -42,6 +42,9 @@ struct SceneDev {
     const float4* edge_wide;
     uint32_t edge_wide_root;
     uint32_t wide_front;      // frontier entries a warp needs over either wide tree
+    const float4* tri_cut;    // top cuts of the wide trees: child records (2 float4 each)
+    const float4* edge_cut;
+    uint32_t n_tri_cut, n_edge_cut;
 };
 
 struct DiscreteArgs {

@@ -526,6 +526,31 @@ WideResult build_wide(const float4* d_nodes, uint32_t n_nodes, uint32_t root, De
     }
     r.nodes = (uint32_t) queue.size();
     r.root = 0;
+    // the top cut: the root's records, each internal one replaced by its node's records, level
+    // by level while the list stays within kWideCut records
+    std::vector<uint32_t> cut;  // record indices (node * kWide + slot)
+    for (int j = 0; j < kWide; ++j)
+        if (host_f2u(wide[2 * j + 1].z) != kNone) cut.push_back((uint32_t) j);
+    while (true) {
+        std::vector<uint32_t> next;
+        bool opened = false;
+        for (uint32_t rec : cut) {
+            const uint32_t ref = host_f2u(wide[2ull * rec + 1].z);
+            if (ref & kLeaf) {
+                next.push_back(rec);
+                continue;
+            }
+            opened = true;
+            for (int j = 0; j < kWide; ++j)
+                if (host_f2u(wide[2ull * (kWide * ref + j) + 1].z) != kNone) next.push_back(kWide * ref + j);
+        }
+        if (!opened || next.size() > (size_t) kWideCut) break;
+        cut.swap(next);
+    }
+    for (uint32_t rec : cut) {
+        r.cut.push_back(wide[2ull * rec]);
+        r.cut.push_back(wide[2ull * rec + 1]);
+    }
     out.ensure(wide.size() * sizeof(float4));
     cuda_check(cudaMemcpyAsync(out.p, wide.data(), wide.size() * sizeof(float4), cudaMemcpyHostToDevice, s),
                "wide nodes upload");

@@ -12,6 +12,7 @@ constexpr uint32_t kLeaf = 0x80000000u;    // child reference: leaf flag | sorte
 constexpr uint32_t kNone = 0xFFFFFFFFu;    // empty tree
 constexpr int kMaxTreeDepth = kStack - 2;  // builders reject deeper trees
 constexpr int kWide = 4;                    // children per node of the scene's wide trees
+constexpr int kWideCut = 64;                // child records in a wide tree's top cut
 
 // Entries a 32-wide LIFO frontier over a kWide-ary tree can hold when every
 // step pops min(size, 32) entries and pushes their internal children, for a
@@ -19,7 +20,9 @@ constexpr int kWide = 4;                    // children per node of the scene's 
 // are one segment of at most 32 * kWide entries; the step after it pops 32 of
 // them (or all), so every segment below the top keeps at most
 // 32 * (kWide - 1); and the smallest depth in each live segment exceeds the
-// one below it, so at most depth + 1 segments are live.
+// one below it, so at most depth + 1 segments are live.  A descent that
+// starts from a top cut of at most kWideCut <= 32 * kWide records obeys the
+// same bound.
 __host__ __device__ constexpr uint32_t wide_frontier(uint32_t depth) {
     return 32u * (kWide - 1) * depth + 32u * kWide;
 }
