@@ -118,7 +118,10 @@ typedef struct {
                                         that share each link-BVH node load, 3 = stages A and B fused in one
                                         warp per item (an item stops generating candidates once its pose
                                         is hit), 4 = 3 with packet descents of the link tree; 0 = 3 (the
-                                        autotuner tries all four) */
+                                        autotuner tries all four).  Sweeps: 1 = the light pass's lanes descend
+                                        the binary edge tree, any other value the 4-wide one (when the
+                                        scene's is shallow enough for a lane stack; the autotuner tries
+                                        both) */
     uint32_t stage_b_chunk;          /* discrete stage B: consecutive candidates one lane takes in order (lanes
                                         form) or 32-candidate groups one warp takes (packets), so a pose's
                                         candidates spread over few workers that stop at its first hit; for
@@ -226,8 +229,9 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
  * threads per block, each at a quarter, half and all of the blocks per SM
  * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
  * then, for the discrete kinds, the four stage B forms, the first two at
- * chunk lengths from 1 to 256 candidates (coordinate descent; sweeps are
- * timed with segment flags on)
+ * chunk lengths from 1 to 256 candidates, for the sweeps the binary and the
+ * 4-wide edge tree (coordinate descent; sweeps are timed with segment flags
+ * on)
  * - times the traversal with device events (median of three after a
  * warm-up run), keeps the fastest configuration in the detector and
  * writes it to best_out (optional).  The upstream picks its batch size per

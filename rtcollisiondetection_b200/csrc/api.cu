@@ -624,6 +624,8 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
         dv.edge_cut = sc->edge_cut.as<float4>();
         dv.n_tri_cut = (uint32_t) wt.cut.size() / 2;
         dv.n_edge_cut = (uint32_t) we.cut.size() / 2;
+        // a depth-first lane descent keeps at most 3 siblings per level plus the last node's 4 children
+        dv.edge_wide_lane = (kWide - 1) * we.depth + kWide <= (uint32_t) kStack ? 1u : 0u;
         dv.tri_nodes = sc->tri.nodes.as<float4>();
         dv.tri_prims = sc->tri.prims.as<float4>();
         dv.tri_root = sc->tri.roots[0];
@@ -1191,6 +1193,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         cuda_check(cudaEventRecord(d->ev[1], s), "event");
         cuda_check(cudaEventRecord(d->ev[2], s), "event");
     }
+    A.binary_tree = d->cfg.stage_b_form == 1 ? 1 : 0;
     if (A.total_units)
         launch_sweep(d->scene->dev, A, d->blocks, d->threads, d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
@@ -1413,7 +1416,7 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
             }
         };
         // coordinate descent: the launch shape, then the light-pass budget,
-        // then (discrete) the stage B form and its chunk length
+        // then the stage B form and its chunk length (discrete) or the tree (sweeps)
         for (uint32_t t : {64u, 128u, 256u}) {
             uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
                                     : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
@@ -1429,6 +1432,11 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         for (uint32_t light : {16u, 32u, 64u}) {
             rtcd_config c = best;
             c.light_steps = light;
+            time_cfg(c);
+        }
+        if (!discrete) {  // the binary or the wide edge tree
+            rtcd_config c = best;
+            c.stage_b_form = best.stage_b_form == 1 ? 0u : 1u;
             time_cfg(c);
         }
         if (discrete) {

@@ -28,6 +28,7 @@
 #include <algorithm>
 
 #include "kernels.h"
+#include "wide.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -948,113 +949,12 @@ __device__ __forceinline__ void mark_overflow(const WaveArgs& W, uint32_t item) 
     if (!(atomicOr(word, bit) & bit)) W.overflow_items[atomicAdd(W.overflow_count, 1u)] = item;
 }
 
-// One round of a wide descent: every lane tests one child record (a, b) -
-// (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, bits(ref), 0); ref kNone in an empty
-// slot or a lane without a record - against the OBB; overlapping internal
-// children are pushed on the frontier fr[0, sp), leaves appended to cb[nc,
-// ...).  Returns false, with the error flag set, if the frontier would
-// overflow (which its size, derived from the tree depth, rules out).
-__device__ __forceinline__ bool wide_round(const float4& a, const float4& b, uint32_t* fr, int& sp, uint32_t* cb,
-                                           int& nc, const ObbW& ob, const f3& ext, uint32_t front_cap, uint32_t* err,
-                                           unsigned long long& n_node, unsigned long long& n_cand) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t ref = __float_as_uint(b.z);
-    bool h = false;
-    if (ref != kNone) {
-        ++n_node;
-        Box bx;
-        bx.lo[0] = a.x; bx.lo[1] = a.y; bx.lo[2] = a.z;
-        bx.hi[0] = a.w; bx.hi[1] = b.x; bx.hi[2] = b.y;
-        h = obb_aabb(bx, ob, ext);
-    }
-    const bool push = h && !(ref & kLeaf), emit = h && (ref & kLeaf);
-    const uint32_t mp = __ballot_sync(0xffffffffu, push), me = __ballot_sync(0xffffffffu, emit);
-    const int npush = __popc(mp);
-    if (sp + npush > (int) front_cap) {
-        if (lane == 0) atomicOr(err, kErrStack);
-        return false;
-    }
-    if (push) fr[sp + __popc(mp & lt)] = ref;
-    if (emit) cb[nc + __popc(me & lt)] = ref & ~kLeaf;
-    sp += npush;
-    const int nemit = __popc(me);
-    nc += nemit;
-    n_cand += lane == 0 ? (unsigned long long) nemit : 0ull;
-    return true;
-}
-
-// One step of a warp's descent of a scene wide tree through its shared LIFO
-// frontier fr[0, sp): pops up to 32 nodes and spreads their children over
-// the lanes (4 lanes per node when at most 8 are waiting, 2 when at most 16,
-// else one lane tests all four children of its node, so a step costs about
-// one box test per lane); at most 32 * kWide leaves are appended per step.
-__device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_t* fr, int& sp, uint32_t* cb, int& nc,
-                                          const ObbW& ob, const f3& ext, uint32_t front_cap, uint32_t* err,
-                                          unsigned long long& n_node, unsigned long long& n_cand) {
-    const int lane = threadIdx.x & 31;
-    const int lg = sp <= 8 ? 2 : (sp <= 16 ? 1 : 0), g = 1 << lg;
-    const int take = min(sp, 32 >> lg);
-    sp -= take;
-    const int j = lane >> lg;
-    const uint32_t node = j < take ? fr[sp + j] : kNone;
-    __syncwarp();
-    // this lane's kWide / g child records, all loads issued before the first test (the
-    // records of one node share a 128-byte line, but each is its own sector)
-    const int c0 = lane & (g - 1), rounds = kWide >> lg;
-    float4 ra[kWide], rb[kWide];
-#pragma unroll
-    for (int r = 0; r < kWide; ++r) {
-        ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-        rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
-        if (r < rounds && node != kNone) {
-            const float4* rec = wn + 2ull * (kWide * (size_t) node + c0 + r * g);
-            ra[r] = __ldg(rec);
-            rb[r] = __ldg(rec + 1);
-        }
-    }
-    bool ok = true;
-#pragma unroll
-    for (int r = 0; r < kWide; ++r) {
-        if (r >= rounds) break;  // warp-uniform
-        if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, ob, ext, front_cap, err, n_node, n_cand)) {
-            ok = false;
-            break;
-        }
-    }
-    __syncwarp();
-    return ok;
-}
-
-// The first step of a descent: the tree's top cut (at most kWideCut child
-// records that cover every root-leaf path), one record per lane.
-__device__ __forceinline__ bool cut_step(const float4* __restrict__ cut, uint32_t n_cut, uint32_t* fr, int& sp,
-                                         uint32_t* cb, int& nc, const ObbW& ob, const f3& ext, uint32_t front_cap,
-                                         uint32_t* err, unsigned long long& n_node, unsigned long long& n_cand) {
-    const int lane = threadIdx.x & 31;
-    float4 ra[kWideCut / 32], rb[kWideCut / 32];
-#pragma unroll
-    for (int r = 0; r < kWideCut / 32; ++r) {
-        const uint32_t i = 32u * r + lane;
-        ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-        rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
-        if (i < n_cut) {
-            ra[r] = __ldg(cut + 2ull * i);
-            rb[r] = __ldg(cut + 2ull * i + 1);
-        }
-    }
-    bool ok = true;
-#pragma unroll
-    for (int r = 0; r < kWideCut / 32; ++r) {
-        if (32u * r >= n_cut) break;  // warp-uniform
-        if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, ob, ext, front_cap, err, n_node, n_cand)) {
-            ok = false;
-            break;
-        }
-    }
-    __syncwarp();
-    return ok;
-}
+// The OBB test of the wide descents (wide.cuh) of the fused and subtree kernels.
+struct ObbTest {
+    const ObbW& ob;
+    const f3& ext;
+    __device__ __forceinline__ bool operator()(const Box& b) const { return obb_aabb(b, ob, ext); }
+};
 
 // Capped at 5 resident blocks per SM worth of registers (a few spills, more
 // warps to hide the node-load latency; measured on the 65,536-pose workload).
@@ -1101,8 +1001,8 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
             if (lane == 0) cb[0] = wroot & ~kLeaf;
             nc = 1;
             __syncwarp();
-        } else if (!cut_step(R2O ? S.tri_cut : S.edge_cut, R2O ? S.n_tri_cut : S.n_edge_cut, fr, sp, cb, nc, ob, ext,
-                             S.wide_front, A.err, n_node, n_cand)) {
+        } else if (!cut_step(R2O ? S.tri_cut : S.edge_cut, R2O ? S.n_tri_cut : S.n_edge_cut, fr, sp, cb, nc,
+                             ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand)) {
             continue;
         }
         while (true) {
@@ -1277,7 +1177,7 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 continue;
             }
             if (sp == 0) break;
-            if (!wide_step(wn, fr, sp, cb, nc, ob, ext, S.wide_front, A.err, n_node, n_cand)) break;
+            if (!wide_step(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand)) break;
         }
         if (overflow && lane == 0) mark_overflow(W, item);
         __syncwarp();
@@ -1370,7 +1270,7 @@ __global__ void __launch_bounds__(kAbWarps * 32) k_subtree(const RobotDev R, con
                 if (!fits) break;
                 continue;  // flush what is buffered, then the item is done here
             }
-            if (!wide_step(wn, fr, sp, cb, nc, ob, ext, S.wide_front, A.err, n_node, n_cand)) break;
+            if (!wide_step(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand)) break;
         }
         __syncwarp();
     }

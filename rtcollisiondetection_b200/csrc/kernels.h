@@ -45,6 +45,7 @@ struct SceneDev {
     const float4* tri_cut;    // top cuts of the wide trees: child records (2 float4 each)
     const float4* edge_cut;
     uint32_t n_tri_cut, n_edge_cut;
+    uint32_t edge_wide_lane;  // nonzero when a lane stack of kStack entries holds a wide edge-tree descent
 };
 
 struct DiscreteArgs {
@@ -152,6 +153,7 @@ struct SweepArgs {
     int want_counts;
     int want_pieces;
     uint32_t light_steps;      // visits before a unit moves to the heavy pass; 0 = no heavy pass
+    int binary_tree;           // light pass on the binary edge tree (else the 4-wide one where the scene allows)
     uint32_t* heavy;           // [heavy_cap] units handed to the heavy pass
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // units appended (may exceed heavy_cap: those stayed in the light pass)

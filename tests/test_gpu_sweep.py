@@ -133,3 +133,20 @@ def test_sweep_graph_replay_matches_direct_path(sweep_setup, panda, kind):
                 ref = ref_det.check(q, off, segments=True)
                 assert np.array_equal(fd.cpu().numpy(), ref['flags']), (off_seed, seed)
                 assert np.array_equal(sd.cpu().numpy(), ref['seg_flags']), (off_seed, seed)
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_binary_and_wide_trees_agree(sweep_setup, panda, kind):
+    """The lane and warp descents over the binary edge tree (stage_b_form 1)
+    and over its 4-wide copy (the default) give the oracle's flags and counts,
+    with short light budgets so the heavy pass takes many units."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = 24 if kind == 'Linear' else scenes.log_uniform_counts(128, 8, 48, seed=3)
+    q, off = scenes.random_walk_trajectories(panda, 128, n_wp, seed=3)
+    ref = O.sweep(kind == 'Quadratic', orob, osc, q, off)
+    for form in (0, 1):
+        for light in (4, 0):
+            det = rtcd.Detector(robot.ctx, kind, robot, scene, stage_b_form=form, light_steps=light)
+            _cmp(det.check(q, off, segments=True), ref)
+            _cmp(det.check(q, off, counts=True, segments=True), ref)
+            det.close()
