@@ -99,7 +99,7 @@ class ClockSampler:
               'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
 
     def __init__(self, gpu):
-        self.gpu, self.rows, self.proc = gpu, [], None
+        self.gpu, self.rows, self.proc, self.pre = gpu, [], None, []
 
     def start(self):
         try:
@@ -111,6 +111,7 @@ class ClockSampler:
             t0 = time.time()
             while not self.rows and time.time() - t0 < 3.0:   # sampling is running before the timed region
                 time.sleep(0.01)
+            self.pre = self.rows[-1:]
             self.rows.clear()
         except OSError:
             self.proc = None
@@ -120,6 +121,15 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(',')])
 
     def stop(self):
+        bracketed = False
+        if self.proc and not self.rows:
+            # a timed region shorter than the sampling interval: bracket it with the sample just
+            # before it and the first one after it
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 1.0:
+                time.sleep(0.002)
+            self.rows[:0] = self.pre
+            bracketed = True
         if self.proc:
             self.proc.terminate()
             try:
@@ -133,8 +143,11 @@ class ClockSampler:
         names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
         reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and 'Active' in r[5 + k]
                           and 'Not' not in r[5 + k]})
-        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
-                'reasons': reasons, 'samples': len(self.rows)}
+        out = {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': max(mx) if mx else None,
+               'reasons': reasons, 'samples': len(self.rows)}
+        if bracketed:
+            out['note'] = 'timed region shorter than the 20 ms sampling interval: samples just before and after it'
+        return out
 
 
 def cpu_baseline(cfg, model, mesh, spheres, q, off, seconds=10.0):
