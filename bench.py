@@ -11,7 +11,8 @@ before every step to flush the 126 MB L2 and each step is timed with CUDA
 events on the launching stream (max over ranks for N > 1, weak scaling:
 every rank checks its own batch).  ``e2e`` repeats the step through the
 public C ABI with host buffers (pose upload and flag download inside the
-timed call).  ``plain`` is the same engine driven the upstream way: frames
+timed call; the step replayed as one CUDA graph that holds the copies
+between the pinned staging and the device, unless ``--no-graph``).  ``plain`` is the same engine driven the upstream way: frames
 of 64 poses with a host round trip per frame.  ``cpu_baseline`` times the
 FP64 oracle (flags only, every host thread) on a bounded sample.
 
@@ -497,13 +498,13 @@ def main():
     flags = fd.cpu().numpy()
     st = det.stats()
 
-    # end to end through the C ABI with host buffers (upload + download inside the call)
+    # end to end through the C ABI with host buffers (upload + download inside the call, in the graph)
     e2e_ms = []
     for k in range(max(3, args.steps // 2) + 2):
         flush.fill_(k & 255)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        out = det.check(q, off, segments=sweep, flags=mode_flags)
+        out = det.check(q, off, segments=sweep, flags=mode_flags | graph)
         dt = (time.perf_counter() - t0) * 1e3
         if k >= 2:
             e2e_ms.append(dt)

@@ -71,9 +71,13 @@ typedef enum {
 #define RTCD_CHECK_TWO_WAY (1u << 9)       /* discrete: run both directions (ObsToRobot and RobotToObs) in one check
                                               over the same FK, cull and items: flags are the union, counts the
                                               sum of the two upstream counts */
-#define RTCD_CHECK_GRAPH (1u << 7)         /* device buffers: replay the launch sequence as a CUDA graph (captured on
-                                              the first call with these pointers, sizes, flags and - for sweeps -
-                                              trajectory offsets; any other call on the detector retires it) */
+#define RTCD_CHECK_GRAPH (1u << 7)         /* replay the launch sequence as a CUDA graph (captured on the first call
+                                              with these pointers, sizes, flags and - for sweeps - trajectory
+                                              offsets; any other call on the detector retires it).  With
+                                              RTCD_CHECK_HOST_BUFFERS the graph holds the upload from the
+                                              detector's pinned staging, the kernels and the download back to it;
+                                              only the copies between the caller's arrays and the staging run
+                                              outside it, and the call returns with the results in place */
 
 typedef struct rtcd_ctx rtcd_ctx;
 typedef struct rtcd_robot rtcd_robot;

@@ -295,6 +295,7 @@ struct rtcd_detector {
     std::vector<uint32_t> W_off_host;
     uint32_t W_max = 0;
     HostBuf pin_in, pin_out, pin_aux;
+    DevBuf hq, hflags, hseg, hcounts;  // device sides of a graph replay with host buffers
     uint64_t last_items = 0, last_culled = 0;
 };
 
@@ -1243,11 +1244,11 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
         if (n == 0) return;
         if (flags & RTCD_CHECK_GRAPH) {
             const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
-            RTCD_REQUIRE(!(flags & (RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_PLAIN)),
-                         "graph replay needs device buffers and the batched path");
+            const bool host = (flags & RTCD_CHECK_HOST_BUFFERS) != 0;
+            RTCD_REQUIRE(!(flags & RTCD_CHECK_PLAIN), "graph replay needs the batched path");
             RTCD_REQUIRE(!discrete || !seg_flags_out, "segment flags exist only for sweep detectors");
             RTCD_REQUIRE(discrete || traj_offsets, "traj_offsets required for sweep detectors");
-            RTCD_REQUIRE(flags_out, "graph replay needs a device flags buffer");
+            RTCD_REQUIRE(flags_out, "graph replay needs a flags buffer");
             // events recorded inside a graph cannot be timed: a replay is timed as a whole
             const bool want_time = (flags & RTCD_CHECK_TIMING) != 0;
             const uint32_t f = flags & ~(RTCD_CHECK_GRAPH | RTCD_CHECK_TIMING);
@@ -1256,19 +1257,74 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             uint64_t h = 1469598103934665603ull;
             if (!discrete)
                 for (uint32_t i = 0; i <= n; ++i) h = (h ^ traj_offsets[i]) * 1099511628211ull;
-            const uint64_t key[8] = {(uint64_t) q, n, (uint64_t) flags_out, (uint64_t) counts_out, f, (uint64_t) s,
-                                     (uint64_t) seg_flags_out, h};
+            // host buffers: the graph runs between the pinned staging and device mirrors; the
+            // copies from and to the caller's arrays stay outside it
+            const float* gq = q;
+            uint8_t* gflags = flags_out;
+            uint8_t* gseg = seg_flags_out;
+            uint32_t* gcounts = counts_out;
+            size_t in_bytes = 0, n_seg = 0, seg_at = 0, counts_at = 0, err_at = 0;
+            if (host) {
+                in_bytes = 4ull * (discrete ? n : traj_offsets[n]) * d->robot->dof;
+                if (seg_flags_out)
+                    for (uint32_t i = 0; i < n; ++i) n_seg += pieces_of(d->kind, traj_offsets[i + 1] - traj_offsets[i], f);
+                d->pin_in.ensure(std::max<size_t>(in_bytes, 16));
+                d->hq.ensure(std::max<size_t>(in_bytes, 16));
+                std::memcpy(d->pin_in.p, q, in_bytes);
+                gq = d->hq.as<float>();
+                d->hflags.ensure(n);
+                gflags = d->hflags.as<uint8_t>();
+                if (seg_flags_out) {
+                    d->hseg.ensure(std::max<size_t>(n_seg, 1));
+                    gseg = d->hseg.as<uint8_t>();
+                }
+                if (counts_out) {
+                    d->hcounts.ensure(4ull * n);
+                    gcounts = d->hcounts.as<uint32_t>();
+                }
+                // pinned results: flags | segment flags | counts | the device error word
+                seg_at = (n + 15) & ~size_t(15);
+                counts_at = seg_at + ((n_seg + 15) & ~size_t(15));
+                err_at = counts_at + (counts_out ? 4ull * n : 0);
+                d->pin_out.ensure(err_at + 16);
+                for (uint64_t v : {(uint64_t) d->pin_in.p, (uint64_t) d->pin_out.p}) h = (h ^ v) * 1099511628211ull;
+            }
+            const uint64_t key[8] = {(uint64_t) gq, n, (uint64_t) gflags, (uint64_t) gcounts, f, (uint64_t) s,
+                                     (uint64_t) gseg, h};
+            uint8_t* po = d->pin_out.as<uint8_t>();
             auto run = [&] {
+                const uint32_t fd = f & ~RTCD_CHECK_HOST_BUFFERS;
+                if (host)
+                    cuda_check(cudaMemcpyAsync(d->hq.p, d->pin_in.p, in_bytes, cudaMemcpyHostToDevice, s), "q upload");
                 if (discrete)
-                    check_discrete(d, q, n, flags_out, counts_out, f, s);
+                    check_discrete(d, gq, n, gflags, gcounts, fd, s);
                 else
-                    check_sweep(d, q, traj_offsets, n, flags_out, seg_flags_out, counts_out, f, s);
+                    check_sweep(d, gq, traj_offsets, n, gflags, gseg, gcounts, fd, s);
+                if (host) {
+                    cuda_check(cudaMemcpyAsync(po, gflags, n, cudaMemcpyDeviceToHost, s), "flags download");
+                    if (gseg) cuda_check(cudaMemcpyAsync(po + seg_at, gseg, n_seg, cudaMemcpyDeviceToHost, s), "download");
+                    if (counts_out)
+                        cuda_check(cudaMemcpyAsync(po + counts_at, gcounts, 4ull * n, cudaMemcpyDeviceToHost, s), "download");
+                    cuda_check(cudaMemcpyAsync(po + err_at, d->err.p, 4, cudaMemcpyDeviceToHost, s), "error readback");
+                }
+            };
+            // host buffers: wait for the download, report a device error, hand the results over
+            auto finish = [&] {
+                if (!host) return;
+                cuda_check(cudaStreamSynchronize(s), "check sync");
+                uint32_t e = 0;
+                std::memcpy(&e, po + err_at, 4);
+                if (e) check_device_errors(d, s);  // resets the word and reports it
+                std::memcpy(flags_out, po, n);
+                if (seg_flags_out) std::memcpy(seg_flags_out, po + seg_at, n_seg);
+                if (counts_out) std::memcpy(counts_out, po + counts_at, 4ull * n);
             };
             if (d->graph_exec && std::equal(key, key + 8, d->graph_key)) {
                 if (want_time) cuda_check(cudaEventRecord(d->ev[0], s), "event");
                 cuda_check(cudaGraphLaunch(d->graph_exec, s), "cudaGraphLaunch");
                 if (want_time) cuda_check(cudaEventRecord(d->ev_end, s), "event");
                 d->timed_total_only = want_time;
+                finish();
                 return;
             }
             // run once normally (this also sizes every workspace), then capture the
@@ -1294,6 +1350,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             cuda_check(cudaStreamEndCapture(s, &d->graph), "cudaStreamEndCapture");
             cuda_check(cudaGraphInstantiate(&d->graph_exec, d->graph, 0), "cudaGraphInstantiate");
             std::copy(key, key + 8, d->graph_key);
+            finish();  // the results of the run before the capture
             return;
         }
         if (d->graph_exec) {  // this call may grow (move) workspaces the graph points into

@@ -234,3 +234,23 @@ def test_two_way_is_union_of_directions(setup, panda, name):
     ok = (ref_h['band'] == 0) & (ref_r['band'] == 0)
     assert np.array_equal(both['flags'][ok], (ref_h['hit'] | ref_r['hit'])[ok])
     assert (both['flags'] > o2r['flags']).sum() + (both['flags'] > r2o['flags']).sum() > 0
+
+
+def test_graph_with_host_buffers(ctx, panda):
+    """RTCD_CHECK_GRAPH with host arrays: the graph holds the staging copies,
+    so replays with new pose values (new host arrays of the same size) return
+    those poses' flags and counts, equal to the plain host path."""
+    mesh = scenes.discrete_small(seed=3)
+    robot = rtcd.Robot(ctx, panda)
+    scene = rtcd.Scene.from_mesh(ctx, mesh)
+    qs = [scenes.uniform_poses(panda, 700, seed=seed) for seed in (0, 1, 2)]
+    for kind in ('RobotToObs', 'ObsToRobot'):
+        det = rtcd.Detector(ctx, kind, robot, scene)
+        refs = [det.check(q, counts=True) for q in qs]
+        for q, ref in zip(qs + qs, refs + refs):   # captured on the first call, replayed after
+            got = det.check(q, counts=True, flags=rtcd.CHECK_GRAPH)
+            assert np.array_equal(got['flags'], ref['flags'])
+            assert np.array_equal(got['counts'], ref['counts'])
+        for q, ref in zip(qs, refs):
+            assert np.array_equal(det.check(q, flags=rtcd.CHECK_GRAPH)['flags'], ref['flags'])
+        det.close()

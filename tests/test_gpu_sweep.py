@@ -150,3 +150,22 @@ def test_binary_and_wide_trees_agree(sweep_setup, panda, kind):
             _cmp(det.check(q, off, segments=True), ref)
             _cmp(det.check(q, off, counts=True, segments=True), ref)
             det.close()
+
+
+def test_graph_with_host_buffers(sweep_setup, panda):
+    """RTCD_CHECK_GRAPH with host arrays on a sweep detector: replays with new
+    waypoints under the same trajectory offsets equal the plain host path
+    (trajectory flags, segment flags, counts)."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(96, 8, 40, seed=4)
+    runs = [scenes.random_walk_trajectories(panda, 96, n_wp, seed=s) for s in (4, 5)]
+    off = runs[0][1]
+    assert all(np.array_equal(o, off) for _, o in runs)
+    for kind in ('Linear', 'Quadratic'):
+        det = rtcd.Detector(robot.ctx, kind, robot, scene)
+        refs = [det.check(q, off, counts=True, segments=True) for q, _ in runs]
+        for (q, _), ref in zip(runs + runs, refs + refs):
+            got = det.check(q, off, counts=True, segments=True, flags=rtcd.CHECK_GRAPH)
+            for k in ('flags', 'seg_flags', 'counts'):
+                assert np.array_equal(got[k], ref[k]), k
+        det.close()
