@@ -962,10 +962,12 @@ template <bool R2O, bool PACKET>
 __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
     extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front]
     __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
+    __shared__ uint32_t s_hits[kAbWarps];  // a lane of the warp's current stage-B step hit its pose
     const DiscreteArgs& A = W.d;
     const int lane = threadIdx.x & 31;
     uint32_t* fr = s_front + (threadIdx.x >> 5) * S.wide_front;
     uint32_t* cb = s_cand[threadIdx.x >> 5];
+    volatile uint32_t* s_hit = s_hits + (threadIdx.x >> 5);
     const uint32_t lt = (1u << lane) - 1u;
     const float4* __restrict__ wn = R2O ? S.tri_wide : S.edge_wide;
     const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
@@ -1050,6 +1052,8 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 ++nbs;
                 bool hit = false;
                 StageBCand C;
+                if (lane == 0) *s_hit = 0u;
+                __syncwarp();
                 if (PACKET) {
                     const bool live =
                         prim != kNone && stage_b_setup<R2O>(R, S, W, make_uint2(item, prim), C, n_skip, n_rej, false);
@@ -1122,6 +1126,8 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                     uint32_t steps = 0, hits = 0;
                     bool spilled = false;
                     while (bsp > 0) {
+                        // flags only: another lane of this step has hit the pose, so the rest is moot
+                        if (!A.want_counts && *s_hit) break;
                         if (++steps > budget) {
                             const uint32_t h = atomicAdd(W.heavy_count, 1u);
                             if (h < W.heavy_cap) {
@@ -1137,7 +1143,10 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                             const uint32_t li = ref & ~kLeaf;
                             if (stage_b_leaf<R2O>(lp, wp, li, C, A.stats)) {
                                 hit = true;
-                                if (!A.want_counts) break;
+                                if (!A.want_counts) {
+                                    *s_hit = 1u;
+                                    break;
+                                }
                                 if (R2O) {
                                     const uint32_t eid = __float_as_uint(__ldg(lp + 2ull * li).w);
                                     atomicOr(A.edge_bits + (size_t) pose * A.edge_words + (eid >> 5), 1u << (eid & 31));
