@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
     uint32_t st[kStack];
     int sp = 0;
     bool busy = false;
-    uint32_t cur = 0, steps = 0, u_hits = 0;
+    uint32_t cur = 0, steps = 0, checked = 0, u_hits = 0;
     SweepUnit U;
     SweepCull c;
     U.traj = U.piece_g = 0;
@@ -493,11 +493,17 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
             busy = true;
             cur = u;
             steps = 0;
+            checked = 0;
             u_hits = 0;
             ++n_acc;
         }
         if (!busy) break;
         uint32_t leaf = kNone;
+        // flags only: every 8 visits, drop a unit whose piece (or trajectory) another unit decided
+        if (!A.want_counts && steps >= checked + 8) {
+            checked = steps;
+            if (A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj)) sp = 0;
+        }
         while (sp > 0) {
             const uint32_t ref = st[--sp];
             ++steps;
@@ -587,7 +593,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
                 busy = false;
                 continue;
             }
-            steps = 0;  // the heavy list is full: finish the unit here
+            steps = checked = 0;  // the heavy list is full: finish the unit here
         }
         if (sp == 0) {
             busy = false;
