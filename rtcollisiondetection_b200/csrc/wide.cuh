@@ -5,6 +5,8 @@
 
 namespace rtcd {
 
+constexpr int kWideBatch = 2;  // child records a lane loads before testing them (2 beat 4: fewer spills)
+
 // One round of a wide descent: every lane tests one child record (a, b) -
 // (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, bits(ref), 0); ref kNone in an empty
 // slot or a lane without a record - with test(box); overlapping internal
@@ -58,28 +60,33 @@ __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_
     const int j = lane >> lg;
     const uint32_t node = j < take ? fr[sp + j] : kNone;
     __syncwarp();
-    // this lane's kWide / g child records, all loads issued before the first test (the
-    // records of one node share a 128-byte line, but each is its own sector)
+    // this lane's kWide / g child records, kWideBatch loads issued before the first test of
+    // each batch (the records of one node share a 128-byte line, but each is its own sector)
     const int c0 = lane & (g - 1), rounds = kWide >> lg;
-    float4 ra[kWide], rb[kWide];
-#pragma unroll
-    for (int r = 0; r < kWide; ++r) {
-        ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
-        rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
-        if (r < rounds && node != kNone) {
-            const float4* rec = wn + 2ull * (kWide * (size_t) node + c0 + r * g);
-            ra[r] = __ldg(rec);
-            rb[r] = __ldg(rec + 1);
-        }
-    }
     bool ok = true;
 #pragma unroll
-    for (int r = 0; r < kWide; ++r) {
-        if (r >= rounds) break;  // warp-uniform
-        if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, test, front_cap, err, n_node, n_cand)) {
-            ok = false;
-            break;
+    for (int r0 = 0; r0 < kWide; r0 += kWideBatch) {
+        if (r0 >= rounds) break;  // warp-uniform
+        float4 ra[kWideBatch], rb[kWideBatch];
+#pragma unroll
+        for (int r = 0; r < kWideBatch; ++r) {
+            ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+            rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
+            if (r0 + r < rounds && node != kNone) {
+                const float4* rec = wn + 2ull * (kWide * (size_t) node + c0 + (r0 + r) * g);
+                ra[r] = __ldg(rec);
+                rb[r] = __ldg(rec + 1);
+            }
         }
+#pragma unroll
+        for (int r = 0; r < kWideBatch; ++r) {
+            if (r0 + r >= rounds) break;  // warp-uniform
+            if (!wide_round(ra[r], rb[r], fr, sp, cb, nc, test, front_cap, err, n_node, n_cand)) {
+                ok = false;
+                break;
+            }
+        }
+        if (!ok) break;
     }
     __syncwarp();
     return ok;
