@@ -461,6 +461,12 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
     const float4* __restrict__ en = WIDE ? S.edge_wide : S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
     const uint32_t root = WIDE ? S.edge_wide_root : S.edge_root;
+    // the piece (trajectory without segment flags) this warp's lanes hit last: the lanes
+    // on it stop at once (flags only; other decided units at their next 8-visit check)
+    __shared__ uint32_t s_decided[BLOCK / 32];
+    volatile uint32_t* decided = s_decided + (threadIdx.x >> 5);
+    if ((threadIdx.x & 31) == 0) *decided = kNone;
+    __syncwarp();
     uint32_t st[kStack];
     int sp = 0;
     bool busy = false;
@@ -500,6 +506,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
         if (!busy) break;
         uint32_t leaf = kNone;
         // flags only: every 8 visits, drop a unit whose piece (or trajectory) another unit decided
+        if (!A.want_counts && *decided == (A.want_pieces ? U.piece_g : U.traj)) sp = 0;
         if (!A.want_counts && steps >= checked + 8) {
             checked = steps;
             if (A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj)) sp = 0;
@@ -582,6 +589,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(con
                     ++u_hits;
                 } else {
                     atomicExch(A.traj_hit + U.traj, 1u);
+                    *decided = A.want_pieces ? U.piece_g : U.traj;
                     sp = 0;  // this unit is decided
                 }
             }
