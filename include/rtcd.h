@@ -117,7 +117,7 @@ typedef struct {
     uint32_t light_steps;            /* node + leaf visits one lane spends on a unit of traversal work (a
                                         discrete (link item, scene primitive) candidate, a sweep (piece,
                                         sphere) unit) before a whole warp takes it over; 0 = 32 (16 for
-                                        the quadratic sweep), 0xFFFFFFFF = never */
+                                        the sweeps), 0xFFFFFFFF = never */
     uint32_t stage_b_form;           /* discrete stage B: 1 = one lane per candidate, 2 = 32-candidate packets
                                         that share each link-BVH node load, 3 = stages A and B fused in one
                                         warp per item (an item stops generating candidates once its pose

@@ -1179,7 +1179,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.want_pieces = want_pieces;
     A.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                     : d->cfg.light_steps                ? d->cfg.light_steps
-                                                              : (quad ? 16u : 32u);
+                                                              : 16u;
     if (A.light_steps) {
         // room for every unit (near dense geometry most units of a piece can spill)
         const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns, 1024), 1u << 24);
