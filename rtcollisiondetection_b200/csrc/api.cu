@@ -923,7 +923,8 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
         launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
     }
     DiscreteArgs F = A;
-    F.items = d->overflow_items.as<uint32_t>();
+    F.items = d->overflow_items.as<uint32_t>();  // item words
+    F.link_major = 0;
     F.n_items = wc + 1;
     F.work_counter = wc + 2;
     launch_discrete(r2o, R, d->scene->dev, F, d->blocks, s);
@@ -951,7 +952,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     if (flags & RTCD_CHECK_NO_CULL) {
         launch_all_items(R, n, d->items.as<uint32_t>(), d->count.as<uint32_t>(), s);
     } else {
-        launch_cull(R, d->scene->dev, d->T.as<float4>(), n, d->mask.as<uint8_t>(), s);
+        launch_cull(R, d->scene->dev, d->T.as<float4>(), n, d->mask.as<uint8_t>(), true, s);
         select_u8(d->mask.as<uint8_t>(), n * L, d->items.as<uint32_t>(), d->count.as<uint32_t>(), d->scan,
                   d->err.as<uint32_t>(), s);
     }
@@ -967,6 +968,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     DiscreteArgs A{};
     A.T = d->T.as<float4>();
     A.items = d->items.as<uint32_t>();
+    A.link_major = (flags & RTCD_CHECK_NO_CULL) ? 0u : 1u;
     A.n_items = d->count.as<uint32_t>();
     A.n_poses = n;
     A.pose_hit = d_hit;

@@ -121,11 +121,26 @@ __device__ __forceinline__ bool obb_overlap(const ObbW& A, const float* B) {
 }
 
 constexpr int kCullChunk = 256;  // obstacle OBBs staged in shared memory per pass
+// The culled items are compacted link by link, the last (most distal) link
+// of every pose first, then every pose's next-to-last, ...: in flags mode a
+// pose hit through one link is decided before most of its other links' items
+// start, and those stop at their first check instead of running beside it.
+// The distal links sweep most of the workspace and decide most colliding
+// poses, so they go first (the 65,536-pose dense scene: 2.07 ms pose-major,
+// 1.51 ms base link first, 1.20 ms last link first).  item_word turns a
+// compacted index back into pose * n_links + link.
+__device__ __forceinline__ uint32_t link_slot(uint32_t link, uint32_t n_links) { return n_links - 1 - link; }
+__device__ __forceinline__ uint32_t item_word(const DiscreteArgs& A, uint32_t n_links, uint32_t j) {
+    if (!A.link_major) return j;
+    const uint32_t slot = j / A.n_poses, pose = j - slot * A.n_poses;
+    return pose * n_links + link_slot(slot, n_links);
+}
 
 // One thread per (pose, link): the link OBB against every obstacle OBB, with a
 // bounding-sphere reject before the full test.
 __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __restrict__ sobb, uint32_t n_obs,
-                                             const float4* __restrict__ T, uint32_t n, uint8_t* __restrict__ mask) {
+                                             const float4* __restrict__ T, uint32_t n, uint8_t* __restrict__ mask,
+                                             bool link_major) {
     __shared__ float s_obb[kCullChunk * 16];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t pose = i / R.n_links, link = i % R.n_links;
@@ -155,13 +170,14 @@ __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __r
             }
         }
     }
-    if (pose < n) mask[i] = hit ? 1 : 0;
+    if (pose < n) mask[link_major ? (size_t) link_slot(link, R.n_links) * n + pose : i] = hit ? 1 : 0;
 }
 
-void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, cudaStream_t s) {
+void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, bool link_major,
+                 cudaStream_t s) {
     uint32_t total = n * R.n_links;
     if (!total) return;
-    k_cull<<<(total + 255) / 256, 256, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask);
+    k_cull<<<(total + 255) / 256, 256, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask, link_major);
     cuda_check(cudaGetLastError(), "k_cull");
 }
 
@@ -348,7 +364,7 @@ __global__ void __launch_bounds__(kTravThreads) k_discrete(const RobotDev R, con
             base = g.shfl(base, 0);
             uint32_t it = base + g.thread_rank();
             if (it >= n_items) break;
-            uint32_t item = A.items[it];
+            uint32_t item = item_word(A, R.n_links, A.items[it]);
             pose = item / R.n_links;
             link = item - pose * R.n_links;
             if (pose >= A.n_poses || wroot == kNone) {
@@ -523,7 +539,7 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
         if (lane == 0) it = atomicAdd(A.work_counter, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
-        const uint32_t item = A.items[it];
+        const uint32_t item = item_word(A, R.n_links, A.items[it]);
         const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
         if (pose >= A.n_poses) {
             if (lane == 0) atomicOr(A.err, kErrRange);
@@ -983,7 +999,7 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
         if (lane == 0) it = atomicAdd(A.work_counter, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= n_items) break;
-        const uint32_t item = A.items[it];
+        const uint32_t item = item_word(A, R.n_links, A.items[it]);
         const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
         if (pose >= A.n_poses) {
             if (lane == 0) atomicOr(A.err, kErrRange);
@@ -1649,7 +1665,7 @@ __global__ void __launch_bounds__(128) k_contain(const RobotDev R, const SceneDe
     const uint32_t n_items = *A.n_items;
     const f3 dir = contain_dir();
     for (uint32_t it = blockIdx.x * blockDim.x + threadIdx.x; it < n_items; it += gridDim.x * blockDim.x) {
-        const uint32_t item = A.items[it];
+        const uint32_t item = item_word(A, R.n_links, A.items[it]);
         const uint32_t pose = item / R.n_links, link = item - pose * R.n_links;
         if (pose >= A.n_poses) {
             atomicOr(A.err, kErrRange);

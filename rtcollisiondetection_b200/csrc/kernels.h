@@ -51,6 +51,7 @@ struct SceneDev {
 struct DiscreteArgs {
     const float4* T;           // [pose][link][3] link transforms
     const uint32_t* items;     // compacted (pose * n_links + link); NULL = all links >= first_link
+    uint32_t link_major;       // items hold (link order slot) * n_poses + pose instead (see item_word)
     const uint32_t* n_items;   // device count of items
     uint32_t n_poses;
     uint32_t* pose_hit;        // [pose] nonzero when colliding
@@ -119,7 +120,10 @@ uint32_t stage_b_blocks(bool robot_to_obs);
 uint32_t stage_b_max_blocks_per_sm(bool robot_to_obs, uint32_t threads);  // threads: 64, 128 or 256
 
 void launch_fk_poses(const Chain& ch, const float* d_q, uint32_t n, float4* d_T, cudaStream_t s);
-void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, cudaStream_t s);
+// link_major: the mask (and so the compacted items) in link order, every pose's
+// last link before any pose's next-to-last one (item_word decodes it).
+void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, bool link_major,
+                 cudaStream_t s);
 void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t* d_count, cudaStream_t s);
 void launch_discrete(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t blocks,
                      cudaStream_t s);
