@@ -968,7 +968,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     DiscreteArgs A{};
     A.T = d->T.as<float4>();
     A.items = d->items.as<uint32_t>();
-    A.link_major = (flags & RTCD_CHECK_NO_CULL) ? 0u : 1u;
+    A.link_major = 1u;
     A.n_items = d->count.as<uint32_t>();
     A.n_poses = n;
     A.pose_hit = d_hit;

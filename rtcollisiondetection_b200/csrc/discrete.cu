@@ -181,12 +181,14 @@ void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32
     cuda_check(cudaGetLastError(), "k_cull");
 }
 
+// Every item, in the link-major order of the culled list (item_word): the
+// slots of links n_links - 1 down to first_link, each over all poses.
 __global__ void k_all_items(uint32_t n_links, uint32_t first, uint32_t n, uint32_t* items, uint32_t* count) {
     uint32_t per = n_links - first;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) *count = n * per;
     if (i >= n * per) return;
-    items[i] = (i / per) * n_links + first + (i % per);
+    items[i] = i;
 }
 
 void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t* d_count, cudaStream_t s) {
