@@ -450,14 +450,15 @@ __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ ep, uint32_t
 // recounted there), so one lane never serialises a unit that meets thousands
 // of nodes.
 // The quadratic form is capped at 96 registers (5 blocks of 128 threads per
-// SM): the extra resident warps hide more load latency than the few spilled
-// registers cost (measured on the 4,096-trajectory quadratic workload).
+// SM), the linear one at 80 (6 blocks): the extra resident warps hide more
+// load latency than the few spilled registers cost (measured on the
+// 4,096-trajectory workloads; 6 blocks slowed the quadratic form).
 // WIDE: the descent runs over the scene's 4-wide edge tree (a node's four
 // child records loaded at once, the overlapping children pushed far to near
 // so the nearest is visited first), half the dependent node loads of the
 // binary tree; it needs a wide tree shallow enough for the lane stack.
 template <bool QUAD, int BLOCK, bool WIDE>
-__global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 1) k_sweep(const SceneDev S, const SweepArgs A) {
+__global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOCK) k_sweep(const SceneDev S, const SweepArgs A) {
     const float4* __restrict__ en = WIDE ? S.edge_wide : S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
     const uint32_t root = WIDE ? S.edge_wide_root : S.edge_root;
