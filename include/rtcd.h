@@ -61,7 +61,7 @@ typedef enum {
 #define RTCD_CHECK_COUNTS (1u << 0)        /* also produce the upstream hit counts (no early exit) */
 #define RTCD_CHECK_HOST_BUFFERS (1u << 1)  /* q, traj offsets and outputs are host memory */
 #define RTCD_CHECK_NO_CULL (1u << 2)       /* skip the OBB prefilter of the discrete detectors (every item goes to
-                                              the traversal, whose first step rejects the far ones: 3-9 % faster at
+                                              the traversal, whose first step rejects the far ones: up to 9 % faster at
                                               a few thousand poses, slower at tens of thousands) */
 #define RTCD_CHECK_PLAIN (1u << 3)         /* frame-by-frame path with a host sync per frame */
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
