@@ -621,12 +621,15 @@ __global__ void __launch_bounds__(kStageAWarps * 32) k_stage_a(const RobotDev R,
 // Stage B works on one candidate (item, scene primitive) at a time: move the
 // scene primitive into the link frame, reject it against the link OBB,
 // descend the link LBVH and run the exact segment-triangle test at the leaves.
+constexpr float kBigTri = 0.03f;  // m: triangles whose box is longer get the edge-axis node test
+
 struct StageBCand {
     float4 T[3];
     f3 c0, c1, c2, cn, cinv;  // primitive in the link frame; triangle normal (R2O) / 1 / segment (O2R)
     float cw;                 // plane offset n.c0 (R2O)
     float blo[3], bhi[3];     // triangle box (R2O)
     uint32_t pose, lroot, prim;
+    bool big;                 // R2O: a triangle large enough for the edge-axis node test
 };
 
 // 0: nothing to do (blank, decided, overflowed item, empty link, OBB reject); 1: descend.
@@ -658,6 +661,7 @@ __device__ __forceinline__ int stage_b_setup(const RobotDev& R, const SceneDev& 
     const float4* __restrict__ wp = R2O ? S.tri_prims : S.edge_prims;
     C.c2 = C.cn = C.cinv = mk(0.f, 0.f, 0.f);
     C.cw = 0.f;
+    C.big = false;
     if (R2O) {
         const float4* t = wp + 3ull * cd.y;
         C.c0 = xf_inv(C.T, f3of(__ldg(t)));
@@ -674,6 +678,7 @@ __device__ __forceinline__ int stage_b_setup(const RobotDev& R, const SceneDev& 
         C.blo[0] = fminf(C.c0.x, fminf(C.c1.x, C.c2.x)) - kBoxTol; C.bhi[0] = fmaxf(C.c0.x, fmaxf(C.c1.x, C.c2.x)) + kBoxTol;
         C.blo[1] = fminf(C.c0.y, fminf(C.c1.y, C.c2.y)) - kBoxTol; C.bhi[1] = fmaxf(C.c0.y, fmaxf(C.c1.y, C.c2.y)) + kBoxTol;
         C.blo[2] = fminf(C.c0.z, fminf(C.c1.z, C.c2.z)) - kBoxTol; C.bhi[2] = fmaxf(C.c0.z, fmaxf(C.c1.z, C.c2.z)) + kBoxTol;
+        C.big = fmaxf(fmaxf(C.bhi[0] - C.blo[0], C.bhi[1] - C.blo[1]), C.bhi[2] - C.blo[2]) > kBigTri;
     } else {
         const float4* e = wp + 2ull * cd.y;
         C.c0 = xf_inv(C.T, f3of(__ldg(e)));
@@ -696,10 +701,44 @@ __device__ __forceinline__ int stage_b_setup(const RobotDev& R, const SceneDev& 
 
 // Node test: the box overlaps the triangle's box and straddles its plane
 // (R2O), or the segment passes through the box (O2R).
-template <bool R2O>
+// The nine edge-cross separating axes of a triangle and a box (edge i x world
+// axis k), the box grown by pad: false when one separates them.  Together
+// with the box overlap and the plane straddle this is the full 13-axis
+// triangle-box test; it prunes the link-tree nodes near a large triangle's
+// plane but beyond its edges.
+__device__ __forceinline__ bool tri_box_edges(const f3& c0, const f3& c1, const f3& c2, const Box& b, float pad) {
+    const f3 m = mk(0.5f * (b.lo[0] + b.hi[0]), 0.5f * (b.lo[1] + b.hi[1]), 0.5f * (b.lo[2] + b.hi[2]));
+    const float hx = 0.5f * (b.hi[0] - b.lo[0]) + pad, hy = 0.5f * (b.hi[1] - b.lo[1]) + pad,
+                hz = 0.5f * (b.hi[2] - b.lo[2]) + pad;
+    const f3 v0 = c0 - m, v1 = c1 - m, v2 = c2 - m;
+    const f3 f[3] = {v1 - v0, v2 - v1, v0 - v2};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const f3 e = f[i];
+        // x cross e = (0, -e.z, e.y)
+        float p0 = -e.z * v0.y + e.y * v0.z, p1 = -e.z * v1.y + e.y * v1.z, p2 = -e.z * v2.y + e.y * v2.z;
+        float r = hy * fabsf(e.z) + hz * fabsf(e.y);
+        if (fminf(p0, fminf(p1, p2)) > r || fmaxf(p0, fmaxf(p1, p2)) < -r) return false;
+        // y cross e = (e.z, 0, -e.x)
+        p0 = e.z * v0.x - e.x * v0.z; p1 = e.z * v1.x - e.x * v1.z; p2 = e.z * v2.x - e.x * v2.z;
+        r = hx * fabsf(e.z) + hz * fabsf(e.x);
+        if (fminf(p0, fminf(p1, p2)) > r || fmaxf(p0, fmaxf(p1, p2)) < -r) return false;
+        // z cross e = (-e.y, e.x, 0)
+        p0 = -e.y * v0.x + e.x * v0.y; p1 = -e.y * v1.x + e.x * v1.y; p2 = -e.y * v2.x + e.x * v2.y;
+        r = hx * fabsf(e.y) + hy * fabsf(e.x);
+        if (fminf(p0, fminf(p1, p2)) > r || fmaxf(p0, fmaxf(p1, p2)) < -r) return false;
+    }
+    return true;
+}
+
+// EDGES: large triangles also get the edge axes (the fused and heavy passes;
+// the one-lane pass over deferred candidates is faster without them).
+template <bool R2O, bool EDGES = true>
 __device__ __forceinline__ bool stage_b_node(const StageBCand& C, const Box& b) {
     constexpr float kBoxTol = 2e-5f;
-    if (R2O) return box_overlap(b, C.blo, C.bhi) && plane_box(C.cn, C.cw, b, kBoxTol);
+    if (R2O)
+        return box_overlap(b, C.blo, C.bhi) && plane_box(C.cn, C.cw, b, kBoxTol) &&
+               (!EDGES || !C.big || tri_box_edges(C.c0, C.c1, C.c2, b, kBoxTol));
     return seg_box(C.c0, C.cinv, b, kBoxTol);
 }
 
@@ -790,7 +829,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_b(const RobotDev R, const Scene
             uint32_t rl, rr;
             load_node(ln, ref, bl, br, rl, rr);
             n_node += 2;
-            const bool hr = stage_b_node<R2O>(C, br), hl = stage_b_node<R2O>(C, bl);
+            const bool hr = stage_b_node<R2O, false>(C, br), hl = stage_b_node<R2O, false>(C, bl);
             if (sp + 2 > kStack) {
                 atomicOr(A.err, kErrStack);
                 break;
