@@ -73,6 +73,14 @@ typedef enum {
 #define RTCD_CHECK_TWO_WAY (1u << 9)       /* discrete: run both directions (ObsToRobot and RobotToObs) in one check
                                               over the same FK, cull and items: flags are the union, counts the
                                               sum of the two upstream counts */
+#define RTCD_CHECK_SURFACE (1u << 10)       /* sweeps: the reference's semantics instead of the solid ones.  The scene's
+                                              directed loop edges (RTCD/Meshes/mesh.h:378-620) are cast, and an edge
+                                              hits a swept piece only when it starts outside the piece and reaches it
+                                              (the curve intersectors report entering rays only, CCCuda.cu:37-41);
+                                              linear pieces are round-capped capsules, quadratic pieces are cut by
+                                              flat caps normal to their end tangents and carry no start/end spheres.
+                                              The first such check on a scene builds its loop-edge tree (once,
+                                              synchronously): make it before any stream capture */
 #define RTCD_CHECK_GRAPH (1u << 7)         /* replay the launch sequence as a CUDA graph (captured on the first call
                                               with these pointers, sizes, flags and - for sweeps - trajectory
                                               offsets; any other call on the detector retires it).  With
@@ -176,6 +184,16 @@ RTCD_API rtcd_status rtcd_urdf_chain_parse(const char* urdf, size_t len, rtcd_ur
 RTCD_API rtcd_status rtcd_obj_load(const char* path, float* verts_out, uint32_t max_verts, uint32_t* n_verts,
                                    uint32_t* tris_out, uint32_t max_tris, uint32_t* n_tris);
 
+/* Directed loop edges of a triangle mesh (upstream meshModel::loadOBJ,
+ * RTCD/Meshes/mesh.h:378-620): every triangle's edges, in the directions
+ * kept, run around it as a loop; an edge two neighbouring triangles need in
+ * opposite directions is kept in both.  The directions follow the upstream
+ * breadth-first walk over the triangles in index order.  edges_out receives
+ * (from, to) vertex pairs, at most max_edges of them; call with NULL to learn
+ * the count.  Host only (no GPU). */
+RTCD_API rtcd_status rtcd_loop_edges(const uint32_t* tris, uint32_t n_tris, uint32_t* edges_out, uint32_t max_edges,
+                                     uint32_t* n_edges);
+
 /* Replaces robot<DOF>(robotConfig) and the link GAS builds
  * (RTCD/Robot/robot.h:91-124, RTCD/Robot/batchIASRobot.h:310-365): uploads
  * the chain and builds one triangle and one edge LBVH per link. */
@@ -246,7 +264,8 @@ RTCD_API rtcd_status rtcd_detector_autotune(rtcd_detector* det, const float* q_d
                                             uint32_t n, void* stream, rtcd_config* best_out, float* best_ms);
 
 /* Segments per trajectory for the sweep kinds: linear n_wp - 1; quadratic
- * max(3, ceil(n_wp/2)) - 2 (+2 start/end spheres unless RTCD_CHECK_NO_ENDPOINTS).
+ * max(3, ceil(n_wp/2)) - 2 (+2 start/end spheres unless RTCD_CHECK_NO_ENDPOINTS
+ * or RTCD_CHECK_SURFACE).
  * offsets_out (n + 1 entries, host) is the exclusive prefix sum. */
 RTCD_API rtcd_status rtcd_segment_offsets(rtcd_detector_kind kind, const uint32_t* traj_offsets, uint32_t n, uint32_t flags,
                                  uint32_t* offsets_out);
@@ -321,14 +340,16 @@ RTCD_API rtcd_status rtcd_server_prepare(rtcd_server* server, rtcd_detector* det
 /* Finishes every accepted request, then stops the workers. */
 RTCD_API rtcd_status rtcd_server_destroy(rtcd_server* server);
 /* Copies the inputs (host memory, as rtcd_check with RTCD_CHECK_HOST_BUFFERS)
- * and returns a ticket at once.  `flags` may carry RTCD_CHECK_COUNTS and
- * RTCD_CHECK_NO_ENDPOINTS. */
+ * and returns a ticket at once.  `flags` may carry RTCD_CHECK_COUNTS,
+ * RTCD_CHECK_NO_ENDPOINTS and RTCD_CHECK_SURFACE. */
 RTCD_API rtcd_status rtcd_server_submit(rtcd_server* server, rtcd_detector* det, const float* q,
                                         const uint32_t* traj_offsets, uint32_t n, uint32_t flags, uint64_t* ticket);
 /* Waits up to timeout_ms (RTCD_WAIT_FOREVER: no limit) for the ticket; on
  * completion copies the outputs (any may be NULL), releases the ticket and
  * reports the request's latency.  RTCD_ERR_DEVICE_TIMEOUT when the wait ran
- * out (the ticket stays valid). */
+ * out (the ticket stays valid).  When several threads wait on one ticket, the
+ * first to find it complete collects it; the others return
+ * RTCD_ERR_INVALID_ARGUMENT ("collected by another waiter"). */
 RTCD_API rtcd_status rtcd_server_wait(rtcd_server* server, uint64_t ticket, int32_t timeout_ms, uint8_t* flags_out,
                                       uint8_t* seg_flags_out, uint32_t* counts_out, double* latency_ms);
 RTCD_API rtcd_status rtcd_server_get_stats(rtcd_server* server, rtcd_server_stats* out);
@@ -385,6 +406,17 @@ RTCD_API rtcd_status rtcd_exclusive_scan_u32(rtcd_ctx* ctx, const uint32_t* in_d
 RTCD_API rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
                                           uint32_t* count_dev, void* stream);
 
+/* Self-test of the failure detection of the bounded device waits.  No
+ * counterpart in the reference (its device code has no bounded waits).  Runs
+ * the compaction of n (1 to 1,048,576) zero flags with the tile counter
+ * seeded so that no block takes tile 0: tile 0's look-back word is never
+ * published, every other tile's look-back waits on it, and each wait gives up
+ * after spin_limit (1 to 65,536) polls, sets the device error word and lets
+ * its block finish.  Returns RTCD_ERR_DEVICE_TIMEOUT when the waits ran out
+ * as designed (the context stays usable), RTCD_ERR_INTERNAL if they did not.
+ * Synchronous on the context stream. */
+RTCD_API rtcd_status rtcd_selftest_lookback_timeout(rtcd_ctx* ctx, uint32_t n, uint32_t spin_limit);
+
 /* rtcd_select_flags_u8 for callers that cannot allocate device memory when
  * they query: a control loop with a hard deadline cannot afford cudaMalloc /
  * cudaFree (they may synchronise the device and take unbounded time), and a
@@ -393,9 +425,10 @@ RTCD_API rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev
  * fixed 131 KB device array inside this library, so the call allocates
  * nothing; that array is held on every GPU that loads the library until the
  * process exits.  Limit: n <= 33,554,432 flags (RTCD_ERR_CAPACITY beyond).
- * The first call on a device, made with that device current, looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  All calls share the one array, and it keeps the
+ * Every call looks up the array's device address on the current device
+ * (cudaGetSymbolAddress), so the call stays valid after cudaDeviceReset; the
+ * first call on a device may also load the library's device code there, so
+ * make that first call before any stream capture.  All calls share the one array, and it keeps the
  * previous call's contents (each call first clears the words it uses); two
  * calls that overlap on the GPU would race on it, so the library serialises
  * them: each call takes a process-wide lock and returns only after its work

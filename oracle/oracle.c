@@ -142,6 +142,189 @@ int orc_unique_edges(const u32* tris, int n_tris, u32* edges) {
     return ne;
 }
 
+/* Loop edges (RTCD/Meshes/mesh.h:378-620): directed edges chosen so that the
+ * three edges of every triangle, taken in their directions, run around it as
+ * a loop (v0->v1->v2->v0 or the reverse); an edge shared by two triangles that
+ * need opposite directions is kept in both.  The continuous detectors cast
+ * these instead of the unique edges: the curve intersectors report only a ray
+ * entering the swept surface, and a triangle boundary that crosses a closed
+ * surface crosses it inwards somewhere along the loop.
+ *
+ * The direction choice follows the upstream breadth-first walk exactly:
+ * start at the first unprocessed triangle (index order); pop a triangle,
+ * classify its three edges against the directed set (forward, backward, both,
+ * undecided), complete the loop by the rules below, mark it processed and
+ * queue its unprocessed neighbours (per undirected edge, triangles in
+ * increasing index).  Rules, by the number of decided edges:
+ *   3: not yet a loop -> the "rule breaker" gets its reverse added (equal
+ *      forward/backward counts: the first edge not in both directions; fewer
+ *      forward: the first forward edge; else the first backward edge);
+ *   2: the two disagree (one forward, one backward) -> the first of them gets
+ *      its reverse added and the undecided edge takes the opposite of that
+ *      edge's direction; they agree -> the undecided edge takes the direction
+ *      of the first edge decided one way only (forward when both are decided
+ *      both ways: the upstream reads an unset variable there);
+ *   1: the undecided edges take the decided edge's direction (an edge decided
+ *      both ways counts as backward, as upstream);
+ *   0: all three forward.
+ * Output order: triangles in index order, per triangle its edges in order,
+ * forward before backward, each directed edge at its first triangle.
+ * Returns the count of directed edges written to `edges` (room for 6 *
+ * n_tris pairs), or -1 when a triangle does not close a loop (the mesh is not
+ * watertight: the upstream throws). */
+typedef struct { uint64_t key; int used; } key_slot;
+typedef struct { key_slot* tab; size_t cap; } key_set;
+
+static uint64_t dkey(u32 a, u32 b) { return ((uint64_t) a << 32) | b; }
+static size_t ks_find(const key_set* s, uint64_t k) {
+    size_t h = hash_pair((u32) (k >> 32), (u32) k) & (s->cap - 1);
+    while (s->tab[h].used && s->tab[h].key != k) h = (h + 1) & (s->cap - 1);
+    return h;
+}
+static int ks_has(const key_set* s, u32 a, u32 b) { return s->tab[ks_find(s, dkey(a, b))].used == 1; }
+static void ks_add(key_set* s, u32 a, u32 b) {
+    size_t h = ks_find(s, dkey(a, b));
+    s->tab[h].used = 1;
+    s->tab[h].key = dkey(a, b);
+}
+static int ks_take(key_set* s, u32 a, u32 b) {  /* erase: the slot stays occupied (2) so probes pass it */
+    size_t h = ks_find(s, dkey(a, b));
+    if (s->tab[h].used != 1) return 0;
+    s->tab[h].used = 2;
+    return 1;
+}
+
+typedef struct { uint64_t key; int tri; } edge_tri;
+static int edge_tri_cmp(const void* a, const void* b) {
+    const edge_tri *x = (const edge_tri*) a, *y = (const edge_tri*) b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->tri - y->tri;
+}
+
+enum { E_UNDEF = 0, E_FWD = 1, E_BWD = 2, E_BOTH = 3 };
+
+int orc_loop_edges(const u32* tris, int n_tris, u32* edges) {
+    if (n_tris <= 0) return 0;
+    key_set S;
+    S.cap = 1;
+    while (S.cap < (size_t) n_tris * 8 + 16) S.cap <<= 1;
+    S.tab = (key_slot*) calloc(S.cap, sizeof(key_slot));
+    /* undirected edge -> triangles, sorted by (edge, triangle) */
+    edge_tri* et = (edge_tri*) malloc(sizeof(edge_tri) * 3 * (size_t) n_tris);
+    unsigned char* done = (unsigned char*) calloc((size_t) n_tris, 1);
+    size_t qcap = (size_t) n_tris * 4 + 16, qh = 0, qt = 0;
+    int* queue = (int*) malloc(sizeof(int) * qcap);
+    if (!S.tab || !et || !done || !queue) { free(S.tab); free(et); free(done); free(queue); return -1; }
+    for (int t = 0; t < n_tris; ++t)
+        for (int k = 0; k < 3; ++k) {
+            u32 a = tris[t * 3 + k], b = tris[t * 3 + (k + 1) % 3];
+            et[t * 3 + k].key = a < b ? dkey(a, b) : dkey(b, a);
+            et[t * 3 + k].tri = t;
+        }
+    size_t n_et = 3 * (size_t) n_tris;
+    qsort(et, n_et, sizeof(edge_tri), edge_tri_cmp);
+    int next_start = 0;
+    while (1) {
+        while (next_start < n_tris && done[next_start]) ++next_start;
+        if (next_start >= n_tris) break;
+        qh = qt = 0;
+        queue[qt++] = next_start;
+        while (qh < qt) {
+            int cur = queue[qh++];
+            if (done[cur]) continue;
+            u32 L[4] = {tris[cur * 3], tris[cur * 3 + 1], tris[cur * 3 + 2], tris[cur * 3]};
+            int ty[3], fc = 0, bc = 0, nd = 0, und[3], nu = 0;
+            for (int i = 0; i < 3; ++i) {
+                int f = ks_has(&S, L[i], L[i + 1]), b = ks_has(&S, L[i + 1], L[i]);
+                ty[i] = f && b ? E_BOTH : f ? E_FWD : b ? E_BWD : E_UNDEF;
+                if (f) ++fc;
+                if (b) ++bc;
+                if (f || b) ++nd; else und[nu++] = i;
+            }
+            if (nd == 3) {
+                if (!(fc == 3 || bc == 3)) {
+                    int rb = -1;
+                    for (int i = 0; i < 3 && rb < 0; ++i) {
+                        if (fc == bc) { if (ty[i] != E_BOTH) rb = i; }
+                        else if (fc < bc) { if (ty[i] == E_FWD) rb = i; }
+                        else if (ty[i] == E_BWD) rb = i;
+                    }
+                    if (rb >= 0) {
+                        if (ty[rb] == E_FWD) ks_add(&S, L[rb + 1], L[rb]);
+                        else ks_add(&S, L[rb], L[rb + 1]);
+                    }
+                }
+            } else if (nd == 2) {
+                int k = und[0], dir = E_FWD;
+                if (!(fc == 2 || bc == 2)) {
+                    for (int i = 0; i < 3; ++i)
+                        if (ty[i] == E_FWD || ty[i] == E_BWD) {
+                            if (ty[i] == E_FWD) { ks_add(&S, L[i + 1], L[i]); dir = E_BWD; }
+                            else { ks_add(&S, L[i], L[i + 1]); dir = E_FWD; }
+                            break;
+                        }
+                } else {
+                    for (int i = 0; i < 3; ++i)
+                        if (ty[i] == E_FWD || ty[i] == E_BWD) { dir = ty[i]; break; }
+                }
+                if (dir == E_FWD) ks_add(&S, L[k], L[k + 1]);
+                else ks_add(&S, L[k + 1], L[k]);
+            } else if (nd == 1) {
+                int dir = E_UNDEF;
+                for (int i = 0; i < 3; ++i)
+                    if (ty[i] != E_UNDEF) { dir = ty[i]; break; }
+                for (int j = 0; j < nu; ++j) {
+                    int k = und[j];
+                    if (dir == E_FWD) ks_add(&S, L[k], L[k + 1]);
+                    else ks_add(&S, L[k + 1], L[k]);
+                }
+            } else {
+                for (int i = 0; i < 3; ++i) ks_add(&S, L[i], L[i + 1]);
+            }
+            done[cur] = 1;
+            for (int i = 0; i < 3; ++i) {
+                u32 a = L[i], b = L[i + 1];
+                uint64_t key = a < b ? dkey(a, b) : dkey(b, a);
+                /* first (edge, triangle) entry of this edge */
+                size_t lo = 0, hi = n_et;
+                while (lo < hi) { size_t m = (lo + hi) / 2; if (et[m].key < key) lo = m + 1; else hi = m; }
+                for (size_t j = lo; j < n_et && et[j].key == key; ++j) {
+                    int t = et[j].tri;
+                    if (j > lo && et[j - 1].tri == t) continue;  /* a set holds each triangle once */
+                    if (t != cur && !done[t]) {
+                        if (qt == qcap) { qcap *= 2; queue = (int*) realloc(queue, sizeof(int) * qcap); }
+                        queue[qt++] = t;
+                    }
+                }
+            }
+        }
+    }
+    /* every triangle must now be a loop */
+    int ok = 1;
+    for (int t = 0; t < n_tris && ok; ++t) {
+        u32 L[4] = {tris[t * 3], tris[t * 3 + 1], tris[t * 3 + 2], tris[t * 3]};
+        int fc = 0, bc = 0;
+        for (int i = 0; i < 3; ++i) {
+            int f = ks_has(&S, L[i], L[i + 1]), b = ks_has(&S, L[i + 1], L[i]);
+            if (!f && !b) ok = 0;
+            fc += f; bc += b;
+        }
+        if (!(fc == 3 || bc == 3)) ok = 0;
+    }
+    int n = 0;
+    if (ok) {
+        for (int t = 0; t < n_tris; ++t) {
+            u32 L[4] = {tris[t * 3], tris[t * 3 + 1], tris[t * 3 + 2], tris[t * 3]};
+            for (int i = 0; i < 3; ++i) {
+                if (ks_take(&S, L[i], L[i + 1])) { edges[2 * n] = L[i]; edges[2 * n + 1] = L[i + 1]; ++n; }
+                if (ks_take(&S, L[i + 1], L[i])) { edges[2 * n] = L[i + 1]; edges[2 * n + 1] = L[i]; ++n; }
+            }
+        }
+    }
+    free(S.tab); free(et); free(done); free(queue);
+    return ok ? n : -1;
+}
+
 /* ------------------------------------------------------------ canonical LBVH */
 static u32 expand_bits(u32 v) {
     v = (v * 0x00010001u) & 0xFF0000FFu;
@@ -868,6 +1051,8 @@ typedef struct {
     d3 a, b;        /* capsule axis (linear) */
     d3 B0, B1, B2;  /* quadratic Bezier piece */
     int quad;
+    int surface;    /* reference semantics: a directed edge hits when it enters the piece (below) */
+    d3 n0, n1;      /* quadratic, surface: unit normals of the flat end caps (zero: no cap) */
     double r, eps;
     const float* sv; const u32* se;  /* scene verts / edges */
     int any_hit, robust, marginal;
@@ -915,10 +1100,116 @@ static double seg_quad_dist(d3 p, d3 q, d3 B0, d3 B1, d3 B2, double hit_below, d
     return ub;
 }
 
+/* ---- surface (reference) semantics of the sweeps.
+ * The upstream casts each directed loop edge p -> q as a ray (tmin 0, tmax
+ * |q - p|, RTCD/CollisionDetector/CCCuda.cu:56-77) against OptiX's built-in
+ * curve intersectors and counts every reported intersection in its any-hit
+ * program (CCCuda.cu:37-41).  Those intersectors report a ray entering a
+ * curve primitive from outside, not a ray that starts inside it; that is why
+ * the curve scenes cast loop edges (RTCD/Meshes/mesh.h:378-620).  Per (edge,
+ * primitive) the predicate is therefore
+ *     hit  <=>  p lies outside the primitive's closed solid P  and  [p, q] meets P.
+ * Linear primitive: the capsule of radius r around the axis, round caps
+ * (endcapFlags = 1, RTCD/Robot/batchCurveRobot.h:230).  Quadratic primitive:
+ * the sphere-swept piece u in [0, 1] cut by flat caps, the planes through its
+ * ends normal to its end tangents (B1 - B0 at u = 0, B2 - B1 at u = 1; B2 - B0
+ * where one of those vanishes); the upstream comment on the quadratic curves'
+ * flat caps is RTCD/CollisionDetector/Test/testCollisionCheckerCurve.cpp:
+ * 157-162.  The cap disks belong to the solid (closed flat caps).  Quadratic
+ * pieces carry no start/end spheres in these semantics.
+ *
+ * Band: the pair is marginal when the decision changes with the radius and
+ * the cap planes moved by eps either way:
+ *   robust hit  = meets(r - eps, caps - eps) and not inside(p; r + eps, caps + eps)
+ *   robust miss = not meets(r + eps, caps + eps) or inside(p; r - eps, caps - eps). */
+static void quad_caps(d3 B0, d3 B1, d3 B2, d3* n0, d3* n1) {
+    d3 t0 = sub(B1, B0), t1 = sub(B2, B1), ch = sub(B2, B0);
+    if (dot(t0, t0) == 0.0) t0 = ch;
+    if (dot(t1, t1) == 0.0) t1 = ch;
+    double l0 = len(t0), l1 = len(t1);
+    *n0 = l0 > 0 ? mul(t0, 1.0 / l0) : v3(0, 0, 0);
+    *n1 = l1 > 0 ? mul(t1, 1.0 / l1) : v3(0, 0, 0);
+}
+
+/* the parameter range [t0, t1] of p + t (q - p), t in [0, 1], inside both cap
+ * half-spaces grown by g (negative g: shrunk); 0 when empty */
+static int cap_clip(const sweep_query* s, d3 p, d3 q, double g, double* t0, double* t1) {
+    d3 d = sub(q, p);
+    double lo = 0.0, hi = 1.0;
+    for (int k = 0; k < 2; ++k) {
+        /* signed distance inside: (x - B0).n0 at the start cap, (B2 - x).n1 at the end cap */
+        double a = k == 0 ? dot(sub(p, s->B0), s->n0) : dot(sub(s->B2, p), s->n1);
+        double b = k == 0 ? dot(d, s->n0) : -dot(d, s->n1);
+        if (k == 0 ? dot(s->n0, s->n0) == 0.0 : dot(s->n1, s->n1) == 0.0) continue;
+        /* a + b t >= -g */
+        if (b == 0.0) { if (a < -g) return 0; continue; }
+        double t = (-g - a) / b;
+        if (b > 0) { if (t > lo) lo = t; }
+        else if (t < hi) hi = t;
+    }
+    if (lo > hi) return 0;
+    *t0 = lo; *t1 = hi;
+    return 1;
+}
+
+static int cap_inside(const sweep_query* s, d3 p, double g) {
+    if (dot(s->n0, s->n0) > 0 && dot(sub(p, s->B0), s->n0) < -g) return 0;
+    if (dot(s->n1, s->n1) > 0 && dot(sub(s->B2, p), s->n1) < -g) return 0;
+    return 1;
+}
+
+/* distance from the part of [p, q] inside the caps grown by g to the piece;
+ * INFINITY when that part is empty */
+static double quad_clipped_dist(const sweep_query* s, d3 p, d3 q, double g, double hit_below, double miss_above) {
+    double t0, t1;
+    if (!cap_clip(s, p, q, g, &t0, &t1)) return INFINITY;
+    d3 d = sub(q, p);
+    return seg_quad_dist(add(p, mul(d, t0)), add(p, mul(d, t1)), s->B0, s->B1, s->B2, hit_below, miss_above);
+}
+
+static void visit_surface(sweep_query* s, d3 p, d3 q) {
+    const double r = s->r, e = s->eps;
+    int hit, rob_hit, rob_miss;
+    if (!s->quad) {
+        double dseg = sqrt(seg_seg2(p, q, s->a, s->b));
+        double dp = sqrt(pt_seg2(p, s->a, s->b));
+        hit = dseg <= r && dp > r;
+        rob_hit = dseg <= r - e && dp > r + e;
+        rob_miss = dseg > r + e || dp < r - e;
+    } else {
+        /* the grown cut first: most pairs are certain misses there */
+        double dg = quad_clipped_dist(s, p, q, e, r - e, r + e);
+        if (dg > r + e) return;  /* robust miss */
+        /* every value below is compared only with r - e, r and r + e: the
+         * branch and bound may stop once it is certainly below r - e or above
+         * r + e, and is exact (to 1e-12 m) in between */
+        double dp = seg_quad_dist(p, p, s->B0, s->B1, s->B2, r - e, r + e);
+        double d0 = quad_clipped_dist(s, p, q, 0.0, r - e, r + e);
+        double ds = quad_clipped_dist(s, p, q, -e, r - e, r + e);
+        int in0 = cap_inside(s, p, 0.0) && dp <= r;
+        int in_g = cap_inside(s, p, e) && dp <= r + e;
+        int in_s = cap_inside(s, p, -e) && dp <= r - e;
+        hit = d0 <= r && !in0;
+        rob_hit = ds <= r - e && !in_g;
+        rob_miss = dg > r + e || in_s;
+    }
+    if (hit) {
+        s->any_hit = 1;
+        s->hits++;
+        if (rob_hit) s->robust = 1; else s->marginal = 1;
+    } else if (!rob_miss) {
+        s->marginal = 1;
+    }
+}
+
 static int visit_edge(void* vctx, u32 e) {
     sweep_query* s = (sweep_query*) vctx;
     d3 p = fv(s->sv + s->se[e * 2] * 3), q = fv(s->sv + s->se[e * 2 + 1] * 3);
     ++s->prim_tests;
+    if (s->surface) {
+        visit_surface(s, p, q);
+        return 0;
+    }
     double d;
     if (!s->quad) d = sqrt(seg_seg2(p, q, s->a, s->b));
     else d = seg_quad_dist(p, q, s->B0, s->B1, s->B2, s->r - s->eps, s->r + s->eps);
@@ -931,7 +1222,7 @@ typedef struct {
     const orc_scene* S;
     const float* q;
     const u32* traj_off;
-    int quad, endpoints;
+    int quad, endpoints, surface;
     double eps;
     bvh_t scene_edge;
     unsigned char *traj_hit, *traj_band, *seg_hit, *seg_band, *traj_marg;
@@ -1021,6 +1312,7 @@ static void sweep_traj(void* vctx, int tr, void* scratch) {
                 sweep_query Q;
                 memset(&Q, 0, sizeof(Q));
                 Q.a = cen[g * ns + s]; Q.b = cen[(g + 1) * ns + s]; Q.r = R->sphere_radii[s]; Q.eps = C->eps;
+                Q.surface = C->surface;
                 Q.sv = C->S->verts; Q.se = C->S->edges;
                 double pad = Q.r + C->eps;
                 double qlo[3] = {fmin(Q.a.x, Q.b.x) - pad, fmin(Q.a.y, Q.b.y) - pad, fmin(Q.a.z, Q.b.z) - pad};
@@ -1051,16 +1343,18 @@ static void sweep_traj(void* vctx, int tr, void* scratch) {
                 for (int w = 0; w < nwp; ++w) acc = add(acc, mul(cen[w * ns + s], W[k * nwp + w]));
                 ctrl[k * ns + s] = acc;
             }
-        int npieces = nc - 2 + (C->endpoints ? 2 : 0);
+        int npieces = nc - 2 + (C->endpoints && !C->surface ? 2 : 0);
         for (int g = 0; g < npieces; ++g) {
             int srob = 0, smarg = 0, shit = 0;
             for (int s = 0; s < ns; ++s) {
                 sweep_query Q;
                 memset(&Q, 0, sizeof(Q));
                 Q.quad = 1; Q.r = R->sphere_radii[s]; Q.eps = C->eps; Q.sv = C->S->verts; Q.se = C->S->edges;
+                Q.surface = C->surface;
                 if (g < nc - 2) {
                     d3 P0 = ctrl[g * ns + s], P1 = ctrl[(g + 1) * ns + s], P2 = ctrl[(g + 2) * ns + s];
                     Q.B0 = mul(add(P0, P1), 0.5); Q.B1 = P1; Q.B2 = mul(add(P1, P2), 0.5);
+                    if (Q.surface) quad_caps(Q.B0, Q.B1, Q.B2, &Q.n0, &Q.n1);
                 } else {
                     d3 c = cen[(g == nc - 2 ? 0 : nwp - 1) * ns + s];
                     Q.B0 = c; Q.B1 = c; Q.B2 = c;
@@ -1092,14 +1386,19 @@ static void sweep_traj(void* vctx, int tr, void* scratch) {
 }
 
 /* quad = 0: piecewise-linear capsules, seg_off[t] = sum of (nwp - 1);
- * quad = 1: quadratic pieces, seg_off[t] = sum of (nc - 2 + 2 * endpoints). */
-int orc_sweep(int quad, int endpoints, const orc_robot* R, const orc_scene* S, const float* q, const u32* traj_off,
+ * quad = 1: quadratic pieces, seg_off[t] = sum of (nc - 2 + 2 * endpoints).
+ * surface = 0: solid semantics (an edge within r of the sphere path), S's
+ * edges the unique edges; surface = 1: the reference's entering-ray
+ * semantics (visit_surface), S's edges the directed loop edges, no end
+ * spheres. */
+int orc_sweep(int quad, int endpoints, int surface, const orc_robot* R, const orc_scene* S, const float* q, const u32* traj_off,
               int n_traj, double eps, int threads, unsigned char* traj_hit, unsigned char* traj_band,
               unsigned char* traj_marg, u32* traj_count, const u32* seg_off, unsigned char* seg_hit,
               unsigned char* seg_band, orc_work* work) {
     sweep_ctx C;
     memset(&C, 0, sizeof(C));
     C.R = R; C.S = S; C.q = q; C.traj_off = traj_off; C.quad = quad; C.endpoints = endpoints; C.eps = eps;
+    C.surface = surface;
     C.traj_hit = traj_hit; C.traj_band = traj_band; C.seg_hit = seg_hit; C.seg_band = seg_band; C.seg_off = seg_off;
     C.traj_marg = traj_marg; C.traj_count = traj_count;
     C.work = work;
@@ -1119,6 +1418,25 @@ int orc_seg_tri(const double* p, const double* q, const double* a, const double*
 double orc_seg_seg(const double* p1, const double* q1, const double* p2, const double* q2) {
     return sqrt(seg_seg2(v3(p1[0], p1[1], p1[2]), v3(q1[0], q1[1], q1[2]), v3(p2[0], p2[1], p2[2]), v3(q2[0], q2[1], q2[2])));
 }
+/* one (directed edge p -> q, primitive) pair under the surface semantics:
+ * quad = 0: capsule b0-b1; quad = 1: flat-capped piece (b0, b1, b2).
+ * *hit = the upstream decision, *band = 1 when it lies in the eps band. */
+void orc_surface_pair(int quad, const double* p, const double* q, const double* b0, const double* b1,
+                      const double* b2, double r, double eps, int* hit, int* band) {
+    sweep_query Q;
+    memset(&Q, 0, sizeof(Q));
+    Q.quad = quad; Q.surface = 1; Q.r = r; Q.eps = eps;
+    if (!quad) {
+        Q.a = v3(b0[0], b0[1], b0[2]); Q.b = v3(b1[0], b1[1], b1[2]);
+    } else {
+        Q.B0 = v3(b0[0], b0[1], b0[2]); Q.B1 = v3(b1[0], b1[1], b1[2]); Q.B2 = v3(b2[0], b2[1], b2[2]);
+        quad_caps(Q.B0, Q.B1, Q.B2, &Q.n0, &Q.n1);
+    }
+    visit_surface(&Q, v3(p[0], p[1], p[2]), v3(q[0], q[1], q[2]));
+    *hit = Q.any_hit;
+    *band = !Q.robust && Q.marginal;
+}
+
 double orc_seg_quad(const double* p, const double* q, const double* b0, const double* b1, const double* b2) {
     return seg_quad_dist(v3(p[0], p[1], p[2]), v3(q[0], q[1], q[2]), v3(b0[0], b0[1], b0[2]), v3(b1[0], b1[1], b1[2]),
                          v3(b2[0], b2[1], b2[2]), -INFINITY, INFINITY);

@@ -89,6 +89,16 @@ def unique_edges(tris):
     return out[:n].copy()
 
 
+def loop_edges(tris):
+    """Directed loop edges of a watertight mesh (upstream RTCD/Meshes/mesh.h:378-620), (m, 2) uint32."""
+    tris = _c(tris, np.uint32)
+    out = np.empty((max(1, 6 * len(tris)), 2), np.uint32)
+    n = lib().orc_loop_edges(_p(tris, U), C.c_int(len(tris)), _p(out, U))
+    if n < 0:
+        raise ValueError('mesh is not watertight: a triangle does not close a loop')
+    return out[:n].copy()
+
+
 class Scene:
     def __init__(self, mesh):
         self.verts = _c(mesh.verts, np.float32)
@@ -98,6 +108,15 @@ class Scene:
         self.edges = unique_edges(self.tris)
         self.s = OrcScene(len(self.verts), _p(self.verts, F), len(self.tris), _p(self.tris, U), len(self.edges),
                           _p(self.edges, U))
+        self._loop = None
+
+    def loop(self):
+        """The scene with its directed loop edges in place of the unique edges (surface semantics)."""
+        if self._loop is None:
+            self.loop_edges = loop_edges(self.tris)
+            self._loop = OrcScene(len(self.verts), _p(self.verts, F), len(self.tris), _p(self.tris, U),
+                                  len(self.loop_edges), _p(self.loop_edges, U))
+        return self._loop
 
 
 def fk(model, q):
@@ -203,11 +222,17 @@ def sweep_seg_offsets(traj_off, quad, endpoints=True):
     return off
 
 
-def sweep(quad, robot, scene, q, traj_off, eps=1e-5, threads=None, endpoints=True, work=False):
-    """Returns dict(traj_hit, traj_band, seg_hit, seg_band, seg_off[, node_tests, prim_tests])."""
+def sweep(quad, robot, scene, q, traj_off, eps=1e-5, threads=None, endpoints=True, work=False, surface=False):
+    """Returns dict(traj_hit, traj_band, seg_hit, seg_band, seg_off[, node_tests, prim_tests]).
+
+    surface=False: solid semantics over the unique edges; surface=True: the
+    reference's entering-ray semantics over the directed loop edges, no end
+    spheres (endpoints is ignored)."""
     q = _c(q, np.float32)
     traj_off = _c(traj_off, np.uint32)
     nt = len(traj_off) - 1
+    if surface:
+        endpoints = False
     seg_off = sweep_seg_offsets(traj_off, quad, endpoints)
     th = np.zeros(nt, np.uint8)
     tb = np.zeros(nt, np.uint8)
@@ -216,7 +241,9 @@ def sweep(quad, robot, scene, q, traj_off, eps=1e-5, threads=None, endpoints=Tru
     sh = np.zeros(max(1, int(seg_off[-1])), np.uint8)
     sb = np.zeros(max(1, int(seg_off[-1])), np.uint8)
     w = (OrcWork * nt)() if work else None
-    lib().orc_sweep(C.c_int(int(quad)), C.c_int(int(endpoints)), C.byref(robot.s), C.byref(scene.s), _p(q, F),
+    sc = scene.loop() if surface else scene.s
+    lib().orc_sweep(C.c_int(int(quad)), C.c_int(int(endpoints)), C.c_int(int(surface)), C.byref(robot.s), C.byref(sc),
+                    _p(q, F),
                     _p(traj_off, U), C.c_int(nt), D(eps), C.c_int(threads or threads_default()), _p(th, B), _p(tb, B),
                     _p(tm, B), _p(tc, U), _p(seg_off, U), _p(sh, B), _p(sb, B), w)
     out = {'traj_hit': th, 'traj_band': tb, 'traj_marg': tm, 'traj_count': tc, 'seg_hit': sh[:seg_off[-1]],
@@ -253,3 +280,12 @@ def seg_quad(p, q, b0, b1, b2):
     lib().orc_seg_quad.restype = C.c_double
     arr = [_c(x, np.float64) for x in (p, q, b0, b1, b2)]
     return lib().orc_seg_quad(*[_p(x, D) for x in arr])
+
+
+def surface_pair(quad, p, q, b0, b1, b2, r, eps=1e-5):
+    """One (directed edge p -> q, primitive) pair under the reference's
+    entering-ray semantics: (hit, band)."""
+    arr = [_c(x, np.float64) for x in (p, q, b0, b1, b2)]
+    hit, band = C.c_int(), C.c_int()
+    lib().orc_surface_pair(C.c_int(int(quad)), *[_p(x, D) for x in arr], D(r), D(eps), C.byref(hit), C.byref(band))
+    return bool(hit.value), bool(band.value)

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -184,6 +185,141 @@ static void fit_obb(const float* pts, const std::vector<uint32_t>& idx, float pa
     out[15] = std::sqrt(fh[0] * fh[0] + fh[1] * fh[1] + fh[2] * fh[2]);
 }
 
+// Directed loop edges (RTCD/Meshes/mesh.h:378-620): every triangle's three
+// edges, in the directions kept, run around it as a loop; an edge two
+// neighbours need in opposite directions is kept in both.  The sweep
+// detectors cast these under the entering-ray semantics (a closed triangle
+// boundary that crosses the swept surface crosses it inwards somewhere along
+// its loop).  The directions follow the upstream breadth-first walk: from the
+// first unprocessed triangle, pop a triangle, complete its loop from the
+// directions already chosen (see complete_loop), queue its unprocessed
+// neighbours (per edge in increasing triangle index).  Output: triangles in
+// index order, each triangle's edges in order, forward before reverse, each
+// directed edge once.  Fails when a triangle does not end up a loop (the
+// upstream throws: the mesh is not watertight).
+namespace {
+enum class Dir : uint8_t { none, fwd, bwd, both };
+
+struct LoopBuilder {
+    std::unordered_set<uint64_t> chosen;  // directed edges a -> b
+    static uint64_t key(uint32_t a, uint32_t b) { return ((uint64_t) a << 32) | b; }
+    bool has(uint32_t a, uint32_t b) const { return chosen.count(key(a, b)) != 0; }
+    void add(uint32_t a, uint32_t b) { chosen.insert(key(a, b)); }
+    Dir dir(uint32_t a, uint32_t b) const {
+        const bool f = has(a, b), r = has(b, a);
+        return f && r ? Dir::both : f ? Dir::fwd : r ? Dir::bwd : Dir::none;
+    }
+    // Adds directions so the triangle (v[0] v[1] v[2]) becomes a loop, by the
+    // upstream rules for 3, 2, 1 and 0 edges already directed.
+    void complete_loop(const uint32_t v[4]) {
+        Dir d[3];
+        int fwd = 0, bwd = 0, set = 0;
+        for (int i = 0; i < 3; ++i) {
+            d[i] = dir(v[i], v[i + 1]);
+            fwd += d[i] == Dir::fwd || d[i] == Dir::both;
+            bwd += d[i] == Dir::bwd || d[i] == Dir::both;
+            set += d[i] != Dir::none;
+        }
+        auto orient = [&](int i, Dir w) {  // edge i in direction w
+            if (w == Dir::fwd) add(v[i], v[i + 1]); else add(v[i + 1], v[i]);
+        };
+        auto first = [&](auto pred) {
+            for (int i = 0; i < 3; ++i)
+                if (pred(d[i])) return i;
+            return -1;
+        };
+        const auto one_way = [](Dir x) { return x == Dir::fwd || x == Dir::bwd; };
+        if (set == 3) {
+            if (fwd == 3 || bwd == 3) return;
+            // the rule breaker gets its other direction too
+            const int i = fwd == bwd ? first([](Dir x) { return x != Dir::both; })
+                          : fwd < bwd ? first([](Dir x) { return x == Dir::fwd; })
+                                      : first([](Dir x) { return x == Dir::bwd; });
+            if (i >= 0) orient(i, d[i] == Dir::fwd ? Dir::bwd : Dir::fwd);
+        } else if (set == 2) {
+            const int open = first([](Dir x) { return x == Dir::none; });
+            Dir w = Dir::fwd;  // both decided edges two-way: forward (the upstream leaves this unset)
+            const int i = first(one_way);
+            if (fwd != 2 && bwd != 2) {  // one forward, one backward: double the first, follow the other
+                orient(i, d[i] == Dir::fwd ? Dir::bwd : Dir::fwd);
+                w = d[i] == Dir::fwd ? Dir::bwd : Dir::fwd;
+            } else if (i >= 0) {
+                w = d[i];
+            }
+            orient(open, w);
+        } else if (set == 1) {
+            const int i = first([](Dir x) { return x != Dir::none; });
+            const Dir w = d[i] == Dir::fwd ? Dir::fwd : Dir::bwd;  // two-way counts as backward, as upstream
+            for (int k = 0; k < 3; ++k)
+                if (d[k] == Dir::none) orient(k, w);
+        } else {
+            for (int k = 0; k < 3; ++k) orient(k, Dir::fwd);
+        }
+    }
+};
+}  // namespace
+
+std::vector<uint32_t> loop_edges(const uint32_t* tris, size_t n_tris) {
+    std::vector<uint32_t> out;
+    if (!n_tris) return out;
+    // triangles around each undirected edge, ascending
+    std::vector<std::pair<uint64_t, uint32_t>> adj;
+    adj.reserve(3 * n_tris);
+    for (size_t t = 0; t < n_tris; ++t)
+        for (int k = 0; k < 3; ++k) {
+            const uint32_t a = tris[3 * t + k], b = tris[3 * t + (k + 1) % 3];
+            adj.emplace_back(LoopBuilder::key(std::min(a, b), std::max(a, b)), (uint32_t) t);
+        }
+    std::sort(adj.begin(), adj.end());
+    adj.erase(std::unique(adj.begin(), adj.end()), adj.end());
+    LoopBuilder L;
+    L.chosen.reserve(4 * n_tris);
+    std::vector<uint8_t> done(n_tris, 0);
+    std::deque<uint32_t> open;
+    size_t start = 0;
+    while (true) {
+        while (start < n_tris && done[start]) ++start;
+        if (start == n_tris) break;
+        open.push_back((uint32_t) start);
+        while (!open.empty()) {
+            const uint32_t cur = open.front();
+            open.pop_front();
+            if (done[cur]) continue;
+            const uint32_t v[4] = {tris[3ull * cur], tris[3ull * cur + 1], tris[3ull * cur + 2], tris[3ull * cur]};
+            L.complete_loop(v);
+            done[cur] = 1;
+            for (int i = 0; i < 3; ++i) {
+                const uint64_t k = LoopBuilder::key(std::min(v[i], v[i + 1]), std::max(v[i], v[i + 1]));
+                auto it = std::lower_bound(adj.begin(), adj.end(), std::make_pair(k, 0u));
+                for (; it != adj.end() && it->first == k; ++it)
+                    if (it->second != cur && !done[it->second]) open.push_back(it->second);
+            }
+        }
+    }
+    out.reserve(2 * L.chosen.size());
+    for (size_t t = 0; t < n_tris; ++t) {
+        const uint32_t v[4] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2], tris[3 * t]};
+        int fwd = 0, bwd = 0;
+        for (int i = 0; i < 3; ++i) {
+            fwd += L.has(v[i], v[i + 1]);
+            bwd += L.has(v[i + 1], v[i]);
+        }
+        if (fwd != 3 && bwd != 3) fail(RTCD_ERR_INVALID_ARGUMENT, "loop edges: a triangle does not close a loop");
+    }
+    for (size_t t = 0; t < n_tris; ++t) {
+        const uint32_t v[4] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2], tris[3 * t]};
+        for (int i = 0; i < 3; ++i)
+            for (int rev = 0; rev < 2; ++rev) {
+                const uint32_t a = rev ? v[i + 1] : v[i], b = rev ? v[i] : v[i + 1];
+                if (L.chosen.erase(LoopBuilder::key(a, b))) {
+                    out.push_back(a);
+                    out.push_back(b);
+                }
+            }
+    }
+    return out;
+}
+
 // Device LBVH over triangles or edges, concatenated over several groups
 // (links); returns per-group roots.
 struct GroupedBvh {
@@ -261,6 +397,13 @@ struct rtcd_scene {
     DevBuf verts, tris, edges, obbs, tri_obs, obs_box, obs_point;
     DevBuf tri_wide, edge_wide, tri_cut, edge_cut;  // 4-wide copies of the two scene trees and their top cuts
     uint32_t n_tris = 0, n_edges = 0, n_obs = 0;
+    // the directed loop edges and their trees, built on the first surface-semantics sweep
+    std::mutex loop_mu;
+    bool loop_built = false;
+    SceneDev dev_loop{};  // dev with the edge fields pointing at the loop-edge trees
+    GroupedBvh loop;
+    DevBuf loop_edges, loop_wide, loop_cut;
+    uint32_t n_loop = 0;
 };
 
 struct rtcd_detector {
@@ -662,6 +805,18 @@ rtcd_status rtcd_scene_info(const rtcd_scene* sc, uint32_t* n_tris, uint32_t* n_
     });
 }
 
+rtcd_status rtcd_loop_edges(const uint32_t* tris, uint32_t n_tris, uint32_t* edges_out, uint32_t max_edges,
+                            uint32_t* n_edges) {
+    return guarded([&] {
+        RTCD_REQUIRE(n_edges && (n_tris == 0 || tris), "NULL argument");
+        const std::vector<uint32_t> e = loop_edges(tris, n_tris);
+        *n_edges = (uint32_t) (e.size() / 2);
+        if (!edges_out) return;
+        RTCD_REQUIRE(e.size() / 2 <= max_edges, "edges_out too small");
+        std::copy(e.begin(), e.end(), edges_out);
+    });
+}
+
 rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_robot* robot, rtcd_scene* scene,
                                  const rtcd_config* config, rtcd_detector** out) {
     return guarded([&] {
@@ -742,9 +897,47 @@ namespace {
 
 uint32_t quad_ctrl_count(uint32_t n_wp) { return std::max<uint32_t>(3, (n_wp + 1) / 2); }
 
+// The scene as the surface-semantics sweeps see it: the edge trees replaced
+// by trees over the directed loop edges, built on first use (the triangles
+// are read back from the device, the loop edges computed on the host, both
+// trees built on the scene's context stream; synchronous, once per scene).
+const SceneDev& scene_loop(rtcd_scene* sc) {
+    std::lock_guard<std::mutex> lk(sc->loop_mu);
+    if (sc->loop_built) return sc->dev_loop;
+    cudaStream_t s = sc->ctx->stream;
+    std::vector<uint32_t> tris(3ull * sc->n_tris);
+    if (sc->n_tris)
+        cuda_check(cudaMemcpyAsync(tris.data(), sc->tris.p, 4ull * tris.size(), cudaMemcpyDeviceToHost, s), "tris");
+    cuda_check(cudaStreamSynchronize(s), "tris");
+    const std::vector<uint32_t> e = loop_edges(tris.data(), sc->n_tris);
+    sc->n_loop = (uint32_t) (e.size() / 2);
+    upload(sc->loop_edges, e.data(), e.size(), s);
+    const std::vector<uint32_t> v0 = {0, 0}, off = {0, sc->n_loop};
+    build_grouped(false, sc->verts.as<float>(), v0, sc->loop_edges.as<uint32_t>(), off, sc->ctx->err.as<uint32_t>(), s,
+                  sc->loop);
+    const WideResult w =
+        build_wide(sc->loop.nodes.as<float4>(), sc->n_loop > 1 ? sc->n_loop - 1 : 0, sc->loop.roots[0], sc->loop_wide, s);
+    upload(sc->loop_cut, w.cut.data(), w.cut.size(), s);
+    SceneDev dv = sc->dev;
+    dv.edge_nodes = sc->loop.nodes.as<float4>();
+    dv.edge_prims = sc->loop.prims.as<float4>();
+    dv.edge_root = sc->loop.roots[0];
+    dv.n_edges = sc->n_loop;
+    dv.edge_wide = sc->loop_wide.as<float4>();
+    dv.edge_wide_root = w.root;
+    dv.edge_cut = sc->loop_cut.as<float4>();
+    dv.n_edge_cut = (uint32_t) w.cut.size() / 2;
+    dv.edge_wide_lane = (kWide - 1) * w.depth + kWide <= (uint32_t) kStack ? 1u : 0u;
+    dv.wide_front = std::max(dv.wide_front, wide_frontier(w.depth));
+    cuda_check(cudaStreamSynchronize(s), "loop-edge trees");
+    sc->dev_loop = dv;
+    sc->loop_built = true;
+    return sc->dev_loop;
+}
+
 uint32_t pieces_of(rtcd_detector_kind kind, uint32_t n_wp, uint32_t flags) {
     if (kind == RTCD_LINEAR_SWEEP) return n_wp > 0 ? n_wp - 1 : 0;
-    return quad_ctrl_count(n_wp) - 2 + ((flags & RTCD_CHECK_NO_ENDPOINTS) ? 0 : 2);
+    return quad_ctrl_count(n_wp) - 2 + ((flags & (RTCD_CHECK_NO_ENDPOINTS | RTCD_CHECK_SURFACE)) ? 0 : 2);
 }
 
 // Least-squares quadratic B-spline fit W = (B^T B)^{-1} B^T (nc x nt), with B
@@ -1170,7 +1363,8 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.n_spheres = ns;
     A.total_units = (uint32_t) (pieces * ns);
     A.quad = quad;
-    A.endpoints = !(flags & RTCD_CHECK_NO_ENDPOINTS);
+    A.endpoints = !(flags & (RTCD_CHECK_NO_ENDPOINTS | RTCD_CHECK_SURFACE));
+    A.surface = (flags & RTCD_CHECK_SURFACE) != 0;
     A.traj_hit = d->pose_hit.as<uint32_t>();
     A.piece_hit = want_pieces ? d->piece_hit.as<uint32_t>() : nullptr;
     A.counts = d_counts;
@@ -1198,7 +1392,8 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     }
     A.binary_tree = d->cfg.stage_b_form == 1 ? 1 : 0;
     if (A.total_units)
-        launch_sweep(d->scene->dev, A, d->blocks, d->threads, d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
+        launch_sweep(A.surface ? scene_loop(d->scene) : d->scene->dev, A, d->blocks, d->threads,
+                     d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     // outputs
     uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
@@ -1620,6 +1815,29 @@ rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_
         ScanScratch sc;
         select_u8(mask_dev, n, idx_dev, count_dev, sc, ctx->err.as<uint32_t>(), s);
         cuda_check(cudaStreamSynchronize(s), "select");
+    });
+}
+
+rtcd_status rtcd_selftest_lookback_timeout(rtcd_ctx* ctx, uint32_t n, uint32_t spin_limit) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx, "NULL context");
+        RTCD_REQUIRE(n >= 1 && n <= (1u << 20), "n must be 1 to 1048576");
+        RTCD_REQUIRE(spin_limit >= 1 && spin_limit <= (1u << 16), "spin_limit must be 1 to 65536");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = ctx->stream;
+        DevBuf mask, words;
+        mask.ensure(n);
+        words.ensure(16);  // [0] output index, [1] count, [2] error word
+        cuda_check(cudaMemsetAsync(mask.p, 0, n, s), "memset");
+        cuda_check(cudaMemsetAsync(words.p, 0, 16, s), "memset");
+        ScanScratch sc;
+        uint32_t* w = words.as<uint32_t>();
+        lookback_timeout_probe(mask.as<uint8_t>(), n, spin_limit, w, w + 1, sc, w + 2, s);
+        uint32_t e = 0;
+        cuda_check(cudaMemcpyAsync(&e, w + 2, 4, cudaMemcpyDeviceToHost, s), "error word read");
+        cuda_check(cudaStreamSynchronize(s), "selftest");
+        if (e & kErrLookback) fail(RTCD_ERR_DEVICE_TIMEOUT, "look-back wait ran out (expected by this self-test)");
+        fail(RTCD_ERR_INTERNAL, "the look-back waits did not run out");
     });
 }
 

@@ -73,6 +73,11 @@ void select_u8_raw(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t*
                    unsigned long long* d_status, uint32_t* d_counter, uint32_t* d_err, cudaStream_t s);
 constexpr uint32_t kSelectTileFlags = 2048;  // flags per look-back tile of the compaction kernel
 
+// Self-test of the bounded look-back wait: a compaction whose tile 0 never
+// publishes, so every wait runs out after spin_limit polls (lbvh.cu).
+void lookback_timeout_probe(const uint8_t* d_mask, uint32_t n, uint32_t spin_limit, uint32_t* d_out,
+                            uint32_t* d_count, ScanScratch& sc, uint32_t* d_err, cudaStream_t s);
+
 // A packed LBVH over one primitive set.
 struct LbvhResult {
     uint32_t root = kNone;  // child reference of the root

@@ -148,6 +148,7 @@ struct SweepArgs {
     uint32_t total_units;      // pieces * spheres
     int quad;
     int endpoints;
+    int surface;               // entering-ray semantics over the loop edges (leaf_hit_surface)
     uint32_t* traj_hit;        // [n_traj]
     uint32_t* piece_hit;       // [pieces] or NULL
     uint32_t* counts;          // [n_traj] or NULL

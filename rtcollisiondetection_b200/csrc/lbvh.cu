@@ -30,7 +30,7 @@ void scan_u32(const uint32_t* d_in, uint32_t* d_out, uint32_t n, uint32_t* d_tot
               cudaStream_t s) {
     sc.prepare(n, s);
     uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
-    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err};
+    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err, kLookbackSpinLimit};
     k_scan_u32<<<tiles, kScanThreads, 0, s>>>(d_in, d_out, n, st, d_total);
     cuda_check(cudaGetLastError(), "k_scan_u32");
 }
@@ -39,7 +39,7 @@ void select_u8(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_c
                cudaStream_t s) {
     sc.prepare(n, s);
     uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
-    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err};
+    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err, kLookbackSpinLimit};
     k_select_u8<<<tiles, kScanThreads, 0, s>>>(d_mask, n, d_out, d_count, st);
     cuda_check(cudaGetLastError(), "k_select_u8");
 }
@@ -47,9 +47,28 @@ void select_u8(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_c
 void select_u8_raw(const uint8_t* d_mask, uint32_t n, uint32_t* d_out, uint32_t* d_count,
                    unsigned long long* d_status, uint32_t* d_counter, uint32_t* d_err, cudaStream_t s) {
     uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
-    ScanState st{d_status, d_counter, d_err};
+    ScanState st{d_status, d_counter, d_err, kLookbackSpinLimit};
     k_select_u8<<<tiles, kScanThreads, 0, s>>>(d_mask, n, d_out, d_count, st);
     cuda_check(cudaGetLastError(), "k_select_u8");
+}
+
+// The compaction of n zero flags with tile 0's look-back word never
+// published: the tile counter starts at 1, so no block takes tile 0 and every
+// tile's look-back waits on a word nothing writes.  Each wait gives up after
+// spin_limit polls and sets kErrLookback in *d_err; the tiles then publish
+// and return.  Every access stays in bounds: tiles 1..T (T = tiles of n) use
+// status words 1..T of the T + 1 zeroed here, read no flags past n and write
+// no indices (no flag is set).  d_mask: n zero bytes; d_out, d_count: one
+// word each; *d_err zeroed by the caller.
+void lookback_timeout_probe(const uint8_t* d_mask, uint32_t n, uint32_t spin_limit, uint32_t* d_out,
+                            uint32_t* d_count, ScanScratch& sc, uint32_t* d_err, cudaStream_t s) {
+    const uint32_t tiles = std::max<uint32_t>(1, scan_tiles(n));
+    sc.prepare((tiles + 1) * (uint32_t) kScanTile, s);  // tiles + 1 zeroed words, counter 0
+    static const uint32_t one = 1;
+    cuda_check(cudaMemcpyAsync(sc.counter.p, &one, sizeof(one), cudaMemcpyHostToDevice, s), "counter seed");
+    ScanState st{sc.status.as<unsigned long long>(), sc.counter.as<uint32_t>(), d_err, spin_limit};
+    k_select_u8<<<tiles, kScanThreads, 0, s>>>(d_mask, n, d_out, d_count, st);
+    cuda_check(cudaGetLastError(), "k_select_u8 (timeout probe)");
 }
 
 // ---------------------------------------------------------------- prim boxes

@@ -19,14 +19,12 @@ namespace {
 
 constexpr uint32_t kMaxTiles = 16384;                               // look-back words
 constexpr uint64_t kMaxFlags = (uint64_t) kMaxTiles * rtcd::kSelectTileFlags;  // 33,554,432
-constexpr int kMaxDevices = 64;
 
 // [0, kMaxTiles): look-back status words; [kMaxTiles]: tile counter (low
 // half); [kMaxTiles + 1]: device error word (low half).
 static __device__ __align__(256) unsigned long long g_select_scratch[kMaxTiles + 2];
 
-std::mutex g_mu;                                      // serialises calls of this process
-unsigned long long* g_scratch_addr[kMaxDevices] = {};  // device address of the array, per device
+std::mutex g_mu;  // serialises calls of this process
 
 }  // namespace
 
@@ -38,19 +36,17 @@ extern "C" RTCD_API rtcd_status rtcd_select_flags_u8_noalloc(const uint8_t* mask
         if ((uint64_t) n > kMaxFlags)
             rtcd::fail(RTCD_ERR_CAPACITY, "rtcd_select_flags_u8_noalloc: n = " + std::to_string(n) +
                                               " exceeds the static scratch limit of 33554432 flags");
-        int dev = 0;
-        rtcd::cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
-        if (dev < 0 || dev >= kMaxDevices) rtcd::fail(RTCD_ERR_CAPACITY, "device index beyond 63");
         cudaStream_t s = (cudaStream_t) stream;
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_addr[dev]) {
-            // first call on this device (with the device current): the host-side
-            // name of the array is not a device address; ask the runtime for it
-            void* p = nullptr;
-            rtcd::cuda_check(cudaGetSymbolAddress(&p, g_select_scratch), "cudaGetSymbolAddress");
-            g_scratch_addr[dev] = static_cast<unsigned long long*>(p);
-        }
-        unsigned long long* base = g_scratch_addr[dev];
+        // The host-side name of the array is not a device address: ask the
+        // runtime for the address on the calling (current) device.  The lookup
+        // is repeated on every call rather than cached, so a context that was
+        // torn down and re-created (cudaDeviceReset) never leaves a stale
+        // address behind; on a device's first call it may also load this
+        // library's device code there.
+        void* p = nullptr;
+        rtcd::cuda_check(cudaGetSymbolAddress(&p, g_select_scratch), "cudaGetSymbolAddress");
+        unsigned long long* base = static_cast<unsigned long long*>(p);
         uint32_t tiles = n ? (uint32_t) ((n + rtcd::kSelectTileFlags - 1) / rtcd::kSelectTileFlags) : 1u;
         // the previous call left its words behind: clear the ones this call uses
         rtcd::cuda_check(cudaMemsetAsync(base, 0, sizeof(unsigned long long) * tiles, s), "scratch clear");

@@ -24,6 +24,7 @@ struct ScanState {
     unsigned long long* status;  // one word per tile: flag << 32 | value; zeroed before launch
     uint32_t* tile_counter;      // zeroed before launch
     uint32_t* error;             // device error word
+    uint32_t spin_limit;         // polls of a predecessor's word before the wait gives up (kLookbackSpinLimit)
 };
 
 __device__ __forceinline__ unsigned long long scan_pack(uint32_t flag, uint32_t v) {
@@ -80,7 +81,7 @@ __device__ __forceinline__ uint32_t tile_lookback(const ScanState& st, uint32_t 
         unsigned long long s = idx >= 0 ? status[idx] : scan_pack(2, 0);
         uint32_t flag = (uint32_t) (s >> 32);
         if (__any_sync(0xffffffffu, flag == 0)) {
-            if (++spins > kLookbackSpinLimit) {
+            if (++spins > st.spin_limit) {
                 if (lane == 0) atomicOr(st.error, kErrLookback);
                 break;
             }

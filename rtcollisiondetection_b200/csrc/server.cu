@@ -136,7 +136,8 @@ rtcd_status run_launch(rtcd_server* S, Slot& slot, rtcd_detector* det, int kind,
     const bool counts = (flags & RTCD_CHECK_COUNTS) != 0;
     rtcd_status st = rtcd_check(c, q.data(), sweep ? off.data() : nullptr, n, out_flags.data(),
                                 sweep ? out_seg.data() : nullptr, counts ? out_counts.data() : nullptr,
-                                (flags & (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS)) | RTCD_CHECK_HOST_BUFFERS,
+                                (flags & (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS | RTCD_CHECK_SURFACE)) |
+                                    RTCD_CHECK_HOST_BUFFERS,
                                 nullptr);
     if (st != RTCD_OK) {
         char buf[512];
@@ -367,8 +368,9 @@ rtcd_status rtcd_server_submit(rtcd_server* S, rtcd_detector* det, const float* 
                                uint32_t n, uint32_t flags, uint64_t* ticket) {
     return guard([&] {
         if (!S || !det || !ticket || (n && !q)) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "NULL argument");
-        if (flags & ~(uint32_t) (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS))
-            rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "server requests accept RTCD_CHECK_COUNTS and RTCD_CHECK_NO_ENDPOINTS");
+        if (flags & ~(uint32_t) (RTCD_CHECK_COUNTS | RTCD_CHECK_NO_ENDPOINTS | RTCD_CHECK_SURFACE))
+            rtcd::fail(RTCD_ERR_INVALID_ARGUMENT,
+                       "server requests accept RTCD_CHECK_COUNTS, RTCD_CHECK_NO_ENDPOINTS and RTCD_CHECK_SURFACE");
         rtcd_ctx* c;
         int kind;
         rtcd_robot* rb;
@@ -412,18 +414,26 @@ rtcd_status rtcd_server_wait(rtcd_server* S, uint64_t ticket, int32_t timeout_ms
     return guard([&] {
         if (!S) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "NULL server");
         std::unique_lock<std::mutex> lk(S->mu);
-        auto it = S->requests.find(ticket);
-        if (it == S->requests.end()) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "unknown ticket");
-        Request* r = it->second.get();
-        auto ready = [&] { return r->done; };
+        if (S->requests.find(ticket) == S->requests.end()) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "unknown ticket");
+        // the ticket is looked up afresh after every wake-up: another thread
+        // waiting on the same ticket may have collected and released it
+        auto ready = [&] {
+            auto j = S->requests.find(ticket);
+            return j == S->requests.end() || j->second->done;
+        };
         if (timeout_ms < 0)
             S->cv_done.wait(lk, ready);
         else if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
             rtcd::fail(RTCD_ERR_DEVICE_TIMEOUT, "request not finished yet");
+        auto it = S->requests.find(ticket);
+        if (it == S->requests.end())
+            rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "unknown ticket (collected by another waiter)");
+        Request* r = it->second.get();
         if (r->status != RTCD_OK) {
             std::string m = r->error;
             int st = r->status;
             S->requests.erase(it);
+            S->cv_done.notify_all();  // other waiters on this ticket learn it is gone
             rtcd::fail(st, m);
         }
         if (flags_out) std::memcpy(flags_out, r->out_flags.data(), r->out_flags.size());
@@ -432,6 +442,7 @@ rtcd_status rtcd_server_wait(rtcd_server* S, uint64_t ticket, int32_t timeout_ms
             std::memcpy(counts_out, r->out_counts.data(), 4 * r->out_counts.size());
         if (latency_ms) *latency_ms = r->latency_ms;
         S->requests.erase(it);
+        S->cv_done.notify_all();
     });
 }
 

@@ -381,65 +381,186 @@ __device__ __forceinline__ bool cull_box(const SweepCull& c, const Box& b, float
     return in;
 }
 
+constexpr float kSweepBand = 2e-6f;  // |d - r| below this (+ 1e-6 r) is re-tested in FP64
+
+// FP32 distance from the segment pq to the unit's Bezier piece, bracketed.
+// C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
+// within e of the chord B0-B2 and back, so the chord distance +- e brackets
+// the exact distance; only the undecided middle needs roots.  certain_miss is
+// set when the value returned (then a lower bound) exceeds r + tol; a value
+// below r - tol is an upper bound (a certain hit); otherwise it is the root-
+// found distance.
+__device__ __forceinline__ float quad_dist_bracket(V3<float> p, V3<float> q, const SweepUnit& U, float r, float tol,
+                                                   bool& certain_miss, unsigned long long& n_roots) {
+    const V3<float> b0 = v3cast<float>(U.P0), b1 = v3cast<float>(U.P1), b2 = v3cast<float>(U.P2);
+    const V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
+    const float e = 0.5f * sqrtf(vdot(dv, dv));
+    const float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
+    if (dc - e > r + tol) {
+        certain_miss = true;
+        return dc - e;
+    }
+    if (dc + e < r - tol) return dc + e;
+    // halve the piece twice more (de Casteljau: the chord deviation of a
+    // half is a quarter), bracketing with the polyline through C(k/4)
+    const float e2 = 0.0625f * e;  // deviation of a quarter piece from its chord
+    float lo = 3.0e38f;
+    V3<float> prev = b0;
+    for (int k = 1; k <= 4; ++k) {
+        const float u = 0.25f * (float) k;
+        const V3<float> cu =
+            vadd(vadd(vscale(b0, (1.f - u) * (1.f - u)), vscale(b1, 2.f * u * (1.f - u))), vscale(b2, u * u));
+        lo = fminf(lo, seg_seg2<float>(p, q, prev, cu));
+        prev = cu;
+    }
+    const float dq = sqrtf(fmaxf(lo, 0.f));
+    if (dq - e2 > r + tol) {
+        certain_miss = true;
+        return dq - e2;
+    }
+    if (dq + e2 < r - tol) return dq + e2;
+    ++n_roots;
+    return seg_quad_dist_f32(make_float4(p.x, p.y, p.z, 0.f), make_float4(q.x, q.y, q.z, 0.f), U.P0, U.P1, U.P2);
+}
+
 // The exact leaf test: does obstacle edge `leaf` come within r of the unit's
 // path?  FP32 with brackets; FP64 inside a narrow band around r.
 template <bool QUAD>
 __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ ep, uint32_t leaf, const SweepUnit& U,
                                          unsigned long long* stats, unsigned long long& n_roots) {
-    constexpr float kBand = 2e-6f;  // |d - r| below this is re-tested in FP64
     const float4* e = ep + 2ull * leaf;
     const float4 ea = __ldg(e), eb = __ldg(e + 1);
     const V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
     const float r = U.r;
     float dist;
     bool decided = false;
-    if (!QUAD) {
+    if (!QUAD)
         dist = sqrtf(fmaxf(seg_seg2<float>(p, q, v3cast<float>(U.P0), v3cast<float>(U.P1)), 0.f));
-    } else {
-        // C(u) - chord(u) = 2u(1-u)(B1 - (B0+B2)/2): every point of the piece is
-        // within e of the chord B0-B2 and back, so the chord distance +- e
-        // brackets the exact distance; only the undecided middle needs roots
-        const V3<float> b0 = v3cast<float>(U.P0), b1 = v3cast<float>(U.P1), b2 = v3cast<float>(U.P2);
-        const V3<float> dv = vsub(b1, vscale(vadd(b0, b2), 0.5f));
-        const float e = 0.5f * sqrtf(vdot(dv, dv));
-        const float dc = sqrtf(fmaxf(seg_seg2<float>(p, q, b0, b2), 0.f));
-        const float tol = kBand + 1e-6f * r;
-        if (dc - e > r + tol) {  // certain miss
-            dist = dc - e;
-            decided = true;
-        } else if (dc + e < r - tol) {  // certain hit
-            dist = dc + e;
-        } else {
-            // halve the piece twice more (de Casteljau: the chord deviation of a
-            // half is a quarter), bracketing with the polyline through C(k/4)
-            const float e2 = 0.0625f * e;  // deviation of a quarter piece from its chord
-            float lo = 3.0e38f;
-            V3<float> prev = b0;
-            for (int k = 1; k <= 4; ++k) {
-                const float u = 0.25f * (float) k;
-                const V3<float> cu = vadd(vadd(vscale(b0, (1.f - u) * (1.f - u)), vscale(b1, 2.f * u * (1.f - u))),
-                                          vscale(b2, u * u));
-                lo = fminf(lo, seg_seg2<float>(p, q, prev, cu));
-                prev = cu;
-            }
-            const float dq = sqrtf(fmaxf(lo, 0.f));
-            if (dq - e2 > r + tol) {
-                dist = dq - e2;
-                decided = true;
-            } else if (dq + e2 < r - tol) {
-                dist = dq + e2;
-            } else {
-                ++n_roots;
-                dist = seg_quad_dist_f32(ea, eb, U.P0, U.P1, U.P2);
-            }
-        }
-    }
+    else
+        dist = quad_dist_bracket(p, q, U, r, kSweepBand + 1e-6f * r, decided, n_roots);
     bool hit = dist <= r;
-    if (!decided && fabsf(dist - r) <= kBand + 1e-6f * r) {
+    if (!decided && fabsf(dist - r) <= kSweepBand + 1e-6f * r) {
         atomicAdd(stats, 1ull);
         hit = sweep_retest_f64<QUAD>(ea, eb, U.P0, U.P1, U.P2, r);
     }
     return hit;
+}
+
+// ---- the reference's entering-ray semantics (RTCD_CHECK_SURFACE).
+// The upstream casts each directed loop edge p -> q (RTCD/Meshes/mesh.h:
+// 378-620) as a ray with tmin 0, tmax |q - p| (RTCD/CollisionDetector/
+// CCCuda.cu:56-77) against OptiX's curve intersectors, which report a ray
+// entering a curve primitive, not one starting inside it; the any-hit
+// program counts every report (CCCuda.cu:37-41).  Per (edge, unit):
+//     hit  <=>  p lies outside the unit's closed solid P  and  [p, q] meets P.
+// Linear: P is the round-capped capsule (endcapFlags = 1, RTCD/Robot/
+// batchCurveRobot.h:230).  Quadratic: the sphere-swept piece cut by flat
+// caps, the planes through B0 and B2 normal to the end tangents B1 - B0 and
+// B2 - B1 (B2 - B0 where one vanishes); the cap disks belong to P.
+//
+// FP32 decides when every margin clears the band: meeting is tested on the
+// segment clipped to the caps grown by the band (a superset of the exact
+// clip) for a certain miss and shrunk by it (a subset) for a certain hit;
+// the start point is certainly inside (a certain miss) or certainly outside
+// likewise.  Anything else is re-tested in FP64.
+
+// Unit normals of the flat caps of a Bezier piece (zero: no cap).
+template <class T>
+__device__ __forceinline__ void quad_caps(V3<T> B0, V3<T> B1, V3<T> B2, V3<T>& n0, V3<T>& n1) {
+    V3<T> t0 = vsub(B1, B0), t1 = vsub(B2, B1);
+    const V3<T> ch = vsub(B2, B0);
+    if (vdot(t0, t0) == T(0)) t0 = ch;
+    if (vdot(t1, t1) == T(0)) t1 = ch;
+    const T l0 = sqrt(vdot(t0, t0)), l1 = sqrt(vdot(t1, t1));
+    n0 = l0 > T(0) ? vscale(t0, T(1) / l0) : vm<T>(T(0), T(0), T(0));
+    n1 = l1 > T(0) ? vscale(t1, T(1) / l1) : vm<T>(T(0), T(0), T(0));
+}
+
+// The part of p + t (q - p), t in [0, 1], inside both caps grown by g
+// (negative: shrunk): false when empty.
+template <class T>
+__device__ __forceinline__ bool cap_clip(V3<T> p, V3<T> q, V3<T> B0, V3<T> B2, V3<T> n0, V3<T> n1, T g, V3<T>& a,
+                                         V3<T>& b) {
+    const V3<T> d = vsub(q, p);
+    T lo = T(0), hi = T(1);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const V3<T> n = k ? n1 : n0;
+        if (vdot(n, n) == T(0)) continue;
+        const T s = k ? vdot(vsub(B2, p), n) : vdot(vsub(p, B0), n);  // signed distance inside
+        const T sl = k ? -vdot(d, n) : vdot(d, n);
+        if (sl == T(0)) {
+            if (s < -g) return false;
+            continue;
+        }
+        const T t = (-g - s) / sl;
+        if (sl > T(0)) lo = t > lo ? t : lo;
+        else hi = t < hi ? t : hi;
+    }
+    if (lo > hi) return false;
+    a = vadd(p, vscale(d, lo));
+    b = vadd(p, vscale(d, hi));
+    return true;
+}
+
+template <class T>
+__device__ __forceinline__ bool cap_inside(V3<T> p, V3<T> B0, V3<T> B2, V3<T> n0, V3<T> n1, T g) {
+    if (vdot(n0, n0) > T(0) && vdot(vsub(p, B0), n0) < -g) return false;
+    if (vdot(n1, n1) > T(0) && vdot(vsub(B2, p), n1) < -g) return false;
+    return true;
+}
+
+// FP64 decision of one (edge, unit) pair under the entering-ray semantics.
+template <bool QUAD>
+__device__ __noinline__ bool surface_retest_f64(float4 ea, float4 eb, float4 P0, float4 P1, float4 P2, float r) {
+    const V3<double> p = v3cast<double>(ea), q = v3cast<double>(eb);
+    const double rr = (double) r * (double) r;
+    if (!QUAD) {
+        const V3<double> a = v3cast<double>(P0), b = v3cast<double>(P1);
+        return seg_seg2<double>(p, q, a, b) <= rr && seg_seg2<double>(p, p, a, b) > rr;
+    }
+    const V3<double> B0 = v3cast<double>(P0), B1 = v3cast<double>(P1), B2 = v3cast<double>(P2);
+    V3<double> n0, n1, a, b;
+    quad_caps<double>(B0, B1, B2, n0, n1);
+    if (!cap_clip<double>(p, q, B0, B2, n0, n1, 0.0, a, b)) return false;
+    if (seg_quad2<double>(a, b, B0, B1, B2, 48) > rr) return false;
+    return !(cap_inside<double>(p, B0, B2, n0, n1, 0.0) && seg_quad2<double>(p, p, B0, B1, B2, 48) <= rr);
+}
+
+template <bool QUAD>
+__device__ __forceinline__ bool leaf_hit_surface(const float4* __restrict__ ep, uint32_t leaf, const SweepUnit& U,
+                                                 unsigned long long* stats, unsigned long long& n_roots) {
+    const float4* e = ep + 2ull * leaf;
+    const float4 ea = __ldg(e), eb = __ldg(e + 1);
+    const V3<float> p = v3cast<float>(ea), q = v3cast<float>(eb);
+    const float r = U.r, tol = kSweepBand + 1e-6f * r;
+    if (!QUAD) {
+        const V3<float> a = v3cast<float>(U.P0), b = v3cast<float>(U.P1);
+        const float dseg = sqrtf(fmaxf(seg_seg2<float>(p, q, a, b), 0.f));
+        if (dseg > r + tol) return false;
+        const float dp = sqrtf(fmaxf(seg_seg2<float>(p, p, a, b), 0.f));
+        if (dp < r - tol) return false;                     // starts inside: never enters
+        if (dseg < r - tol && dp > r + tol) return true;    // a certain hit
+    } else {
+        const V3<float> B0 = v3cast<float>(U.P0), B1 = v3cast<float>(U.P1), B2 = v3cast<float>(U.P2);
+        V3<float> n0, n1, a, b;
+        quad_caps<float>(B0, B1, B2, n0, n1);
+        if (!cap_clip<float>(p, q, B0, B2, n0, n1, kSweepBand, a, b)) return false;
+        bool miss = false;
+        const float dg = quad_dist_bracket(a, b, U, r, tol, miss, n_roots);
+        if (miss || dg > r + tol) return false;
+        bool pm = false;
+        const float dp = quad_dist_bracket(p, p, U, r, tol, pm, n_roots);
+        if (!pm && dp < r - tol && cap_inside<float>(p, B0, B2, n0, n1, -kSweepBand)) return false;  // inside
+        const bool maybe_inside = !pm && dp <= r + tol && cap_inside<float>(p, B0, B2, n0, n1, kSweepBand);
+        if (!maybe_inside) {
+            bool sm = false;
+            const bool clipped = cap_clip<float>(p, q, B0, B2, n0, n1, -kSweepBand, a, b);
+            if (clipped && quad_dist_bracket(a, b, U, r, tol, sm, n_roots) < r - tol && !sm) return true;
+        }
+    }
+    atomicAdd(stats, 1ull);
+    return surface_retest_f64<QUAD>(ea, eb, U.P0, U.P1, U.P2, r);
 }
 
 // Light pass: one lane per unit, "while-while" (Aila and Laine 2009): lanes
@@ -457,7 +578,7 @@ __device__ __forceinline__ bool leaf_hit(const float4* __restrict__ ep, uint32_t
 // child records loaded at once, the overlapping children pushed far to near
 // so the nearest is visited first), half the dependent node loads of the
 // binary tree; it needs a wide tree shallow enough for the lane stack.
-template <bool QUAD, int BLOCK, bool WIDE>
+template <bool QUAD, int BLOCK, bool WIDE, bool SURF>
 __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOCK) k_sweep(const SceneDev S, const SweepArgs A) {
     const float4* __restrict__ en = WIDE ? S.edge_wide : S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
@@ -583,7 +704,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
         }
         if (leaf != kNone) {
             ++n_leaf;
-            if (leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
+            if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots) : leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
                 if (A.want_pieces) atomicExch(A.piece_hit + U.piece_g, 1u);
                 if (A.want_counts) {
                     A.traj_hit[U.traj] = 1u;
@@ -624,7 +745,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
 constexpr int kHeavyWarps = 4;
 constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
 
-template <bool QUAD>
+template <bool QUAD, bool SURF>
 __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev S, const SweepArgs A) {
     __shared__ uint32_t s_front[kHeavyWarps][kFrontier];
     __shared__ uint32_t s_leaf[kHeavyWarps][kLeafBuf];
@@ -659,7 +780,8 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
                 bool hit = false;
                 if (leaf != kNone) {
                     ++n_leaf;
-                    hit = leaf_hit<QUAD>(S.edge_prims, leaf, U, A.stats, n_roots);
+                    hit = SURF ? leaf_hit_surface<QUAD>(S.edge_prims, leaf, U, A.stats, n_roots)
+                               : leaf_hit<QUAD>(S.edge_prims, leaf, U, A.stats, n_roots);
                 }
                 const uint32_t mh = __ballot_sync(0xffffffffu, hit);
                 if (mh) {
@@ -728,13 +850,13 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
 
 template <bool QUAD>
 static int sweep_per_sm(int threads) {
-    int per_sm = 0;  // the wide and binary forms share their register caps
+    int per_sm = 0;  // the wide and binary forms (and both semantics) share their register caps
     if (threads == 64)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 64, true>, 64, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 64, true, false>, 64, 0);
     else if (threads == 256)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 256, true>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 256, true, false>, 256, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 128, true>, 128, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<QUAD, 128, true, false>, 128, 0);
     return std::max(1, per_sm);
 }
 
@@ -744,52 +866,55 @@ uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads) {
 
 uint32_t sweep_persistent_blocks(bool quad) { return sweep_max_blocks_per_sm(quad, kTravThreads) * device_sm_count(); }
 
-template <bool QUAD>
+template <bool QUAD, bool SURF>
 static uint32_t heavy_blocks() {
     static uint32_t blocks = 0;
     if (!blocks) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD>, kHeavyWarps * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD, SURF>, kHeavyWarps * 32, 0);
         blocks = (uint32_t) std::max(1, per_sm) * device_sm_count();
     }
     return blocks;
 }
 
-template <bool QUAD>
+template <bool QUAD, bool SURF>
 static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads,
                            uint32_t heavy_share, cudaStream_t s) {
     if (S.edge_wide_lane && !A.binary_tree) {
         if (threads == 64)
-            k_sweep<QUAD, 64, true><<<blocks, 64, 0, s>>>(S, A);
+            k_sweep<QUAD, 64, true, SURF><<<blocks, 64, 0, s>>>(S, A);
         else if (threads == 256)
-            k_sweep<QUAD, 256, true><<<blocks, 256, 0, s>>>(S, A);
+            k_sweep<QUAD, 256, true, SURF><<<blocks, 256, 0, s>>>(S, A);
         else
-            k_sweep<QUAD, 128, true><<<blocks, 128, 0, s>>>(S, A);
+            k_sweep<QUAD, 128, true, SURF><<<blocks, 128, 0, s>>>(S, A);
     } else {
         if (threads == 64)
-            k_sweep<QUAD, 64, false><<<blocks, 64, 0, s>>>(S, A);
+            k_sweep<QUAD, 64, false, SURF><<<blocks, 64, 0, s>>>(S, A);
         else if (threads == 256)
-            k_sweep<QUAD, 256, false><<<blocks, 256, 0, s>>>(S, A);
+            k_sweep<QUAD, 256, false, SURF><<<blocks, 256, 0, s>>>(S, A);
         else
-            k_sweep<QUAD, 128, false><<<blocks, 128, 0, s>>>(S, A);
+            k_sweep<QUAD, 128, false, SURF><<<blocks, 128, 0, s>>>(S, A);
     }
     cuda_check(cudaGetLastError(), "k_sweep");
     // the heavy pass stays on the binary tree: for a thin capsule its inner boxes cull more than a
     // wide node's four child boxes (the wide warp descent tested 25-40 % more boxes, measured on
     // the 4,096-trajectory sweeps)
     if (A.light_steps) {
-        const uint32_t hb = std::max(1u, heavy_blocks<QUAD>() * heavy_share / 100);
-        k_sweep_heavy<QUAD><<<hb, kHeavyWarps * 32, 0, s>>>(S, A);
+        const uint32_t hb = std::max(1u, heavy_blocks<QUAD, SURF>() * heavy_share / 100);
+        k_sweep_heavy<QUAD, SURF><<<hb, kHeavyWarps * 32, 0, s>>>(S, A);
         cuda_check(cudaGetLastError(), "k_sweep_heavy");
     }
 }
 
 void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, uint32_t heavy_share,
                   cudaStream_t s) {
-    if (A.quad)
-        sweep_dispatch<true>(S, A, blocks, threads, heavy_share, s);
-    else
-        sweep_dispatch<false>(S, A, blocks, threads, heavy_share, s);
+    if (A.quad) {
+        if (A.surface) sweep_dispatch<true, true>(S, A, blocks, threads, heavy_share, s);
+        else sweep_dispatch<true, false>(S, A, blocks, threads, heavy_share, s);
+    } else {
+        if (A.surface) sweep_dispatch<false, true>(S, A, blocks, threads, heavy_share, s);
+        else sweep_dispatch<false, false>(S, A, blocks, threads, heavy_share, s);
+    }
 }
 
 }  // namespace rtcd

@@ -30,6 +30,7 @@ CHECK_FUSED = 1 << 6
 CHECK_GRAPH = 1 << 7
 CHECK_CONTAINMENT = 1 << 8
 CHECK_TWO_WAY = 1 << 9
+CHECK_SURFACE = 1 << 10
 
 STATUS = {0: 'RTCD_OK', 1: 'RTCD_ERR_INVALID_ARGUMENT', 2: 'RTCD_ERR_CUDA', 3: 'RTCD_ERR_OUT_OF_MEMORY',
           4: 'RTCD_ERR_DEVICE_TIMEOUT', 5: 'RTCD_ERR_CAPACITY', 6: 'RTCD_ERR_INTERNAL'}
@@ -41,7 +42,8 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_server_create', 'rtcd_server_destroy', 'rtcd_server_submit', 'rtcd_server_wait',
            'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
            'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights', 'rtcd_urdf_chain_parse', 'rtcd_obj_load',
-           'rtcd_halton_samples', 'rtcd_knn', 'rtcd_check_edges']
+           'rtcd_halton_samples', 'rtcd_knn', 'rtcd_check_edges', 'rtcd_selftest_lookback_timeout',
+           'rtcd_loop_edges']
 
 
 class RTCDError(RuntimeError):
@@ -142,6 +144,23 @@ def exclusive_scan_u32(ctx, in_dev, out_dev, n, total_dev=None, stream=None):
 def select_flags_u8(ctx, mask_dev, n, idx_dev, count_dev, stream=None):
     _ok(lib().rtcd_select_flags_u8(ctx.h, _ptr(mask_dev, C.c_uint8), C.c_uint32(n), _ptr(idx_dev, C.c_uint32),
                                    _ptr(count_dev, C.c_uint32), C.c_void_p(stream) if stream else None))
+
+
+def loop_edges(tris):
+    """Directed loop edges of a mesh as the library builds them (host only): (m, 2) uint32."""
+    tris = _arr(tris, np.uint32).reshape(-1, 3)
+    n = C.c_uint32()
+    _ok(lib().rtcd_loop_edges(_ptr(tris, C.c_uint32), C.c_uint32(len(tris)), None, C.c_uint32(0), C.byref(n)))
+    out = np.zeros((max(n.value, 1), 2), np.uint32)
+    _ok(lib().rtcd_loop_edges(_ptr(tris, C.c_uint32), C.c_uint32(len(tris)), _ptr(out, C.c_uint32),
+                              C.c_uint32(n.value), C.byref(n)))
+    return out[:n.value]
+
+
+def selftest_lookback_timeout(ctx, n, spin_limit):
+    """Runs the bounded-wait self-test; returns its status code (4 = RTCD_ERR_DEVICE_TIMEOUT is the
+    designed outcome: every look-back wait ran out and the kernel returned)."""
+    return lib().rtcd_selftest_lookback_timeout(ctx.h, C.c_uint32(n), C.c_uint32(spin_limit))
 
 
 def quad_fit_weights(n_ctrl, n_wp):
@@ -365,10 +384,11 @@ class Detector:
     def sweep(self):
         return self.kind in (LINEAR_SWEEP, QUAD_SWEEP)
 
-    def check(self, q, traj_off=None, counts=False, segments=False, flags=0):
-        """Host-buffer call: q is a numpy array; returns dict of numpy outputs."""
+    def check(self, q, traj_off=None, counts=False, segments=False, flags=0, surface=False):
+        """Host-buffer call: q is a numpy array; returns dict of numpy outputs.
+        surface=True: the sweeps' reference (entering-ray) semantics."""
         q = _arr(q, np.float32)
-        flags |= CHECK_HOST_BUFFERS | (CHECK_COUNTS if counts else 0)
+        flags |= CHECK_HOST_BUFFERS | (CHECK_COUNTS if counts else 0) | (CHECK_SURFACE if surface else 0)
         if self.sweep:
             traj_off = _arr(traj_off, np.uint32)
             n = len(traj_off) - 1
@@ -530,9 +550,10 @@ class Server:
         """Size every slot's workspace for `det` up front (serving then never allocates)."""
         _ok(lib().rtcd_server_prepare(self.h, det.h, C.c_uint32(max_units)))
 
-    def submit(self, det, q, traj_off=None, counts=False, endpoints=True):
+    def submit(self, det, q, traj_off=None, counts=False, endpoints=True, surface=False):
         q = _arr(q, np.float32)
-        flags = (CHECK_COUNTS if counts else 0) | (0 if endpoints else CHECK_NO_ENDPOINTS)
+        flags = (CHECK_COUNTS if counts else 0) | (0 if endpoints else CHECK_NO_ENDPOINTS) | \
+            (CHECK_SURFACE if surface else 0)
         if det.sweep:
             traj_off = _arr(traj_off, np.uint32)
             n = len(traj_off) - 1

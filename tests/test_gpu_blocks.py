@@ -91,3 +91,29 @@ def test_lbvh_bit_identical_to_canonical(ctx, which):
         assert np.array_equal(conv, child.astype(np.int64))
         assert np.array_equal(g['node_lo'], nlo) and np.array_equal(g['node_hi'], nhi)
     assert g['depth'] <= 62
+
+
+@pytest.mark.parametrize('n', [1, 5000, 70001])
+def test_lookback_wait_runs_out_and_reports(ctx, n):
+    """Failure detection of the bounded device waits, made to fire on purpose:
+    tile 0 of the look-back compaction never publishes (no block takes it),
+    so every other tile's wait runs out after a short spin limit.  The kernel
+    must return, the call must report RTCD_ERR_DEVICE_TIMEOUT, and the context
+    must stay usable: a normal compaction on it afterwards is exact."""
+    import time
+
+    import torch
+    t0 = time.time()
+    st = rtcd.selftest_lookback_timeout(ctx, n, 256)
+    assert st == 4, (st, rtcd.last_error())  # RTCD_ERR_DEVICE_TIMEOUT
+    assert 'ran out' in rtcd.last_error()
+    assert time.time() - t0 < 30.0
+    m = (np.arange(4097) % 3 == 0).astype(np.uint8)
+    md = torch.from_numpy(m).cuda()
+    idx = torch.zeros(len(m), dtype=torch.int32, device='cuda')
+    cnt = torch.zeros(1, dtype=torch.int32, device='cuda')
+    rtcd.select_flags_u8(ctx, md, len(m), idx, cnt)
+    torch.cuda.synchronize()
+    ref = np.nonzero(m)[0]
+    assert int(cnt.item()) == len(ref)
+    assert np.array_equal(idx.cpu().numpy()[:len(ref)], ref)
