@@ -214,7 +214,8 @@ def oracle_errors(cfg, model, mesh, spheres, q, off, flags, n_sample=512, two_wa
             'collision_rate': float(ref['traj_hit'].mean())}
 
 
-def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0, server_kw=None, details=False):
+def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0, server_kw=None, details=False,
+                  saturate_requests=0):
     """Mixed request stream against three resident scenes (5k, 50k, ~500k
     triangles): Poisson arrivals at `rate` req/s for `seconds`; half discrete
     RobotToObs batches of log-uniform[1, 4096] poses, half continuous batches
@@ -223,7 +224,11 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
     server from a submitter thread at their arrival times; latency is submit
     to result.  The same arrivals (first `plain_seconds`) are then replayed on
     the plain form - one request at a time, each a frame-by-frame check with a
-    host round trip per frame - for comparison."""
+    host round trip per frame - for comparison.  With saturate_requests, the
+    first that many requests of the mix are also submitted all at once (no
+    arrival gaps), and the units the server completes per second are set
+    beside the plain form's on the same requests (saturated throughput, not
+    the offered load)."""
     import threading
     from rtcollisiondetection_b200 import rtcd, scenes
     model = scenes.load_panda()
@@ -282,6 +287,32 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
         return lat, wall, st
 
     lat, wall, st = run_server()
+
+    def saturated(m):
+        """Units per second (poses + trajectories) of the first m requests, all submitted at once to
+        the server, and the same requests checked one at a time on the plain form."""
+        server = rtcd.Server(ctx, slots=slots, **(server_kw or {}))
+        for d in dets:
+            for det in d.values():
+                server.prepare(det, 1 << 17 if det.sweep else 0)
+        units = float(sum(r[3] for r in reqs[:m]))
+        t0 = time.perf_counter()
+        tickets = [server.submit(det, q, off) for det, q, off, _ in reqs[:m]]
+        for t in tickets:
+            server.wait(t)
+        sw = time.perf_counter() - t0
+        server.close()
+        t0 = time.perf_counter()
+        for det, q, off, _ in reqs[:m]:
+            det.check(q, off, flags=0 if det.sweep else rtcd.CHECK_PLAIN)
+        pw = time.perf_counter() - t0
+        return {'requests': m, 'units': units, 'served_units_per_s': units / sw, 'served_wall_s': sw,
+                'plain_units_per_s': units / pw, 'plain_wall_s': pw, 'served_over_plain': pw / sw,
+                'note': 'units = poses + trajectories of the mixed requests; served = all submitted at once, '
+                        'continuous batching over 4 slots; plain = one request at a time (discrete requests on '
+                        'the upstream-shaped frame path, sweep requests as one call each)'}
+
+    sat = saturated(min(saturate_requests, n_req)) if saturate_requests > 0 else None
     disc = np.array([r[2] is None for r in reqs])
     sizes = np.array([r[3] for r in reqs])
     poses = int(sizes[disc].sum())
@@ -292,7 +323,11 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
            'p50_ms_all': float(np.percentile(lat, 50)), 'p99_ms_all': float(np.percentile(lat, 99)),
            'poses_per_s': poses / wall, 'trajectories_per_s': trajs / wall, 'batches': st['batches'],
            'queue_p50_ms': st['queue_p50_ms'], 'queue_p99_ms': st['queue_p99_ms'], 'run_p99_ms': st['run_p99_ms'],
-           'scenes_tris': [m.n_tris for m in meshes]}
+           'scenes_tris': [m.n_tris for m in meshes],
+           'p99_margin_ms_discrete_le4096': 2.0 - float(np.percentile(lat[disc], 99)),
+           'p99_margin_ms_all': 2.0 - float(np.percentile(lat, 99))}
+    if sat:
+        out['saturated'] = sat
     if details:
         scene_of = {id(det): i for i, d in enumerate(dets) for det in d.values()}
         out['details'] = {'latency_ms': lat, 'discrete': disc, 'size': sizes,
@@ -400,6 +435,75 @@ def run_reference(args, cfg, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _free_port():
+    import socket
+    sk = socket.socket()
+    sk.bind(('127.0.0.1', 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    return port
+
+
+def spawn_ranks(n):
+    """`--gpus N` without an outside launcher: start N copies of this script,
+    one per GPU, with RANK / LOCAL_RANK / WORLD_SIZE and a rendezvous on
+    127.0.0.1 (what torch.distributed.run would set), and wait for them.
+    Rank 0 prints the JSON line; the exit code is the worst of the ranks'."""
+    port = _free_port()
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n), LOCAL_WORLD_SIZE=str(n),
+                   MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:], env=env))
+    rc = 0
+    for p in procs:
+        rc = max(rc, p.wait())
+    return rc
+
+
+def run_dry(args, cfg, rank, world):
+    """The multi-rank plumbing without a GPU (gloo on CPU): every rank checks
+    its own seeded batch with the CPU oracle, the flags are all-gathered as
+    in the GPU run, and rank 0 checks the gathered array against its own
+    single-process run of every rank's batch."""
+    import datetime
+
+    import torch.distributed as dist
+    from oracle import oracle as O
+    from rtcollisiondetection_b200 import scenes, sharding
+    if world > 1:
+        dist.init_process_group('gloo', rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        n = min(cfg['n'], args.dry_units)
+        model, mesh, spheres, q, off = make_inputs(dict(cfg, n=n), rank, scenes)
+        robot, scene = O.Robot(model, spheres=spheres), O.Scene(mesh)
+
+        def check(q, off):
+            if off is None:
+                kind = O.ROBOT_TO_OBS if cfg['kind'] == 'RobotToObs' else O.OBS_TO_ROBOT
+                return O.discrete(kind, robot, scene, q)['hit']
+            return O.sweep(cfg['kind'] == 'Quadratic', robot, scene, q, off)['traj_hit']
+
+        t0 = time.perf_counter()
+        local = check(q, off)
+        dt = sharding.max_over_ranks(time.perf_counter() - t0)
+        flags = sharding.gather_flags(local, n * world, world)
+        if rank == 0:
+            want = np.concatenate([check(*make_inputs(dict(cfg, n=n), r, scenes)[3:]) for r in range(world)])
+            line = {'metric': METRIC, 'value': n * world / dt, 'unit': 'trajectories/s' if off is not None else 'poses/s',
+                    'n_gpus': world, 'steps': 1, 'warmup': 0, 'ms_per_step': dt * 1e3, 'higher_is_better': True,
+                    'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                    'dry': 'CPU oracle per rank over gloo: exercises the launcher and the flag all-gather only',
+                    'config': {'workload': cfg['workload'], 'units_per_gpu': n},
+                    'gathered': {'units': int(len(flags)), 'equal_to_single_process': bool(np.array_equal(flags, want))}}
+            print(json.dumps(line), flush=True)
+            if not np.array_equal(flags, want):
+                sys.exit(3)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -410,18 +514,28 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-check', action='store_true')
     ap.add_argument('--ref-sample', type=int, default=8192)
-    ap.add_argument('--plain-frame', type=int, default=64)
+    ap.add_argument('--plain-frame', type=int, default=1024, help='poses per frame of the plain arm (upstream batchSize)')
+    ap.add_argument('--plain-streams', type=int, default=4, help='streams / host threads of the plain arm (upstream NSTREAM)')
     ap.add_argument('--fused', action='store_true', help='discrete: the thread-per-item traversal kernel')
     ap.add_argument('--no-graph', action='store_true', help='launch the timed steps directly, not as a CUDA graph')
     ap.add_argument('--two-way', action='store_true', help='discrete: both directions in one check (flags = union)')
     ap.add_argument('--containment', action='store_true', help='discrete: add the containment test')
-    ap.add_argument('--serve-seconds', type=float, default=5.0,
+    ap.add_argument('--serve-seconds', type=float, default=60.0,
                     help='length of the served mixed stream reported under "served" (0: skip)')
+    ap.add_argument('--saturate-requests', type=int, default=4000,
+                    help='requests of the served mix submitted at once to measure saturated throughput (0: skip)')
+    ap.add_argument('--dry', action='store_true', help='no GPU: the multi-rank plumbing with the CPU oracle over gloo')
+    ap.add_argument('--dry-units', type=int, default=256, help='units per rank of a --dry run')
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if args.gpus > 1 and 'WORLD_SIZE' not in os.environ:
+        sys.exit(spawn_ranks(args.gpus))
     rank = int(os.environ.get('RANK', 0))
     world = int(os.environ.get('WORLD_SIZE', 1))
     local = int(os.environ.get('LOCAL_RANK', 0))
+    if args.dry:
+        run_dry(args, cfg, rank, world)
+        return
     if args.impl == 'reference':
         run_reference(args, cfg, rank, world)
         return
@@ -438,7 +552,7 @@ def main():
     ctx = rtcd.Context(local)
     robot = rtcd.Robot(ctx, model, spheres=spheres)
     scene = rtcd.Scene.from_mesh(ctx, mesh)
-    det = rtcd.Detector(ctx, cfg['kind'], robot, scene, frame_size=args.plain_frame)
+    det = rtcd.Detector(ctx, cfg['kind'], robot, scene, frame_size=args.plain_frame, plain_streams=args.plain_streams)
     sweep = det.sweep
     n = cfg['n']
     # a dedicated stream: the legacy default stream has handle 0, which the ABI
@@ -497,6 +611,18 @@ def main():
     unit = 'trajectories/s' if sweep else 'poses/s'
     flags = fd.cpu().numpy()
     st = det.stats()
+    gathered = None
+    if dist:
+        # the one exchange of the sharded path: every rank's flags, concatenated (NCCL all-gather);
+        # rank 0 checks them against its own run of every rank's batch
+        from rtcollisiondetection_b200 import sharding
+        allf = sharding.gather_flags(flags, n * world, world, device=torch.device('cuda', local))
+        if rank == 0:
+            ok = True
+            for r in range(world):
+                qr, offr = make_inputs(cfg, r, scenes)[3:]
+                ok &= bool(np.array_equal(det.check(qr, offr, flags=mode_flags)['flags'], allf[r * n:(r + 1) * n]))
+            gathered = {'units': int(len(allf)), 'equal_to_rank0_rerun': ok}
 
     # end to end through the C ABI with host buffers (upload + download inside the call, in the graph)
     e2e_ms = []
@@ -515,20 +641,31 @@ def main():
     h2d = q.nbytes + (0 if off is None else off.nbytes)
     d2h = n + n_seg
 
-    # plain path: frames of 64 poses, host round trip per frame (the upstream check() shape)
-    plain = None
+    # plain path: the upstream check() shape - frames of 1,024 poses over 4 streams, one host thread per
+    # stream, a host round trip per frame, a wait after every 4 frames; plus the 64-pose single-stream
+    # frame path as a labelled extra
+    plain = plain64 = None
     if not sweep:
-        pm = []
-        for k in range(3):
-            flush.fill_(k & 255)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            det.check_device(qd, n, fd, flags=rtcd.CHECK_PLAIN | mode_flags, stream=sp)
-            torch.cuda.synchronize()
-            pm.append((time.perf_counter() - t0) * 1e3)
-        assert np.array_equal(fd.cpu().numpy(), flags), 'plain path disagrees'
-        plain = {'value': units_all / (np.median(pm) / 1e3), 'unit': unit, 'frame': args.plain_frame,
-                 'ms_per_step': float(np.median(pm))}
+        def time_plain(d):
+            pm = []
+            for k in range(3):
+                flush.fill_(k & 255)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                d.check_device(qd, n, fd, flags=rtcd.CHECK_PLAIN | mode_flags, stream=sp)
+                torch.cuda.synchronize()
+                pm.append((time.perf_counter() - t0) * 1e3)
+            assert np.array_equal(fd.cpu().numpy(), flags), 'plain path disagrees'
+            return float(np.median(pm))
+        pms = time_plain(det)
+        plain = {'value': n / (pms / 1e3), 'unit': unit, 'frame': args.plain_frame, 'streams': args.plain_streams,
+                 'host_threads': args.plain_streams, 'ms_per_step': pms,
+                 'shape': 'upstream check(): frames round-robin over streams, one host thread per stream, item '
+                          'count read back per frame, wait after every group of frames'}
+        det64 = rtcd.Detector(ctx, cfg['kind'], robot, scene, frame_size=64, plain_streams=1)
+        pm64 = time_plain(det64)
+        det64.close()
+        plain64 = {'value': n / (pm64 / 1e3), 'unit': unit, 'frame': 64, 'streams': 1, 'ms_per_step': pm64}
 
     peaks, peak_src = load_peaks()
     # traversal span of the same step, timed with events around its kernels (graph replays are timed whole)
@@ -557,22 +694,47 @@ def main():
         t = json.load(open(tp)).get(args.config)
         if t and t.get('span') == span:
             traffic = t['bytes_per_span']
-    # FP32 work the kernels did, from their own counters (mean over the timed steps)
+    # FP32 work each kernel did, from its own counters, over its own event-timed duration (the
+    # counters are the means over the timed steps; the durations the means over the span runs)
     links = model['cos_mask'].shape[0] + 1
-    nodes = float(np.mean([s['node_tests'] for s in trav]))
-    leaves = float(np.mean([s['exact_tests'] for s in trav]))
-    if sweep:
-        w_ours = 18 * nodes + (200 if cfg['kind'] == 'Quadratic' else 45) * leaves + 72 * links * float(off[-1])
-    else:
-        cands = float(np.mean([s['candidates'] for s in trav]))
-        w_ours = (18 * nodes + 40 * leaves + 36 * cands + 180 * n * (links - 1) * scene.n_obstacles
-                  + 72 * links * n)
-    fp32 = {'achieved': w_ours / (t_trav / 1e3) / 1e12, 'peak': FP32_PEAK_TFLOPS, 'unit': 'TFLOP/s',
-            'frac': w_ours / (t_trav / 1e3) / 1e12 / FP32_PEAK_TFLOPS, 'flops_per_step': w_ours,
-            'node_tests': nodes, 'leaf_tests': leaves,
-            'peak_source': 'nominal (148 SMs x 128 lanes x 2 x 1.965 GHz)',
-            'weights': 'flops per op: node slab/box test 18, segment-triangle 40, segment-capsule 45, '
-                       'segment-quadratic 200, OBB SAT pair 180, FK link 72, primitive transform 36'}
+
+    def mean(key, runs=trav):
+        return float(np.mean([r[key] for r in runs]))
+
+    nodes, leaves = mean('node_tests'), mean('exact_tests')
+    nodes1, leaves1 = mean('first_node_tests'), mean('first_exact_tests')
+    w_leaf = 40 if not sweep else (200 if cfg['kind'] == 'Quadratic' else 45)
+    w_span = 18 * nodes + w_leaf * leaves
+    w_first = 18 * nodes1 + w_leaf * leaves1
+    if not sweep:
+        cands = mean('candidates')
+        w_span += 36 * cands   # every candidate primitive is moved into its link's frame
+    t_first = float(np.mean([r['ms_first_pass'] for r in spans]))
+    t_rest = max(t_trav - t_first, 1e-6)
+
+    def kern(flops, ms):
+        return {'flops': flops, 'ms': ms, 'achieved': flops / (ms / 1e3) / 1e12,
+                'frac': flops / (ms / 1e3) / 1e12 / FP32_PEAK_TFLOPS}
+    kernels = {'traversal_span': kern(w_span, t_trav),
+               'first_pass': dict(kern(w_first, t_first), kernel='k_sweep (light pass)' if sweep else
+                                  ('k_stage_ab' if form in (0, 3, 4) else 'k_stage_a')),
+               'later_passes': dict(kern(max(w_span - w_first, 0.0), t_rest),
+                                    kernel='k_sweep_heavy' if sweep else
+                                    'k_subtree x 2 + k_stage_b + k_stage_b_heavy + k_discrete')}
+    if not sweep:
+        sats, sph = mean('cull_sat_tests'), mean('cull_sphere_tests')
+        t_cull = float(np.mean([r['ms_cull'] for r in spans]))
+        kernels['cull'] = dict(kern(180 * sats + 8 * sph + 36 * n * (links - 1), t_cull),
+                               kernel='k_cull + k_select_u8', sat_pairs=sats, sphere_tests=sph,
+                               all_pairs=n * (links - 1) * scene.n_obstacles)
+    fp32 = {'achieved': kernels['traversal_span']['achieved'], 'peak': FP32_PEAK_TFLOPS, 'unit': 'TFLOP/s',
+            'frac': kernels['traversal_span']['frac'], 'flops_per_step': w_span,
+            'node_tests': nodes, 'leaf_tests': leaves, 'kernels': kernels,
+            'peak_source': 'nominal fallback: no FP32 peak in MEASURED_PEAKS.json '
+                           '(148 SMs x 128 lanes x 2 x 1.965 GHz)',
+            'weights': 'flops per counted op: node slab/box test 18, segment-triangle 40, segment-capsule 45, '
+                       'segment-quadratic 200, candidate moved to the link frame 36, OBB SAT 180, '
+                       'bounding-sphere test 8, world OBB 36'}
     if not args.no_check:
         fp32['reference_work'] = fp32_work(cfg, model, mesh, spheres, q, off, scene, t_trav)
     line = {
@@ -604,15 +766,20 @@ def main():
                              'read+write of the span\'s kernels (profiles/traffic.json)'},
         'clocks': clocks,
     }
+    if gathered:
+        line['gathered'] = gathered
     if plain:
+        # per GPU on both sides: the plain arm runs on rank 0's GPU alone
         line['plain'] = plain
-        line['batched_over_plain'] = value / plain['value']
+        line['batched_over_plain'] = value / world / plain['value']
+        line['plain_frame64'] = plain64
+        line['batched_over_plain_frame64'] = value / world / plain64['value']
     if not args.no_check and rank == 0:
         line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags, two_way=args.two_way,
                                       containment=args.containment)
         line['fp64_retests'] = st['fp64_retests']
     if args.serve_seconds > 0 and rank == 0 and args.config == 'c2':
-        line['served'] = served_stream(ctx, args.serve_seconds)
+        line['served'] = served_stream(ctx, args.serve_seconds, saturate_requests=args.saturate_requests)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         line['cpu_baseline'] = cpu_baseline(cfg, model, mesh, spheres, q, off)
     if rank == 0:

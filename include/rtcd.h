@@ -63,7 +63,10 @@ typedef enum {
 #define RTCD_CHECK_NO_CULL (1u << 2)       /* skip the OBB prefilter of the discrete detectors (every item goes to
                                               the traversal, whose first step rejects the far ones: up to 9 % faster at
                                               a few thousand poses, slower at tens of thousands) */
-#define RTCD_CHECK_PLAIN (1u << 3)         /* frame-by-frame path with a host sync per frame */
+#define RTCD_CHECK_PLAIN (1u << 3)         /* discrete: the upstream check() shape - frames of frame_size poses over
+                                              plain_streams streams, one host thread per stream, a host round trip
+                                              per frame (the culled item count) and a wait after every group of
+                                              plain_streams frames; synchronous */
 #define RTCD_CHECK_NO_ENDPOINTS (1u << 4)  /* quadratic: do not add the start/end waypoint spheres */
 #define RTCD_CHECK_TIMING (1u << 5)        /* record device events around the stages (rtcd_last_stats) */
 #define RTCD_CHECK_FUSED (1u << 6)         /* discrete: one fused traversal kernel instead of the two-stage wavefront */
@@ -118,7 +121,8 @@ typedef struct {
 } rtcd_robot_desc;
 
 typedef struct {
-    uint32_t frame_size;             /* poses per frame of the plain path; 0 = 64 */
+    uint32_t frame_size;             /* poses per frame of the plain path; 0 = 1024 (the upstream benchmark's
+                                        batchSize, RTCD/Benchmark/Discrete/benchmarkUtils.h:16) */
     uint32_t traverse_threads;       /* threads per block of the traversal kernel: 64, 128 or 256; 0 = 128 */
     uint32_t traverse_blocks_per_sm; /* resident traversal blocks per SM; 0 = as many as fit */
     int32_t stream_priority;         /* priority of the detector's own stream (CUDA convention: lower = higher) */
@@ -142,6 +146,14 @@ typedef struct {
                                         the fused forms, the stage-B steps (32 candidates each) an item runs
                                         in its warp before its further candidates go to a one-lane pass over
                                         the whole GPU; 0 = 64 lanes / 4 packets / 8 steps; at most 4096 */
+    uint32_t plain_streams;          /* streams of the plain path, each driven by its own host thread; frames go to
+                                        them round-robin and the call waits for every group of plain_streams
+                                        frames (upstream NSTREAM = 4 and its thread pool,
+                                        RTCD/CollisionDetector/CollisionDetector.h:396-433); 0 = 4, at most 16 */
+    uint32_t sweep_unstaged;         /* sweeps: 0 = the light pass stages each trajectory's FK (and quadratic fit)
+                                        in shared memory when the batch's longest trajectory fits; 1 = sphere
+                                        centres and control points go through global memory (separate FK and
+                                        fit kernels) */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -292,6 +304,14 @@ typedef struct {
     uint64_t exact_tests;  /* primitive-pair tests run in FP32 */
     uint64_t skipped;      /* candidates dropped because their pose (trajectory) was already decided */
     uint64_t node_tests;   /* BVH child-box tests of the traversal kernels */
+    float ms_first_pass;   /* with RTCD_CHECK_TIMING: the first traversal kernel alone (discrete: the fused or
+                              stage-A kernel of the first direction; sweeps: the light pass) */
+    uint32_t reserved0;
+    uint64_t first_node_tests;   /* node_tests of that first kernel (the rest: the passes after it) */
+    uint64_t first_exact_tests;  /* exact_tests of that first kernel */
+    uint64_t cull_sphere_tests;  /* discrete: bounding-sphere tests of the OBB cull */
+    uint64_t cull_sat_tests;     /* discrete: 15-axis SATs the cull evaluated (after the sphere reject, up to each
+                                    item's first overlap) */
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 

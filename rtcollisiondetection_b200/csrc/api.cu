@@ -9,12 +9,15 @@
 // 354-471).
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <new>
+#include <thread>
 #include <unordered_set>
 
 #include "../../include/rtcd.h"
@@ -406,6 +409,73 @@ struct rtcd_scene {
     uint32_t n_loop = 0;
 };
 
+// Host threads of the plain path: worker i runs the frames handed to it on
+// stream i (the upstream ThreadPool, RTCD/CollisionDetector/threadPool.h:
+// 10-92, one task per frame).  run() hands each worker its job for one
+// group and returns when all have finished.
+struct PlainPool {
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv, cv_done;
+    std::vector<std::function<void()>> jobs;
+    uint64_t generation = 0;
+    size_t pending = 0;
+    bool stop = false;
+    std::exception_ptr error;
+
+    explicit PlainPool(size_t n) : jobs(n) {
+        for (size_t i = 0; i < n; ++i) threads.emplace_back([this, i] { work(i); });
+    }
+    ~PlainPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv.notify_all();
+        for (auto& t : threads) t.join();
+    }
+    void work(size_t i) {
+        uint64_t seen = 0;
+        while (true) {
+            std::function<void()> job;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return stop || (generation != seen && jobs[i]); });
+                if (stop) return;
+                seen = generation;
+                job.swap(jobs[i]);
+            }
+            std::exception_ptr ep;
+            try {
+                job();
+            } catch (...) {
+                ep = std::current_exception();
+            }
+            std::lock_guard<std::mutex> lk(mu);
+            if (ep && !error) error = ep;
+            if (--pending == 0) cv_done.notify_all();
+        }
+    }
+    // jobs_in[i] (empty: worker i idles this group)
+    void run(std::vector<std::function<void()>>& jobs_in) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            pending = 0;
+            for (size_t i = 0; i < jobs.size(); ++i)
+                if (jobs_in[i]) {
+                    jobs[i] = std::move(jobs_in[i]);
+                    ++pending;
+                }
+            ++generation;
+            error = nullptr;
+        }
+        cv.notify_all();
+        std::unique_lock<std::mutex> lk(mu);
+        cv_done.wait(lk, [&] { return pending == 0; });
+        if (error) std::rethrow_exception(error);
+    }
+};
+
 struct rtcd_detector {
     rtcd_ctx* ctx = nullptr;
     rtcd_detector_kind kind = RTCD_OBS_TO_ROBOT;
@@ -417,6 +487,7 @@ struct rtcd_detector {
     cudaEvent_t staged = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // stage timing: start, prepared, culled, traversed
     cudaEvent_t ev_end = nullptr;
+    cudaEvent_t ev_first = nullptr;      // after the first traversal kernel (RTCD_CHECK_TIMING)
     bool timed = false;
     cudaStream_t last_stream = nullptr;  // stream of the last check (stats read on it)
     cudaGraph_t graph = nullptr;         // captured launch sequence (RTCD_CHECK_GRAPH)
@@ -440,6 +511,9 @@ struct rtcd_detector {
     HostBuf pin_in, pin_out, pin_aux;
     DevBuf hq, hflags, hseg, hcounts;  // device sides of a graph replay with host buffers
     uint64_t last_items = 0, last_culled = 0;
+    // plain path: one clone of this detector per stream (own stream and workspace) and their threads
+    std::vector<rtcd_detector*> plain_clones;
+    std::unique_ptr<PlainPool> plain_pool;
 };
 
 namespace {
@@ -833,7 +907,9 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         d->robot = robot;
         d->scene = scene;
         if (config) d->cfg = *config;
-        if (!d->cfg.frame_size) d->cfg.frame_size = 64;
+        if (!d->cfg.frame_size) d->cfg.frame_size = 1024;
+        if (!d->cfg.plain_streams) d->cfg.plain_streams = 4;
+        RTCD_REQUIRE(d->cfg.plain_streams <= 16, "plain_streams must be at most 16");
         int lo_prio = 0, hi_prio = 0;
         cuda_check(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio), "cudaDeviceGetStreamPriorityRange");
         const int prio = std::min(lo_prio, std::max(hi_prio, (int) d->cfg.stream_priority));
@@ -841,17 +917,18 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         cuda_check(cudaEventCreateWithFlags(&d->staged, cudaEventDisableTiming), "cudaEventCreate");
         for (auto& e : d->ev) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         cuda_check(cudaEventCreate(&d->ev_end), "cudaEventCreate");
+        cuda_check(cudaEventCreate(&d->ev_first), "cudaEventCreate");
         if (kind == RTCD_OBS_TO_ROBOT || kind == RTCD_ROBOT_TO_OBS) {
             d->blocks = discrete_persistent_blocks(kind == RTCD_ROBOT_TO_OBS);
             d->blocks_a = d->blocks_a_full = stage_a_blocks(kind == RTCD_ROBOT_TO_OBS);
         }
         apply_launch_shape(d.get());
         d->err.ensure(4);
-        d->stats.ensure(8 * 8);
+        d->stats.ensure(8 * kStatWords);
         d->work.ensure(16);  // [0] work counter, [1] heavy units appended, [2] heavy-pass counter
         d->count.ensure(4);
         cuda_check(cudaMemset(d->err.p, 0, 4), "memset");
-        cuda_check(cudaMemset(d->stats.p, 0, 64), "memset");
+        cuda_check(cudaMemset(d->stats.p, 0, 8 * kStatWords), "memset");
         if (kind == RTCD_QUAD_SWEEP) ensure_weights(d.get(), kWeightsPrebuilt);
         *out = d.release();
     });
@@ -880,11 +957,14 @@ rtcd_status rtcd_detector_destroy(rtcd_detector* d) {
         if (!d) return;
         DeviceScope ds(d->ctx->device);
         cudaStreamSynchronize(d->stream);
+        d->plain_pool.reset();
+        for (rtcd_detector* c : d->plain_clones) rtcd_detector_destroy(c);
         if (d->graph_exec) cudaGraphExecDestroy(d->graph_exec);
         if (d->graph) cudaGraphDestroy(d->graph);
         cudaEventDestroy(d->staged);
         for (auto& e : d->ev) cudaEventDestroy(e);
         cudaEventDestroy(d->ev_end);
+        cudaEventDestroy(d->ev_first);
         cudaStreamDestroy(d->stream);
         delete d;
     });
@@ -1050,13 +1130,16 @@ void check_device_errors(rtcd_detector* d, cudaStream_t s) {
 // One discrete pass over poses [0, n) of d_q.  When `plain`, the item count
 // is read back and the traversal grid sized to it (the upstream shape).
 // The traversal of one direction over the items of the current pass.
+// The first kernel counts into stats bank 0 (and is followed by ev_first,
+// when given), the later passes into bank 1.
 static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t n, bool plain, uint32_t blocks,
-                     uint32_t flags, cudaStream_t s) {
+                     uint32_t flags, cudaStream_t s, cudaEvent_t ev_first) {
     RobotDev& R = d->robot->dev;
     const uint32_t L = R.n_links;
     cuda_check(cudaMemsetAsync(d->work.p, 0, 8, s), "memset");
     if (flags & RTCD_CHECK_FUSED) {
         launch_discrete(r2o, R, d->scene->dev, A, blocks, s);
+        if (ev_first) cuda_check(cudaEventRecord(ev_first, s), "event");
         return;
     }
     // stage A (+ B) -> heavy pass -> the thread-per-item kernel over items whose candidates overflowed
@@ -1102,20 +1185,25 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
     }
     uint32_t ba = plain ? std::max<uint32_t>(1, blocks * kTravThreads / (kStageAWarps * 32)) : d->blocks_a;
     const uint32_t share = d->cfg.residency_percent ? d->cfg.residency_percent : 100;
+    WaveArgs W1 = W;  // the later passes count into bank 1
+    W1.d.stats = A.stats + kStatBank;
     if (fused_form) {
         const bool packets = d->cfg.stage_b_form == 4;
         const uint32_t full = stage_ab_blocks(r2o, packets, d->scene->dev);
         launch_stage_ab(r2o, packets, R, d->scene->dev, W, plain ? std::min(ba, full) : std::max(1u, full * share / 100),
                         s);
+        if (ev_first) cuda_check(cudaEventRecord(ev_first, s), "event");
         // the rest of the crowded items' descents, the one-lane pass over the candidates they
         // deferred, then the heavy pass
-        launch_subtree(r2o, R, d->scene->dev, W, share, s);
-        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, false, s);
+        launch_subtree(r2o, R, d->scene->dev, W1, share, s);
+        launch_stage_b(r2o, R, d->scene->dev, W1, d->blocks_b, d->threads, share, false, s);
     } else {
         launch_stage_a(r2o, R, d->scene->dev, W, std::min(ba, d->blocks_a), s);
-        launch_stage_b(r2o, R, d->scene->dev, W, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
+        if (ev_first) cuda_check(cudaEventRecord(ev_first, s), "event");
+        launch_stage_b(r2o, R, d->scene->dev, W1, d->blocks_b, d->threads, share, d->cfg.stage_b_form == 2, s);
     }
     DiscreteArgs F = A;
+    F.stats = A.stats + kStatBank;
     F.items = d->overflow_items.as<uint32_t>();  // item words
     F.link_major = 0;
     F.n_items = wc + 1;
@@ -1145,7 +1233,8 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
     if (flags & RTCD_CHECK_NO_CULL) {
         launch_all_items(R, n, d->items.as<uint32_t>(), d->count.as<uint32_t>(), s);
     } else {
-        launch_cull(R, d->scene->dev, d->T.as<float4>(), n, d->mask.as<uint8_t>(), true, s);
+        launch_cull(R, d->scene->dev, d->T.as<float4>(), n, d->mask.as<uint8_t>(), true, d->stats.as<unsigned long long>(),
+                    s);
         select_u8(d->mask.as<uint8_t>(), n * L, d->items.as<uint32_t>(), d->count.as<uint32_t>(), d->scan,
                   d->err.as<uint32_t>(), s);
     }
@@ -1185,7 +1274,7 @@ void discrete_pass(rtcd_detector* d, const float* d_q, uint32_t n, uint32_t* d_h
         DiscreteArgs Ad = A;
         Ad.counts = (counts && !r2o) ? d_counts : nullptr;
         Ad.edge_bits = (counts && r2o) ? d_bits : nullptr;
-        traverse(d, r2o, Ad, n, plain, blocks, flags, s);
+        traverse(d, r2o, Ad, n, plain, blocks, flags, s, timed && k == 0 ? d->ev_first : nullptr);
         if (counts && r2o) launch_popcount_rows(d_bits, A.edge_words, n, d_counts, s);
     }
     if (d_contain) launch_contain(R, d->scene->dev, A, d_contain, s);
@@ -1234,12 +1323,47 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
     }
     d->last_items = 0;
     if (flags & RTCD_CHECK_PLAIN) {
-        uint32_t fs = d->cfg.frame_size;
-        for (uint32_t start = 0; start < n; start += fs) {
-            uint32_t m = std::min(fs, n - start);
-            discrete_pass(d, d_q + (size_t) start * dof, m, d->pose_hit.as<uint32_t>() + start,
-                          d_counts ? d_counts + start : nullptr, d_bits ? d_bits + (size_t) start * words : nullptr,
-                          d_contain ? d_contain + start : nullptr, flags, true, s);
+        // The upstream check() shape (RTCD/CollisionDetector/CollisionDetector.h:354-433): frames of
+        // frame_size poses, frame f on stream f % plain_streams, each stream driven by its own host
+        // thread; a frame reads its culled item count back to the host before its traversal (the
+        // upstream compaction round trip, RTCD/Robot/batchRayRobot.h:467); after every group of
+        // plain_streams frames the call waits for the group's streams.
+        const uint32_t fs = d->cfg.frame_size, ns = d->cfg.plain_streams;
+        if (d->plain_clones.size() != ns) {
+            d->plain_pool.reset();
+            for (rtcd_detector* c : d->plain_clones) rtcd_detector_destroy(c);
+            d->plain_clones.clear();
+            rtcd_config cc = d->cfg;
+            cc.plain_streams = 1;
+            for (uint32_t i = 0; i < ns; ++i) {
+                rtcd_detector* c = nullptr;
+                if (rtcd_detector_create(d->ctx, d->kind, d->robot, d->scene, &cc, &c) != RTCD_OK)
+                    fail(RTCD_ERR_INTERNAL, "plain path: " + g_last_error);
+                d->plain_clones.push_back(c);
+            }
+            d->plain_pool.reset(new PlainPool(ns));
+        }
+        cuda_check(cudaStreamSynchronize(s), "plain staging");  // inputs and cleared outputs ready
+        const int dev = d->ctx->device;
+        for (uint32_t start = 0; start < n; start += fs * ns) {
+            std::vector<std::function<void()>> jobs(ns);
+            for (uint32_t i = 0; i < ns && start + i * fs < n; ++i) {
+                const uint32_t a = start + i * fs, m = std::min(fs, n - a);
+                rtcd_detector* c = d->plain_clones[i];
+                jobs[i] = [=] {
+                    cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+                    c->last_items = 0;
+                    discrete_pass(c, d_q + (size_t) a * dof, m, d->pose_hit.as<uint32_t>() + a,
+                                  d_counts ? d_counts + a : nullptr, d_bits ? d_bits + (size_t) a * words : nullptr,
+                                  d_contain ? d_contain + a : nullptr, flags, true, c->stream);
+                };
+            }
+            d->plain_pool->run(jobs);
+            for (uint32_t i = 0; i < ns && start + i * fs < n; ++i) {
+                rtcd_detector* c = d->plain_clones[i];
+                check_device_errors(c, c->stream);  // waits for the frame's stream
+                d->last_items += c->last_items;
+            }
         }
     } else {
         discrete_pass(d, d_q, n, d->pose_hit.as<uint32_t>(), d_counts, d_bits, d_contain, flags, false, s);
@@ -1329,15 +1453,23 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     const uint32_t* dpo = dwp + (n + 1);
     const uint32_t* dco = dwp + 2 * (n + 1);
     const uint32_t* dpt = dwp + 3 * (n + 1);
-    d->centers.ensure(16ull * total_wp * ns);
+    // the staged light pass runs each trajectory's FK (and fit) in shared memory; when the longest
+    // trajectory does not fit there, centres and control points go through global memory
+    uint32_t max_pieces = 0;
+    for (uint32_t i = 0; i < n; ++i) max_pieces = std::max(max_pieces, piece_off[i + 1] - piece_off[i]);
+    const uint32_t max_nc = quad ? quad_ctrl_count(max_wp) : 0;
+    const bool staged = !d->cfg.sweep_unstaged && sweep_staged_smem(quad, R.n_links, max_wp, max_nc, max_pieces) != 0;
     const bool timed = (flags & RTCD_CHECK_TIMING) != 0;
     d->timed = timed;
     if (timed) cuda_check(cudaEventRecord(d->ev[0], s), "event");
-    launch_fk_spheres(R, d_q, total_wp, d->centers.as<float4>(), s);
-    if (quad) {
-        d->ctrl.ensure(16ull * ctrl_total * ns);
-        launch_fit(d->centers.as<float4>(), dwp, dco, d->W.as<float>(), d->W_off.as<uint32_t>(), n, ns,
-                   d->ctrl.as<float4>(), s);
+    if (!staged) {
+        d->centers.ensure(16ull * total_wp * ns);
+        launch_fk_spheres(R, d_q, total_wp, d->centers.as<float4>(), s);
+        if (quad) {
+            d->ctrl.ensure(16ull * ctrl_total * ns);
+            launch_fit(d->centers.as<float4>(), dwp, dco, d->W.as<float>(), d->W_off.as<uint32_t>(), n, ns,
+                       d->ctrl.as<float4>(), s);
+        }
     }
     d->pose_hit.ensure(4ull * n);
     cuda_check(cudaMemsetAsync(d->pose_hit.p, 0, 4ull * n, s), "memset");
@@ -1353,8 +1485,14 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     }
     cuda_check(cudaMemsetAsync(d->work.p, 0, 12, s), "memset");
     SweepArgs A{};
-    A.centers = d->centers.as<float4>();
-    A.ctrl = quad ? d->ctrl.as<float4>() : nullptr;
+    A.centers = staged ? nullptr : d->centers.as<float4>();
+    A.ctrl = quad && !staged ? d->ctrl.as<float4>() : nullptr;
+    A.q = d_q;
+    A.W = d->W.as<float>();
+    A.W_off = d->W_off.as<uint32_t>();
+    A.max_wp = max_wp;
+    A.max_nc = max_nc;
+    A.max_pieces = max_pieces;
     A.traj_piece_off = dpo;
     A.traj_wp_off = dwp;
     A.traj_ctrl_off = dco;
@@ -1378,9 +1516,9 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
                                                               : 16u;
     if (A.light_steps) {
         // room for every unit (near dense geometry most units of a piece can spill)
-        const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns, 1024), 1u << 24);
-        d->heavy.ensure(4ull * cap);
-        A.heavy = d->heavy.as<uint32_t>();
+        const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns, 1024), 1u << 20);
+        d->heavy.ensure(sizeof(SweepRec) * cap);
+        A.heavy = d->heavy.as<SweepRec>();
         A.heavy_cap = cap;
         A.heavy_count = d->work.as<uint32_t>() + 1;
         A.heavy_work = d->work.as<uint32_t>() + 2;
@@ -1392,8 +1530,11 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     }
     A.binary_tree = d->cfg.stage_b_form == 1 ? 1 : 0;
     if (A.total_units)
-        launch_sweep(A.surface ? scene_loop(d->scene) : d->scene->dev, A, d->blocks, d->threads,
-                     d->cfg.residency_percent ? d->cfg.residency_percent : 100, s);
+        launch_sweep(A.surface ? scene_loop(d->scene) : d->scene->dev, R, A, d->blocks, d->threads,
+                     d->cfg.residency_percent ? d->cfg.residency_percent : 100, staged, s,
+                     timed ? d->ev_first : nullptr);
+    else if (timed)
+        cuda_check(cudaEventRecord(d->ev_first, s), "event");
     if (timed) cuda_check(cudaEventRecord(d->ev[3], s), "event");
     // outputs
     uint8_t* d_flags = (host || !flags_out) ? (d->flags.ensure(n), d->flags.as<uint8_t>()) : flags_out;
@@ -1437,7 +1578,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
         d->timed = false;
         d->timed_total_only = false;
         d->last_stream = s;
-        if (n) cuda_check(cudaMemsetAsync(d->stats.p, 0, 64, s), "stats reset");
+        if (n) cuda_check(cudaMemsetAsync(d->stats.p, 0, 8 * kStatWords, s), "stats reset");
         if (n == 0) return;
         if (flags & RTCD_CHECK_GRAPH) {
             const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
@@ -1598,15 +1739,20 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
         std::lock_guard<std::mutex> lock(d->mu);
         DeviceScope ds(d->ctx->device);
         std::memset(out, 0, sizeof(*out));
-        unsigned long long st[8] = {0};
+        unsigned long long sb[kStatWords] = {0}, st[kStatBank] = {0};
         uint32_t cnt = 0;
         cudaStream_t s = d->last_stream ? d->last_stream : d->stream;
-        cuda_check(cudaMemcpyAsync(st, d->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s), "stats");
+        cuda_check(cudaMemcpyAsync(sb, d->stats.p, sizeof(sb), cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, s), "stats");
         uint32_t cand = 0;
         if (d->wave_counts.p)
             cuda_check(cudaMemcpyAsync(&cand, d->wave_counts.p, 4, cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaStreamSynchronize(s), "stats sync");
+        for (int k = 0; k < kStatBank; ++k) st[k] = sb[k] + sb[kStatBank + k];
+        out->first_node_tests = sb[7];
+        out->first_exact_tests = sb[4];
+        out->cull_sphere_tests = sb[kStatCullSpheres];
+        out->cull_sat_tests = sb[kStatCullSats];
         out->fp64_retests = st[0];
         // discrete: the candidate buffer's count, or the fused form's in-warp count
         out->candidates = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) ? (st[6] ? st[6] : cand) : st[5];
@@ -1617,6 +1763,7 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
             cuda_check(cudaEventElapsedTime(&out->ms_prepare, d->ev[0], d->ev[1]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_cull, d->ev[1], d->ev[2]), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_traverse, d->ev[2], d->ev[3]), "elapsed");
+            cuda_check(cudaEventElapsedTime(&out->ms_first_pass, d->ev[2], d->ev_first), "elapsed");
             cuda_check(cudaEventElapsedTime(&out->ms_total, d->ev[0], d->ev_end), "elapsed");
         } else if (d->timed_total_only) {
             cuda_check(cudaEventElapsedTime(&out->ms_total, d->ev[0], d->ev_end), "elapsed");
@@ -1766,7 +1913,7 @@ rtcd_status rtcd_check_edges(rtcd_detector* d, const float* nodes_dev, uint32_t 
             d->graph_exec = nullptr;
             d->graph = nullptr;
         }
-        cuda_check(cudaMemsetAsync(d->stats.p, 0, 64, s), "stats reset");
+        cuda_check(cudaMemsetAsync(d->stats.p, 0, 8 * kStatWords, s), "stats reset");
         const uint32_t dof = d->robot->dof;
         const uint32_t total = n_edges * n_wp;
         d->edge_q.ensure(4ull * total * dof);

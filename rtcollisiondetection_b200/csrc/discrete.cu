@@ -140,7 +140,7 @@ __device__ __forceinline__ uint32_t item_word(const DiscreteArgs& A, uint32_t n_
 // bounding-sphere reject before the full test.
 __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __restrict__ sobb, uint32_t n_obs,
                                              const float4* __restrict__ T, uint32_t n, uint8_t* __restrict__ mask,
-                                             bool link_major) {
+                                             bool link_major, unsigned long long* stats) {
     __shared__ float s_obb[kCullChunk * 16];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t pose = i / R.n_links, link = i % R.n_links;
@@ -152,6 +152,7 @@ __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __r
         arad = sqrtf(dot(A.h, A.h)) + 2e-5f;
     }
     bool hit = false;
+    unsigned long long n_sphere = 0, n_sat = 0;  // bounding-sphere tests, then the SATs they let through
     for (uint32_t base = 0; base < n_obs; base += kCullChunk) {
         uint32_t m = min((uint32_t) kCullChunk, n_obs - base);
         __syncthreads();
@@ -162,7 +163,9 @@ __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __r
                 const float* B = s_obb + o * 16;
                 f3 d = mk(B[0], B[1], B[2]) - A.c;
                 float rr = arad + B[15];
+                ++n_sphere;
                 if (dot(d, d) > rr * rr) continue;
+                ++n_sat;
                 if (obb_overlap(A, B)) {
                     hit = true;
                     break;
@@ -171,13 +174,15 @@ __global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __r
         }
     }
     if (pose < n) mask[link_major ? (size_t) link_slot(link, R.n_links) * n + pose : i] = hit ? 1 : 0;
+    warp_count(stats + kStatCullSpheres, n_sphere);
+    warp_count(stats + kStatCullSats, n_sat);
 }
 
 void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, bool link_major,
-                 cudaStream_t s) {
+                 unsigned long long* d_stats, cudaStream_t s) {
     uint32_t total = n * R.n_links;
     if (!total) return;
-    k_cull<<<(total + 255) / 256, 256, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask, link_major);
+    k_cull<<<(total + 255) / 256, 256, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask, link_major, d_stats);
     cuda_check(cudaGetLastError(), "k_cull");
 }
 

@@ -123,7 +123,7 @@ void launch_fk_poses(const Chain& ch, const float* d_q, uint32_t n, float4* d_T,
 // link_major: the mask (and so the compacted items) in link order, every pose's
 // last link before any pose's next-to-last one (item_word decodes it).
 void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32_t n, uint8_t* d_mask, bool link_major,
-                 cudaStream_t s);
+                 unsigned long long* d_stats, cudaStream_t s);
 void launch_all_items(const RobotDev& R, uint32_t n, uint32_t* d_items, uint32_t* d_count, cudaStream_t s);
 void launch_discrete(bool robot_to_obs, const RobotDev& R, const SceneDev& S, const DiscreteArgs& A, uint32_t blocks,
                      cudaStream_t s);
@@ -136,6 +136,14 @@ void launch_contain(const RobotDev& R, const SceneDev& S, const DiscreteArgs& A,
 uint32_t discrete_persistent_blocks(bool robot_to_obs);
 
 // ---- sweeps
+// A sweep unit handed to the heavy pass: its geometry (linear: capsule axis
+// P0-P1; quadratic: Bezier piece P0 P1 P2, or an end sphere), radius, owner.
+struct SweepRec {
+    float4 P0, P1, P2;
+    float r;
+    uint32_t traj, piece_g, pad;
+};
+
 struct SweepArgs {
     const float4* centers;     // [waypoint][sphere] world centre xyz, radius w
     const float4* ctrl;        // [control point][sphere] (quadratic) or NULL
@@ -159,10 +167,16 @@ struct SweepArgs {
     int want_pieces;
     uint32_t light_steps;      // visits before a unit moves to the heavy pass; 0 = no heavy pass
     int binary_tree;           // light pass on the binary edge tree (else the 4-wide one where the scene allows)
-    uint32_t* heavy;           // [heavy_cap] units handed to the heavy pass
+    SweepRec* heavy;           // [heavy_cap] units handed to the heavy pass
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // units appended (may exceed heavy_cap: those stayed in the light pass)
     uint32_t* heavy_work;      // heavy-pass work counter
+    // the staged light pass (k_sweep_traj): a block takes one trajectory at a time from work_counter,
+    // runs its FK (and quadratic fit) into shared memory and its units from there
+    const float* q;            // [waypoint][dof] joint values
+    const float* W;            // quadratic fit tables, W_off[n] = the table of n waypoints
+    const uint32_t* W_off;
+    uint32_t max_wp, max_nc, max_pieces;  // largest trajectory of the batch (shared-memory sizing)
 };
 
 void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s);
@@ -170,8 +184,15 @@ void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_
                 const uint32_t* d_W_off, uint32_t n_traj, uint32_t n_spheres, float4* d_ctrl, cudaStream_t s);
 // The light pass on `blocks` blocks of `threads`, then (when A.light_steps)
 // the heavy pass on heavy_share percent of its full persistent grid.
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, uint32_t heavy_share,
-                  cudaStream_t s);
+// ev_light (optional) is recorded between the two passes.  The heavy pass
+// counts into the second stats bank (A.stats + kStatBank).  staged: the
+// light pass stages each trajectory's FK (and fit) in shared memory
+// (k_sweep_traj) instead of reading A.centers / A.ctrl.
+void launch_sweep(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, uint32_t threads,
+                  uint32_t heavy_share, bool staged, cudaStream_t s, cudaEvent_t ev_light = nullptr);
+// Shared memory of the staged light pass for a batch; 0 when it does not fit (the caller then
+// computes the centres and control points in global memory and runs the unstaged light pass).
+size_t sweep_staged_smem(bool quad, uint32_t n_links, uint32_t max_wp, uint32_t max_nc, uint32_t max_pieces);
 uint32_t sweep_persistent_blocks(bool quad);
 uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads);  // threads: 64, 128 or 256
 

@@ -57,6 +57,16 @@ __device__ __forceinline__ void load_node(const float4* __restrict__ nodes, uint
 // when the warp's total is zero (per-thread atomics on one address at the
 // end of a large grid serialise in L2 for a noticeable time).  Every lane of
 // the warp must call it; per-lane counts fit 32 bits.
+// Work counters of a check (64-bit words on the device).  Two banks of
+// kStatBank words with the same layout: bank 0 for the first traversal kernel
+// of a check (the fused or stage-A discrete kernel, the light sweep pass) and
+// the cull, bank 1 for the passes that follow (subtree, deferred and heavy
+// candidates, the overflow fallback, the heavy sweep pass).
+constexpr int kStatBank = 16;
+constexpr int kStatWords = 2 * kStatBank;
+constexpr int kStatCullSpheres = 8;   // bank 0: bounding-sphere tests of the OBB cull
+constexpr int kStatCullSats = 9;      // bank 0: 15-axis SATs the cull evaluated
+
 __device__ __forceinline__ void warp_count(unsigned long long* p, unsigned long long v) {
     const unsigned total = __reduce_add_sync(0xffffffffu, (unsigned) v);
     if ((threadIdx.x & 31) == 0 && total) atomicAdd(p, (unsigned long long) total);

@@ -305,6 +305,24 @@ struct SweepUnit {
     uint32_t traj, piece_g;
 };
 
+__device__ __forceinline__ void store_rec(SweepRec* r, const SweepUnit& U) {
+    r->P0 = U.P0;
+    r->P1 = U.P1;
+    r->P2 = U.P2;
+    r->r = U.r;
+    r->traj = U.traj;
+    r->piece_g = U.piece_g;
+}
+
+__device__ __forceinline__ void load_rec(const SweepRec* r, SweepUnit& U) {
+    U.P0 = r->P0;
+    U.P1 = r->P1;
+    U.P2 = r->P2;
+    U.r = r->r;
+    U.traj = r->traj;
+    U.piece_g = r->piece_g;
+}
+
 template <bool QUAD>
 __device__ __forceinline__ bool load_unit(const SweepArgs& A, uint32_t u, SweepUnit& U) {
     U.piece_g = u / A.n_spheres;
@@ -381,6 +399,7 @@ __device__ __forceinline__ bool cull_box(const SweepCull& c, const Box& b, float
     return in;
 }
 
+constexpr size_t kSweepStagedMaxSmem = 96 * 1024;  // largest shared staging of one trajectory (per block)
 constexpr float kSweepBand = 2e-6f;  // |d - r| below this (+ 1e-6 r) is re-tested in FP64
 
 // FP32 distance from the segment pq to the unit's Bezier piece, bracketed.
@@ -563,6 +582,86 @@ __device__ __forceinline__ bool leaf_hit_surface(const float4* __restrict__ ep, 
     return surface_retest_f64<QUAD>(ea, eb, U.P0, U.P1, U.P2, r);
 }
 
+// One lane's descent to its next leaf over the obstacle-edge tree (WIDE: the
+// 4-wide copy, children pushed far to near; else the binary tree, the child
+// met first along the chord visited first).  Returns the leaf, or kNone when
+// the stack ran empty.
+template <bool QUAD, bool WIDE>
+__device__ __forceinline__ uint32_t sweep_descend(const float4* __restrict__ en, uint32_t* st, int& sp, uint32_t& steps,
+                                                  const SweepCull& c, unsigned long long& n_node, uint32_t* err) {
+    uint32_t leaf = kNone;
+    while (sp > 0) {
+        const uint32_t ref = st[--sp];
+        ++steps;
+        if (ref & kLeaf) {
+            leaf = ref & ~kLeaf;
+            break;
+        }
+        if (WIDE) {
+            const float4* rec = en + 2ull * kWide * ref;
+            float4 ra[kWide], rb[kWide];
+#pragma unroll
+            for (int j = 0; j < kWide; ++j) {
+                ra[j] = __ldg(rec + 2 * j);
+                rb[j] = __ldg(rec + 2 * j + 1);
+            }
+            // key = entry parameter along the chord, 2 (past every hit's) for a miss
+            float t[kWide];
+            uint32_t cr[kWide];
+#pragma unroll
+            for (int j = 0; j < kWide; ++j) {
+                cr[j] = __float_as_uint(rb[j].z);
+                t[j] = 2.f;
+                if (cr[j] != kNone) {
+                    ++n_node;
+                    Box bx;
+                    bx.lo[0] = ra[j].x; bx.lo[1] = ra[j].y; bx.lo[2] = ra[j].z;
+                    bx.hi[0] = ra[j].w; bx.hi[1] = rb[j].x; bx.hi[2] = rb[j].y;
+                    float te;
+                    if (cull_box<QUAD>(c, bx, te)) t[j] = te;
+                }
+            }
+            // descending keys (a 4-input sorting network): misses first, then far to near
+            auto cx = [&](int i, int k) {
+                if (t[i] < t[k]) {
+                    const float tt = t[i]; t[i] = t[k]; t[k] = tt;
+                    const uint32_t rt = cr[i]; cr[i] = cr[k]; cr[k] = rt;
+                }
+            };
+            cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+            if (sp + kWide > kStack) {  // cannot happen: the wide form runs only on shallow enough trees
+                atomicOr(err, kErrStack);
+                sp = 0;
+            } else {
+#pragma unroll
+                for (int j = 0; j < kWide; ++j)
+                    if (t[j] < 2.f) st[sp++] = cr[j];
+            }
+            continue;
+        }
+        Box bl, br;
+        uint32_t rl, rr;
+        load_node(en, ref, bl, br, rl, rr);
+        n_node += 2;
+        float tl, tr;
+        bool hr = cull_box<QUAD>(c, br, tr), hl = cull_box<QUAD>(c, bl, tl);
+        if (sp + 2 > kStack) {
+            atomicOr(err, kErrStack);
+            hr = hl = false;
+            sp = 0;
+        }
+        // the child met first along the chord is visited first
+        if (hr && hl && tr < tl) {
+            st[sp++] = rl;
+            st[sp++] = rr;
+        } else {
+            if (hr) st[sp++] = rr;
+            if (hl) st[sp++] = rl;
+        }
+    }
+    return leaf;
+}
+
 // Light pass: one lane per unit, "while-while" (Aila and Laine 2009): lanes
 // without a unit take their next one, every lane descends to its next leaf,
 // then the warp's leaf tests run together.  A unit still open after
@@ -592,7 +691,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
     uint32_t st[kStack];
     int sp = 0;
     bool busy = false;
-    uint32_t cur = 0, steps = 0, checked = 0, u_hits = 0;
+    uint32_t steps = 0, checked = 0, u_hits = 0;
     SweepUnit U;
     SweepCull c;
     U.traj = U.piece_g = 0;
@@ -619,7 +718,6 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
             st[0] = root;
             sp = 1;
             busy = true;
-            cur = u;
             steps = 0;
             checked = 0;
             u_hits = 0;
@@ -633,75 +731,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
             checked = steps;
             if (A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj)) sp = 0;
         }
-        while (sp > 0) {
-            const uint32_t ref = st[--sp];
-            ++steps;
-            if (ref & kLeaf) {
-                leaf = ref & ~kLeaf;
-                break;
-            }
-            if (WIDE) {
-                const float4* rec = en + 2ull * kWide * ref;
-                float4 ra[kWide], rb[kWide];
-#pragma unroll
-                for (int j = 0; j < kWide; ++j) {
-                    ra[j] = __ldg(rec + 2 * j);
-                    rb[j] = __ldg(rec + 2 * j + 1);
-                }
-                // key = entry parameter along the chord, 2 (past every hit's) for a miss
-                float t[kWide];
-                uint32_t cr[kWide];
-#pragma unroll
-                for (int j = 0; j < kWide; ++j) {
-                    cr[j] = __float_as_uint(rb[j].z);
-                    t[j] = 2.f;
-                    if (cr[j] != kNone) {
-                        ++n_node;
-                        Box bx;
-                        bx.lo[0] = ra[j].x; bx.lo[1] = ra[j].y; bx.lo[2] = ra[j].z;
-                        bx.hi[0] = ra[j].w; bx.hi[1] = rb[j].x; bx.hi[2] = rb[j].y;
-                        float te;
-                        if (cull_box<QUAD>(c, bx, te)) t[j] = te;
-                    }
-                }
-                // descending keys (a 4-input sorting network): misses first, then far to near
-                auto cx = [&](int i, int k) {
-                    if (t[i] < t[k]) {
-                        const float tt = t[i]; t[i] = t[k]; t[k] = tt;
-                        const uint32_t rt = cr[i]; cr[i] = cr[k]; cr[k] = rt;
-                    }
-                };
-                cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
-                if (sp + kWide > kStack) {  // cannot happen: the wide form runs only on shallow enough trees
-                    atomicOr(A.err, kErrStack);
-                    sp = 0;
-                } else {
-#pragma unroll
-                    for (int j = 0; j < kWide; ++j)
-                        if (t[j] < 2.f) st[sp++] = cr[j];
-                }
-                continue;
-            }
-            Box bl, br;
-            uint32_t rl, rr;
-            load_node(en, ref, bl, br, rl, rr);
-            n_node += 2;
-            float tl, tr;
-            bool hr = cull_box<QUAD>(c, br, tr), hl = cull_box<QUAD>(c, bl, tl);
-            if (sp + 2 > kStack) {
-                atomicOr(A.err, kErrStack);
-                hr = hl = false;
-                sp = 0;
-            }
-            // the child met first along the chord is visited first
-            if (hr && hl && tr < tl) {
-                st[sp++] = rl;
-                st[sp++] = rr;
-            } else {
-                if (hr) st[sp++] = rr;
-                if (hl) st[sp++] = rl;
-            }
-        }
+        leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err);
         if (leaf != kNone) {
             ++n_leaf;
             if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots) : leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
@@ -719,7 +749,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
         if (sp > 0 && steps > budget) {
             const uint32_t slot = atomicAdd(A.heavy_count, 1u);
             if (slot < A.heavy_cap) {
-                A.heavy[slot] = cur;
+                store_rec(A.heavy + slot, U);
                 busy = false;
                 continue;
             }
@@ -728,6 +758,172 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
         if (sp == 0) {
             busy = false;
             if (u_hits) atomicAdd(A.counts + U.traj, u_hits);
+        }
+    }
+    warp_count(A.stats + 1, n_acc);
+    warp_count(A.stats + 2, n_skip);
+    warp_count(A.stats + 4, n_leaf);
+    warp_count(A.stats + 5, n_roots);
+    warp_count(A.stats + 7, n_node);
+}
+
+// Staged light pass: one trajectory per block at a time.  The block takes a
+// trajectory from A.work_counter, runs FK for its waypoints into shared
+// memory (one thread per waypoint, link transforms [waypoint][link][12]) and,
+// for the quadratic sweep, the least-squares fit there as well: the control
+// point of sphere s is C_k = (sum_t W_n[k][t] T_t[link(s)]) p_s, so the fit
+// runs once per (control point, link) on the 3x4 transforms instead of once
+// per (control point, sphere) on the centres (upstream genCtrlPtsKern,
+// RTCD/Robot/sweptVolume.cu:22-83, fits the sphere centres).  Lanes then take
+// the trajectory's (piece, sphere) units from a shared counter and build each
+// unit's centres from the staged transforms: no sphere centre or control
+// point goes through global memory.  A hit sets the piece's (or the
+// trajectory's) flag in shared memory, which every lane on it checks at
+// every visit.  Same descent, leaf tests, light budget and heavy hand-off as
+// k_sweep.
+template <bool QUAD, int BLOCK, bool WIDE, bool SURF>
+__global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOCK)
+    k_sweep_traj(const SceneDev S, const RobotDev R, const SweepArgs A) {
+    extern __shared__ float4 s_dyn[];
+    const uint32_t L = R.n_links, ns = R.n_spheres, L12 = L * 12;
+    float* s_T = reinterpret_cast<float*>(s_dyn);                   // [max_wp][L][12]
+    float* s_C = s_T + (size_t) A.max_wp * L12;                     // [max_nc][L][12] (quadratic)
+    volatile uint32_t* s_piece = reinterpret_cast<volatile uint32_t*>(s_C + (QUAD ? (size_t) A.max_nc * L12 : 0));
+    __shared__ uint32_t s_tr, s_next;
+    __shared__ volatile uint32_t s_hit;
+    const float4* __restrict__ en = WIDE ? S.edge_wide : S.edge_nodes;
+    const float4* __restrict__ ep = S.edge_prims;
+    const uint32_t root = WIDE ? S.edge_wide_root : S.edge_root;
+    uint32_t st[kStack];
+    unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0, n_node = 0;
+    const uint32_t budget = A.light_steps ? A.light_steps : 0xFFFFFFFFu;
+    const int dof = R.chain.dof;
+
+    while (true) {
+        __syncthreads();  // the previous trajectory's shared state is no longer read
+        if (threadIdx.x == 0) {
+            s_tr = atomicAdd(A.work_counter, 1u);
+            s_next = 0;
+            s_hit = 0;
+        }
+        __syncthreads();
+        const uint32_t tr = s_tr;
+        if (tr >= A.n_traj) break;
+        const uint32_t w0 = A.traj_wp_off[tr], nwp = A.traj_wp_off[tr + 1] - w0;
+        const uint32_t p0 = A.traj_piece_off[tr], np = A.traj_piece_off[tr + 1] - p0;
+        const uint32_t nc = QUAD ? A.traj_ctrl_off[tr + 1] - A.traj_ctrl_off[tr] : 0;
+        if (nwp > A.max_wp || np > A.max_pieces || (QUAD && nc + 0u * nwp > A.max_nc)) {  // sized by the host
+            if (threadIdx.x == 0) atomicOr(A.err, kErrRange);
+            continue;
+        }
+        for (uint32_t w = threadIdx.x; w < nwp; w += BLOCK) {
+            float qq[kMaxDof];
+            for (int k = 0; k < dof; ++k) qq[k] = __ldg(A.q + (size_t) (w0 + w) * dof + k);
+            fk_chain(R.chain, qq, reinterpret_cast<float(*)[12]>(s_T + (size_t) w * L12));
+        }
+        for (uint32_t k = threadIdx.x; k < np; k += BLOCK) s_piece[k] = 0;
+        __syncthreads();
+        if (QUAD) {
+            const float* Wn = A.W + A.W_off[nwp];
+            for (uint32_t idx = threadIdx.x; idx < nc * L12; idx += BLOCK) {
+                const uint32_t k = idx / L12, le = idx - k * L12;
+                const float* wr = Wn + (size_t) k * nwp;
+                float acc = 0.f;
+                for (uint32_t t = 0; t < nwp; ++t) acc = fmaf(__ldg(wr + t), s_T[(size_t) t * L12 + le], acc);
+                s_C[idx] = acc;
+            }
+            __syncthreads();
+        }
+        const uint32_t units = np * ns;
+        // world centre of sphere s under a staged 3x4 transform M
+        auto at = [](const float* M, float4 p) {
+            return make_float4(M[0] * p.x + M[1] * p.y + M[2] * p.z + M[3], M[4] * p.x + M[5] * p.y + M[6] * p.z + M[7],
+                               M[8] * p.x + M[9] * p.y + M[10] * p.z + M[11], p.w);
+        };
+        int sp = 0;
+        bool busy = false;
+        uint32_t steps = 0, u_hits = 0, piece = 0;
+        SweepUnit U;
+        SweepCull c;
+        U.traj = tr;
+        U.piece_g = p0;
+        while (true) {
+            while (!busy) {
+                const uint32_t u = atomicAdd(&s_next, 1u);
+                if (u >= units) break;
+                piece = u / ns;
+                const uint32_t s = u - piece * ns;
+                if (!A.want_counts && (A.want_pieces ? s_piece[piece] : s_hit)) {
+                    ++n_skip;
+                    continue;
+                }
+                const float4 sp4 = __ldg(R.spheres + s);
+                const uint32_t link = __ldg(R.sphere_link + s);
+                U.piece_g = p0 + piece;
+                U.r = sp4.w;
+                if constexpr (!QUAD) {
+                    U.P0 = at(s_T + (size_t) (piece * L + link) * 12, sp4);
+                    U.P1 = at(s_T + (size_t) ((piece + 1) * L + link) * 12, sp4);
+                    U.P2 = U.P1;
+                } else if (piece + 2 < nc) {
+                    const float4 a = at(s_C + (size_t) (piece * L + link) * 12, sp4);
+                    const float4 b = at(s_C + (size_t) ((piece + 1) * L + link) * 12, sp4);
+                    const float4 cc = at(s_C + (size_t) ((piece + 2) * L + link) * 12, sp4);
+                    U.P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), sp4.w);
+                    U.P1 = b;
+                    U.P2 = make_float4(0.5f * (b.x + cc.x), 0.5f * (b.y + cc.y), 0.5f * (b.z + cc.z), sp4.w);
+                } else {  // the start / end sphere
+                    const uint32_t w = (piece + 2 == nc) ? 0 : nwp - 1;
+                    U.P0 = at(s_T + (size_t) (w * L + link) * 12, sp4);
+                    U.P1 = U.P0;
+                    U.P2 = U.P0;
+                }
+                if (root == kNone) continue;
+                make_cull<QUAD>(U, c);
+                st[0] = root;
+                sp = 1;
+                busy = true;
+                steps = 0;
+                u_hits = 0;
+                ++n_acc;
+            }
+            if (!busy) break;
+            // flags only: drop the unit once its piece (or trajectory) is decided
+            if (!A.want_counts && (A.want_pieces ? s_piece[piece] : s_hit)) sp = 0;
+            const uint32_t leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err);
+            if (leaf != kNone) {
+                ++n_leaf;
+                if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots)
+                         : leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
+                    if (A.want_pieces) {
+                        s_piece[piece] = 1u;
+                        atomicExch(A.piece_hit + U.piece_g, 1u);
+                    }
+                    if (A.want_counts) {
+                        A.traj_hit[tr] = 1u;
+                        ++u_hits;
+                    } else {
+                        if (!s_hit) {
+                            s_hit = 1u;
+                            atomicExch(A.traj_hit + tr, 1u);
+                        }
+                        sp = 0;  // this unit is decided
+                    }
+                }
+            }
+            if (sp > 0 && steps > budget) {
+                const uint32_t slot = atomicAdd(A.heavy_count, 1u);
+                if (slot < A.heavy_cap) {
+                    store_rec(A.heavy + slot, U);
+                    busy = false;
+                    continue;
+                }
+                steps = 0;  // the heavy list is full: finish the unit here
+            }
+            if (sp == 0) {
+                busy = false;
+                if (u_hits) atomicAdd(A.counts + tr, u_hits);
+            }
         }
     }
     warp_count(A.stats + 1, n_acc);
@@ -761,10 +957,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
         h = __shfl_sync(0xffffffffu, h, 0);
         if (h >= n_heavy) break;
         SweepUnit U;
-        if (!load_unit<QUAD>(A, A.heavy[h], U)) {
-            if (lane == 0) atomicOr(A.err, kErrRange);
-            continue;
-        }
+        load_rec(A.heavy + h, U);
         SweepCull c;
         make_cull<QUAD>(U, c);
         if (lane == 0) fr[0] = S.edge_root;
@@ -848,6 +1041,11 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
     warp_count(A.stats + 7, n_node);
 }
 
+size_t sweep_staged_smem(bool quad, uint32_t n_links, uint32_t max_wp, uint32_t max_nc, uint32_t max_pieces) {
+    const size_t bytes = 48ull * n_links * (max_wp + (quad ? max_nc : 0)) + 4ull * max_pieces;
+    return bytes <= kSweepStagedMaxSmem ? ((bytes + 15) & ~size_t(15)) : 0;
+}
+
 template <bool QUAD>
 static int sweep_per_sm(int threads) {
     int per_sm = 0;  // the wide and binary forms (and both semantics) share their register caps
@@ -877,10 +1075,41 @@ static uint32_t heavy_blocks() {
     return blocks;
 }
 
+// The staged light pass at `threads` per block with `smem` bytes of shared
+// memory per block, on at most as many blocks as fit.
+template <bool QUAD, int BLOCK, bool WIDE, bool SURF>
+static void launch_staged(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, size_t smem,
+                          cudaStream_t s) {
+    auto kern = k_sweep_traj<QUAD, BLOCK, WIDE, SURF>;
+    static bool attr = false;
+    if (!attr) {  // allow up to the largest staged size (set once, outside any capture: the first launch)
+        cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kSweepStagedMaxSmem),
+                   "cudaFuncSetAttribute");
+        attr = true;
+    }
+    int per_sm = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, smem), "occupancy");
+    blocks = std::min<uint32_t>(blocks, (uint32_t) std::max(1, per_sm) * device_sm_count());
+    blocks = std::min<uint32_t>(blocks, std::max<uint32_t>(A.n_traj, 1));
+    kern<<<blocks, BLOCK, smem, s>>>(S, R, A);
+}
+
 template <bool QUAD, bool SURF>
-static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads,
-                           uint32_t heavy_share, cudaStream_t s) {
-    if (S.edge_wide_lane && !A.binary_tree) {
+static void sweep_dispatch(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, uint32_t threads,
+                           uint32_t heavy_share, bool staged, cudaStream_t s, cudaEvent_t ev_light) {
+    const bool wide = S.edge_wide_lane && !A.binary_tree;
+    if (staged) {
+        const size_t smem = sweep_staged_smem(QUAD, R.n_links, A.max_wp, A.max_nc, A.max_pieces);
+        if (wide) {
+            if (threads == 64) launch_staged<QUAD, 64, true, SURF>(S, R, A, blocks, smem, s);
+            else if (threads == 256) launch_staged<QUAD, 256, true, SURF>(S, R, A, blocks, smem, s);
+            else launch_staged<QUAD, 128, true, SURF>(S, R, A, blocks, smem, s);
+        } else {
+            if (threads == 64) launch_staged<QUAD, 64, false, SURF>(S, R, A, blocks, smem, s);
+            else if (threads == 256) launch_staged<QUAD, 256, false, SURF>(S, R, A, blocks, smem, s);
+            else launch_staged<QUAD, 128, false, SURF>(S, R, A, blocks, smem, s);
+        }
+    } else if (wide) {
         if (threads == 64)
             k_sweep<QUAD, 64, true, SURF><<<blocks, 64, 0, s>>>(S, A);
         else if (threads == 256)
@@ -895,25 +1124,28 @@ static void sweep_dispatch(const SceneDev& S, const SweepArgs& A, uint32_t block
         else
             k_sweep<QUAD, 128, false, SURF><<<blocks, 128, 0, s>>>(S, A);
     }
-    cuda_check(cudaGetLastError(), "k_sweep");
+    cuda_check(cudaGetLastError(), staged ? "k_sweep_traj" : "k_sweep");
+    if (ev_light) cuda_check(cudaEventRecord(ev_light, s), "event");
     // the heavy pass stays on the binary tree: for a thin capsule its inner boxes cull more than a
     // wide node's four child boxes (the wide warp descent tested 25-40 % more boxes, measured on
     // the 4,096-trajectory sweeps)
     if (A.light_steps) {
+        SweepArgs H = A;
+        H.stats = A.stats + kStatBank;
         const uint32_t hb = std::max(1u, heavy_blocks<QUAD, SURF>() * heavy_share / 100);
-        k_sweep_heavy<QUAD, SURF><<<hb, kHeavyWarps * 32, 0, s>>>(S, A);
+        k_sweep_heavy<QUAD, SURF><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
         cuda_check(cudaGetLastError(), "k_sweep_heavy");
     }
 }
 
-void launch_sweep(const SceneDev& S, const SweepArgs& A, uint32_t blocks, uint32_t threads, uint32_t heavy_share,
-                  cudaStream_t s) {
+void launch_sweep(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, uint32_t threads,
+                  uint32_t heavy_share, bool staged, cudaStream_t s, cudaEvent_t ev_light) {
     if (A.quad) {
-        if (A.surface) sweep_dispatch<true, true>(S, A, blocks, threads, heavy_share, s);
-        else sweep_dispatch<true, false>(S, A, blocks, threads, heavy_share, s);
+        if (A.surface) sweep_dispatch<true, true>(S, R, A, blocks, threads, heavy_share, staged, s, ev_light);
+        else sweep_dispatch<true, false>(S, R, A, blocks, threads, heavy_share, staged, s, ev_light);
     } else {
-        if (A.surface) sweep_dispatch<false, true>(S, A, blocks, threads, heavy_share, s);
-        else sweep_dispatch<false, false>(S, A, blocks, threads, heavy_share, s);
+        if (A.surface) sweep_dispatch<false, true>(S, R, A, blocks, threads, heavy_share, staged, s, ev_light);
+        else sweep_dispatch<false, false>(S, R, A, blocks, threads, heavy_share, staged, s, ev_light);
     }
 }
 

@@ -65,14 +65,17 @@ class RobotDesc(C.Structure):
 class Config(C.Structure):
     _fields_ = [('frame_size', C.c_uint32), ('traverse_threads', C.c_uint32), ('traverse_blocks_per_sm', C.c_uint32),
                 ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('light_steps', C.c_uint32),
-                ('stage_b_form', C.c_uint32), ('stage_b_chunk', C.c_uint32)]
+                ('stage_b_form', C.c_uint32), ('stage_b_chunk', C.c_uint32), ('plain_streams', C.c_uint32),
+                ('sweep_unstaged', C.c_uint32)]
 
 
 class Stats(C.Structure):
     _fields_ = [('work_items', C.c_uint64), ('culled_items', C.c_uint64), ('fp64_retests', C.c_uint64),
                 ('ms_prepare', C.c_float), ('ms_cull', C.c_float), ('ms_traverse', C.c_float),
                 ('ms_total', C.c_float), ('candidates', C.c_uint64), ('exact_tests', C.c_uint64),
-                ('skipped', C.c_uint64), ('node_tests', C.c_uint64)]
+                ('skipped', C.c_uint64), ('node_tests', C.c_uint64), ('ms_first_pass', C.c_float),
+                ('reserved0', C.c_uint32), ('first_node_tests', C.c_uint64), ('first_exact_tests', C.c_uint64),
+                ('cull_sphere_tests', C.c_uint64), ('cull_sat_tests', C.c_uint64)]
 
 
 _lib = None
@@ -364,7 +367,8 @@ class Detector:
     """One detector of one kind over a robot and a scene."""
 
     def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
-                 stream_priority=0, residency_percent=0, light_steps=0, stage_b_form=0, stage_b_chunk=0):
+                 stream_priority=0, residency_percent=0, light_steps=0, stage_b_form=0, stage_b_chunk=0,
+                 plain_streams=0, sweep_unstaged=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -377,6 +381,8 @@ class Detector:
         cfg.light_steps = light_steps
         cfg.stage_b_form = stage_b_form
         cfg.stage_b_chunk = stage_b_chunk
+        cfg.plain_streams = plain_streams
+        cfg.sweep_unstaged = sweep_unstaged
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -441,10 +447,7 @@ class Detector:
     def stats(self):
         s = Stats()
         _ok(lib().rtcd_last_stats(self.h, C.byref(s)))
-        return {'work_items': s.work_items, 'fp64_retests': s.fp64_retests, 'ms_prepare': s.ms_prepare,
-                'ms_cull': s.ms_cull, 'ms_traverse': s.ms_traverse, 'ms_total': s.ms_total,
-                'candidates': s.candidates, 'exact_tests': s.exact_tests, 'skipped': s.skipped,
-                'node_tests': s.node_tests}
+        return {k: getattr(s, k) for k, _ in Stats._fields_ if not k.startswith('reserved')}
 
     def close(self):
         if self.h:

@@ -29,3 +29,19 @@ def test_reference_arm_line():
     cb = d['cpu_baseline']
     assert cb['value'] == d['value'] and cb['kind'] in ('port', 'reference') and cb['cores'] >= 1
     assert d['config']['workload']
+
+
+def test_two_rank_launcher_gathers_flags_on_cpu():
+    """`bench.py --gpus 2` starts two ranks itself (RANK / LOCAL_RANK /
+    WORLD_SIZE, rendezvous on 127.0.0.1); the --dry path runs them over gloo
+    with the CPU oracle, all-gathers the flags and rank 0 checks the gathered
+    array against a single-process run of both ranks' batches."""
+    d = run_bench('--gpus', '2', '--dry', '--config', 'c1', '--dry-units', '128')
+    assert d['n_gpus'] == 2 and d['scaling'] == 'weak'
+    assert d['gathered'] == {'units': 256, 'equal_to_single_process': True}
+
+
+def test_two_rank_launcher_sweep_on_cpu():
+    d = run_bench('--gpus', '2', '--dry', '--config', 'c3', '--dry-units', '16')
+    assert d['n_gpus'] == 2 and d['unit'] == 'trajectories/s'
+    assert d['gathered'] == {'units': 32, 'equal_to_single_process': True}
