@@ -354,6 +354,110 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
     return out
 
 
+def fp64_statement(cfg, ctx, model, mesh, spheres, q, off, n_pairs=4096, seed=0):
+    """The error of the FP32 exact tests against FP64, on near-degenerate pairs
+    drawn from this workload's own geometry, run through the device's own
+    arithmetic (rtcd_exact_test_probe) and checked against the oracle on the
+    same float inputs.
+
+    Discrete: segments crossing scene triangles within 1e-7..1e-5 m of an
+    edge, a vertex or the plane: how many the FP32 filter hands to FP64, and
+    how many of its certain decisions (or the FP64 re-test's) disagree with
+    the oracle where the oracle's margin exceeds 1e-12 m (both must be 0).
+    Sweeps: segments passing within +-20 um of the radius of the workload's
+    own pieces (capsules or quadratic Bezier pieces): the largest FP32 and FP64
+    distance errors against the oracle's FP64 branch and bound, and the count
+    of FP32 sides wrong outside the FP64 re-test band (must be 0)."""
+    from oracle import oracle as O
+    from rtcollisiondetection_b200 import rtcd
+    rng = np.random.default_rng(seed)
+    if cfg['kind'] in ('RobotToObs', 'ObsToRobot'):
+        tri = mesh.verts[mesh.tris[rng.integers(0, len(mesh.tris), n_pairs)]].astype(np.float64)  # n x 3 x 3
+        nrm = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        mode = rng.integers(0, 3, n_pairs)        # 0 near an edge, 1 near a vertex, 2 endpoint near the plane
+        delta = rng.choice([-1e-5, -1e-6, -1e-7, 1e-7, 1e-6, 1e-5], n_pairs)
+        k = rng.integers(0, 3, n_pairs)
+        a, b = tri[np.arange(n_pairs), k], tri[np.arange(n_pairs), (k + 1) % 3]
+        c = tri[np.arange(n_pairs), (k + 2) % 3]
+        t = rng.uniform(0.1, 0.9, n_pairs)[:, None]
+        on_edge = a + t * (b - a)
+        inward = c - on_edge - ((c - on_edge) * (b - a)).sum(1, keepdims=True) / ((b - a) ** 2).sum(1, keepdims=True) * (b - a)
+        inward /= np.linalg.norm(inward, axis=1, keepdims=True)
+        x = np.where((mode == 0)[:, None], on_edge + delta[:, None] * inward,
+                     np.where((mode == 1)[:, None], a + delta[:, None] * inward, tri.mean(1)))
+        L = 0.01
+        p = x - L * nrm
+        qq = x + np.where((mode == 2)[:, None], delta[:, None], L) * nrm
+        seg = np.concatenate([p, qq], 1).astype(np.float32)
+        trif = tri.reshape(n_pairs, 9).astype(np.float32)
+        cls, dec = rtcd.exact_test_probe(ctx, 0, seg, trif)
+        wrong32 = wrong64 = margin_ok = 0
+        for i in range(n_pairs):
+            s64 = seg[i].astype(np.float64)
+            t64 = trif[i].astype(np.float64)
+            hit, m = O.seg_tri(s64[:3], s64[3:], t64[:3], t64[3:6], t64[6:])
+            if m <= 1e-12:
+                continue
+            margin_ok += 1
+            if cls[i] != 2 and bool(cls[i]) != hit:
+                wrong32 += 1
+            if bool(dec[i]) != hit:
+                wrong64 += 1
+        return {'test': 'segment-triangle', 'pairs': n_pairs, 'decided_by_oracle': margin_ok,
+                'fp32_undecided': int((cls == 2).sum()), 'fp32_certain_wrong': wrong32, 'fp64_wrong': wrong64,
+                'sample': 'segments crossing the scene\'s own triangles within 1e-7..1e-5 m of an edge, a vertex '
+                          'or the plane'}
+    # sweeps: pieces of the first trajectories of this batch
+    quad = cfg['kind'] == 'Quadratic'
+    nt = min(64, len(off) - 1)
+    T = O.fk(model, q[:off[nt]])                            # FP64 link transforms per waypoint
+    cen, rad, lnk = spheres[0].astype(np.float64), spheres[1].astype(np.float64), spheres[2]
+    segs, pieces, rs = [], [], []
+    for i in range(n_pairs):
+        tr = int(rng.integers(0, nt))
+        w0, nw = int(off[tr]), int(off[tr + 1] - off[tr])
+        sph = int(rng.integers(0, len(rad)))
+        P = np.stack([T[w0 + w, lnk[sph]].reshape(3, 4) @ np.append(cen[sph], 1.0) for w in range(nw)])
+        if quad:
+            nc = O.quad_ctrl_count(nw)
+            C = O.fit_weights(nc, nw) @ P
+            g = int(rng.integers(0, nc - 2))
+            B = np.stack([(C[g] + C[g + 1]) / 2, C[g + 1], (C[g + 1] + C[g + 2]) / 2])
+        else:
+            g = int(rng.integers(0, nw - 1))
+            B = np.stack([P[g], P[g + 1], P[g + 1]])
+        B = B.astype(np.float32).astype(np.float64)
+        u = rng.uniform(0, 1)
+        pt = (1 - u) ** 2 * B[0] + 2 * u * (1 - u) * B[1] + u ** 2 * B[2]
+        tg = 2 * (1 - u) * (B[1] - B[0]) + 2 * u * (B[2] - B[1])
+        if np.linalg.norm(tg) < 1e-9:   # a sphere that does not move (base link): any direction
+            tg = rng.normal(size=3)
+        tg = tg / np.linalg.norm(tg)
+        nv = np.cross(tg, rng.normal(size=3))
+        nv /= np.linalg.norm(nv)
+        ev = np.cross(nv, tg) if rng.random() < 0.5 else tg
+        r = float(rad[sph])
+        x = pt + (r + rng.uniform(-2e-5, 2e-5)) * nv
+        segs.append(np.concatenate([x - 0.02 * ev, x + 0.02 * ev]))
+        pieces.append(B.reshape(9))
+        rs.append(r)
+    seg = np.array(segs, np.float32)
+    pc = np.array(pieces, np.float32)
+    d32, d64 = rtcd.exact_test_probe(ctx, 2 if quad else 1, seg, pc)
+    ref = np.array([O.seg_quad(seg[i, :3], seg[i, 3:], pc[i, :3], pc[i, 3:6], pc[i, 6:]) if quad else
+                    O.seg_seg(seg[i, :3], seg[i, 3:], pc[i, :3], pc[i, 3:6]) for i in range(n_pairs)])
+    rs = np.array(rs)
+    band = 2e-6 + 1e-6 * rs
+    outside = np.abs(ref - rs) > band
+    wrong = int((((d32 <= rs) != (ref <= rs)) & outside).sum())
+    return {'test': 'segment-quadratic piece' if quad else 'segment-capsule', 'pairs': n_pairs,
+            'max_abs_err_fp32_m': float(np.abs(d32 - ref).max()), 'max_abs_err_fp64_m': float(np.abs(d64 - ref).max()),
+            'in_fp64_band': int((~outside).sum()), 'fp32_side_wrong_outside_band': wrong,
+            'sample': 'segments within +-20 um of the radius of this batch\'s own %s' % (
+                'quadratic pieces (fitted control points)' if quad else 'capsules')}
+
+
 FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal: SMs x FP32 lanes x FMA x max SM clock
 
 
@@ -778,6 +882,10 @@ def main():
         line['check'] = oracle_errors(cfg, model, mesh, spheres, q, off, flags, two_way=args.two_way,
                                       containment=args.containment)
         line['fp64_retests'] = st['fp64_retests']
+        line['fp64'] = dict(fp64_statement(cfg, ctx, model, mesh, spheres, q, off),
+                            retests_per_step=st['fp64_retests'],
+                            root_findings_per_step=st['candidates'] if cfg['kind'] == 'Quadratic' else None,
+                            in_band_of_checked=line['check']['in_band'])
     if args.serve_seconds > 0 and rank == 0 and args.config == 'c2':
         line['served'] = served_stream(ctx, args.serve_seconds, saturate_requests=args.saturate_requests)
     if not args.no_cpu_baseline and rank == 0 and world == 1:

@@ -426,6 +426,19 @@ RTCD_API rtcd_status rtcd_exclusive_scan_u32(rtcd_ctx* ctx, const uint32_t* in_d
 RTCD_API rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_t n, uint32_t* idx_dev,
                                           uint32_t* count_dev, void* stream);
 
+/* Diagnostics of the exact tests' arithmetic, on n pairs given in world
+ * coordinates (device arrays, asynchronous on `stream`).  test 0:
+ * segment-triangle - a: n x 6 floats (p, q), b: n x 9 (triangle a, b, c);
+ * f32_out[i] = the FP32 filter's class (0 certain miss, 1 certain hit, 2 too
+ * close to call: re-tested in FP64), f64_out[i] = the FP64 re-test's decision
+ * (0 / 1).  test 1: segment vs capsule axis - b: n x 9 (axis B0 B1, 3 floats
+ * unused); test 2: segment vs quadratic Bezier piece - b: n x 9 (B0 B1 B2);
+ * f32_out = the distance the light pass computes in FP32, f64_out = the FP64
+ * re-test's distance.  No counterpart in the reference (its intersectors are
+ * closed). */
+RTCD_API rtcd_status rtcd_exact_test_probe(rtcd_ctx* ctx, int test, const float* a_dev, const float* b_dev, uint32_t n,
+                                           float* f32_out_dev, double* f64_out_dev, void* stream);
+
 /* Self-test of the failure detection of the bounded device waits.  No
  * counterpart in the reference (its device code has no bounded waits).  Runs
  * the compaction of n (1 to 1,048,576) zero flags with the tile counter

@@ -1965,6 +1965,18 @@ rtcd_status rtcd_select_flags_u8(rtcd_ctx* ctx, const uint8_t* mask_dev, uint32_
     });
 }
 
+rtcd_status rtcd_exact_test_probe(rtcd_ctx* ctx, int test, const float* a_dev, const float* b_dev, uint32_t n,
+                                  float* f32_dev, double* f64_dev, void* stream) {
+    return guarded([&] {
+        RTCD_REQUIRE(ctx && (n == 0 || (a_dev && b_dev && f32_dev && f64_dev)), "NULL argument");
+        RTCD_REQUIRE(test >= 0 && test <= 2, "test must be 0 (segment-triangle), 1 (capsule) or 2 (quadratic)");
+        DeviceScope ds(ctx->device);
+        cudaStream_t s = stream ? (cudaStream_t) stream : ctx->stream;
+        if (test == 0) launch_probe_segtri(a_dev, b_dev, n, f32_dev, f64_dev, s);
+        else launch_probe_sweep(test == 2, a_dev, b_dev, n, f32_dev, f64_dev, s);
+    });
+}
+
 rtcd_status rtcd_selftest_lookback_timeout(rtcd_ctx* ctx, uint32_t n, uint32_t spin_limit) {
     return guarded([&] {
         RTCD_REQUIRE(ctx, "NULL context");

@@ -1636,6 +1636,28 @@ __global__ void k_popcount_rows(const uint32_t* __restrict__ bits, uint32_t word
     }
 }
 
+// Diagnostics of the segment-triangle arithmetic: per pair the FP32 filter's
+// class (0 certain miss, 1 certain hit, 2 handed to FP64) and the FP64
+// re-test's decision, on pairs given in world coordinates.
+__global__ void k_probe_segtri(const float* __restrict__ seg, const float* __restrict__ tri, uint32_t n,
+                               float* __restrict__ cls, double* __restrict__ dec) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* e = seg + 6ull * i;
+    const float* t = tri + 9ull * i;
+    const f3 p = mk(e[0], e[1], e[2]), q = mk(e[3], e[4], e[5]);
+    const f3 a = mk(t[0], t[1], t[2]), b = mk(t[3], t[4], t[5]), c = mk(t[6], t[7], t[8]);
+    cls[i] = (float) seg_tri_f32(p, q, a, b, c);
+    dec[i] = seg_tri_f64(d3of(p), d3of(q), d3of(a), d3of(b), d3of(c)) ? 1.0 : 0.0;
+}
+
+void launch_probe_segtri(const float* d_seg, const float* d_tri, uint32_t n, float* d_cls, double* d_dec,
+                         cudaStream_t s) {
+    if (!n) return;
+    k_probe_segtri<<<(n + 127) / 128, 128, 0, s>>>(d_seg, d_tri, n, d_cls, d_dec);
+    cuda_check(cudaGetLastError(), "k_probe_segtri");
+}
+
 void launch_popcount_rows(const uint32_t* d_bits, uint32_t words, uint32_t rows, uint32_t* d_out, cudaStream_t s) {
     if (!rows) return;
     k_popcount_rows<<<rows, 128, 0, s>>>(d_bits, words, rows, d_out);

@@ -196,6 +196,12 @@ size_t sweep_staged_smem(bool quad, uint32_t n_links, uint32_t max_wp, uint32_t 
 uint32_t sweep_persistent_blocks(bool quad);
 uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads);  // threads: 64, 128 or 256
 
+// diagnostics of the exact tests (discrete.cu, sweep.cu)
+void launch_probe_segtri(const float* d_seg, const float* d_tri, uint32_t n, float* d_cls, double* d_dec,
+                         cudaStream_t s);
+void launch_probe_sweep(bool quad, const float* d_seg, const float* d_piece, uint32_t n, float* d32, double* d64,
+                        cudaStream_t s);
+
 // planner side (planner.cu)
 constexpr uint32_t kKnnMaxK = 32;
 constexpr uint32_t kKnnMaxDim = 16;

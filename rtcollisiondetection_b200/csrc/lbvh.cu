@@ -222,70 +222,140 @@ __global__ void k_morton(const float4* __restrict__ lo, const float4* __restrict
 }
 
 // ---------------------------------------------------------------- radix sort
-// Stable LSD radix sort of (code, index) pairs, 8-bit digits.  Per digit pass:
-// a per-tile histogram, a decoupled look-back scan of the digit-major
-// histogram, and a scatter that ranks keys stably inside the tile with warp
-// match masks.
+// Stable LSD radix sort of (code, index) pairs in the Onesweep form (Adinets
+// and Merrill, "Onesweep: A Faster Least Significant Digit Radix Sort for
+// GPUs", 2022): one kernel counts the digits of every pass at once, then each
+// 8-bit pass is a single kernel - a tile (2048 keys, its index taken from an
+// atomic counter) ranks its keys stably, publishes its per-digit counts,
+// looks back over the tiles before it for each digit's running prefix
+// (decoupled look-back, one thread per digit) and scatters.  No per-pass
+// histogram or scan kernel, no host round trip.
 constexpr int kRsThreads = 256;
 constexpr int kRsRounds = 8;
 constexpr int kRsTile = kRsThreads * kRsRounds;
+constexpr int kRsPasses = 4;  // 30-bit codes: digits at bits 0, 8, 16, 24
+constexpr uint32_t kRsAgg = 1u << 30, kRsInc = 2u << 30, kRsCount = (1u << 30) - 1u;
 
-__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift,
-                                                       uint32_t n_tiles, uint32_t* hist) {
-    __shared__ uint32_t cnt[256];
-    cnt[threadIdx.x] = 0;
+// Digit counts of every pass: ghist[pass][digit].
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist_all(const uint32_t* __restrict__ keys, uint32_t n,
+                                                           uint32_t* __restrict__ ghist) {
+    __shared__ uint32_t h[kRsPasses][256];
+    for (int p = 0; p < kRsPasses; ++p) h[p][threadIdx.x] = 0;
     __syncthreads();
-    const size_t base = (size_t) blockIdx.x * kRsTile;
-    for (int r = 0; r < kRsRounds; ++r) {
-        size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
-        if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1u);
+    for (size_t i = (size_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < kRsPasses; ++p) atomicAdd(&h[p][(k >> (8 * p)) & 255u], 1u);
     }
     __syncthreads();
-    hist[(size_t) threadIdx.x * n_tiles + blockIdx.x] = cnt[threadIdx.x];
+    for (int p = 0; p < kRsPasses; ++p)
+        if (h[p][threadIdx.x]) atomicAdd(ghist + p * 256 + threadIdx.x, h[p][threadIdx.x]);
 }
 
-__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t* __restrict__ kin,
-                                                          const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-                                                          uint32_t* __restrict__ vout, uint32_t n, int shift,
-                                                          uint32_t n_tiles, const uint32_t* __restrict__ offsets) {
+// One pass.  status: [tile][256] words (flag << 30 | count), zeroed before
+// the pass; counter: the pass's tile counter, zeroed.
+__global__ void __launch_bounds__(kRsThreads) k_rs_onesweep(const uint32_t* __restrict__ kin,
+                                                           const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+                                                           uint32_t* __restrict__ vout, uint32_t n, int pass,
+                                                           const uint32_t* __restrict__ ghist, uint32_t* status,
+                                                           uint32_t* counter, uint32_t* err) {
     constexpr int W = kRsThreads / 32;
+    __shared__ uint32_t s_tile;
     __shared__ uint32_t run[256];
     __shared__ uint32_t wcnt[W][256];
-    __shared__ uint32_t goff[256];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    run[threadIdx.x] = 0;
-    goff[threadIdx.x] = offsets[(size_t) threadIdx.x * n_tiles + blockIdx.x];
-    const size_t base = (size_t) blockIdx.x * kRsTile;
+    __shared__ uint32_t s_start[256];  // first position of each digit in this pass's output
+    __shared__ uint32_t s_warp[W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, shift = 8 * pass;
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    // exclusive scan of the pass's digit counts (256 digits, one per thread)
+    {
+        const uint32_t c = ghist[pass * 256 + threadIdx.x];
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        run[threadIdx.x] = 0;
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; ++w) before += s_warp[w];
+        s_start[threadIdx.x] = before + inc - c;
+    }
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const size_t base = (size_t) tile * kRsTile;
     const uint32_t lt = (1u << lane) - 1u;
+    uint32_t key[kRsRounds], val[kRsRounds], rank[kRsRounds];
+    // stable ranks inside the tile: round by round, warp by warp, lane by lane
+#pragma unroll
     for (int r = 0; r < kRsRounds; ++r) {
 #pragma unroll
         for (int w = 0; w < W; ++w) wcnt[w][threadIdx.x] = 0;
         __syncthreads();
-        size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
-        bool valid = i < n;
-        uint32_t key = valid ? kin[i] : 0u, val = valid ? vin[i] : 0u;
-        uint32_t d = valid ? ((key >> shift) & 255u) : 256u;
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        uint32_t rank = __popc(peers & lt);
-        if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
+        const size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
+        const bool valid = i < n;
+        key[r] = valid ? kin[i] : 0u;
+        val[r] = valid ? vin[i] : 0u;
+        const uint32_t d = valid ? ((key[r] >> shift) & 255u) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        rank[r] = __popc(peers & lt);
+        if (valid && rank[r] == 0) wcnt[warp][d] = __popc(peers);
         __syncthreads();
         {
-            uint32_t dd = threadIdx.x, acc = run[dd];
+            const uint32_t dd = threadIdx.x;
+            uint32_t acc = run[dd];
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                uint32_t t = wcnt[w][dd];
+                const uint32_t t = wcnt[w][dd];
                 wcnt[w][dd] = acc;
                 acc += t;
             }
             run[dd] = acc;
         }
         __syncthreads();
-        if (valid) {
-            uint32_t pos = goff[d] + wcnt[warp][d] + rank;
-            kout[pos] = key;
-            vout[pos] = val;
+        if (valid) rank[r] += wcnt[warp][d];
+        __syncthreads();  // wcnt is cleared by the next round
+    }
+    // publish this tile's count of digit d, look back for the count of d in the tiles before it
+    {
+        const uint32_t d = threadIdx.x, cnt = run[d];
+        volatile uint32_t* st = status;
+        uint32_t excl = 0;
+        if (tile == 0) {
+            atomicExch(status + d, kRsInc | cnt);
+        } else {
+            atomicExch(status + (size_t) tile * 256 + d, kRsAgg | cnt);
+            long long p = (long long) tile - 1;
+            uint32_t spins = 0;
+            while (p >= 0) {
+                const uint32_t w = st[(size_t) p * 256 + d];
+                if ((w & ~kRsCount) == 0) {
+                    if (++spins > kLookbackSpinLimit) {
+                        atomicOr(err, kErrLookback);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                excl += w & kRsCount;
+                if (w & kRsInc) break;
+                --p;
+            }
+            atomicExch(status + (size_t) tile * 256 + d, kRsInc | (excl + cnt));
         }
-        __syncthreads();
+        run[d] = s_start[d] + excl;  // the tile's first position for digit d
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRsRounds; ++r) {
+        const size_t i = base + (size_t) r * kRsThreads + threadIdx.x;
+        if (i < n) {
+            const uint32_t pos = run[(key[r] >> shift) & 255u] + rank[r];
+            kout[pos] = key[r];
+            vout[pos] = val[r];
+        }
     }
 }
 
@@ -396,8 +466,7 @@ LbvhResult build_lbvh(const float4* d_lo, const float4* d_hi, uint32_t n, float4
     LbvhResult r;
     if (n == 0) return r;
     if (n >= (1u << 30)) fail(5, "LBVH: too many primitives");
-    DevBuf bounds, codes_a, codes_b, idx_a, idx_b, hist, offs, child, parent, nlo, nhi, visits, depth;
-    ScanScratch sc;
+    DevBuf bounds, codes_a, codes_b, idx_a, idx_b, hist, child, parent, nlo, nhi, visits, depth;
     bounds.ensure(6 * sizeof(uint32_t));
     uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
     cuda_check(cudaMemcpyAsync(bounds.p, init, sizeof(init), cudaMemcpyHostToDevice, s), "bounds init");
@@ -408,15 +477,21 @@ LbvhResult build_lbvh(const float4* d_lo, const float4* d_hi, uint32_t n, float4
     k_morton<<<(n + 255) / 256, 256, 0, s>>>(d_lo, d_hi, n, bounds.as<uint32_t>(), codes_a.as<uint32_t>(),
                                              idx_a.as<uint32_t>());
     cuda_check(cudaGetLastError(), "k_morton");
-    uint32_t tiles = (n + kRsTile - 1) / kRsTile;
-    hist.ensure(4ull * 256 * tiles);
-    offs.ensure(4ull * 256 * tiles);
+    const uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+    // one zeroed block: the digit counts of every pass [4][256], the tile counters [4] and the
+    // look-back words of every pass [4][tiles][256]
+    const size_t words = (size_t) kRsPasses * 256 + kRsPasses + (size_t) kRsPasses * tiles * 256;
+    hist.ensure(4 * words);
+    cuda_check(cudaMemsetAsync(hist.p, 0, 4 * words, s), "radix memset");
+    uint32_t* ghist = hist.as<uint32_t>();
+    uint32_t* counters = ghist + kRsPasses * 256;
+    uint32_t* status = counters + kRsPasses;
     uint32_t *ka = codes_a.as<uint32_t>(), *kb = codes_b.as<uint32_t>(), *va = idx_a.as<uint32_t>(),
              *vb = idx_b.as<uint32_t>();
-    for (int shift = 0; shift < 30; shift += 8) {
-        k_rs_hist<<<tiles, kRsThreads, 0, s>>>(ka, n, shift, tiles, hist.as<uint32_t>());
-        scan_u32(hist.as<uint32_t>(), offs.as<uint32_t>(), 256 * tiles, nullptr, sc, d_err, s);
-        k_rs_scatter<<<tiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, tiles, offs.as<uint32_t>());
+    k_rs_hist_all<<<std::max(1, std::min<int>((int) tiles, sms * 4)), kRsThreads, 0, s>>>(ka, n, ghist);
+    for (int pass = 0; pass < kRsPasses; ++pass) {
+        k_rs_onesweep<<<tiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, pass, ghist, status + (size_t) pass * tiles * 256,
+                                                  counters + pass, d_err);
         cuda_check(cudaGetLastError(), "radix pass");
         std::swap(ka, kb);
         std::swap(va, vb);

@@ -1041,6 +1041,41 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
     warp_count(A.stats + 7, n_node);
 }
 
+// Diagnostics of the sweeps' arithmetic: per (segment, piece) pair the FP32
+// distance the light pass computes (linear: segment-segment; quadratic: the
+// root-found distance to the Bezier piece) and the FP64 distance of the
+// re-test, on pairs given in world coordinates (piece: B0 B1 B2, linear axis
+// B0-B1).
+template <bool QUAD>
+__global__ void k_probe_sweep(const float* __restrict__ seg, const float* __restrict__ piece, uint32_t n,
+                              float* __restrict__ d32, double* __restrict__ d64) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* e = seg + 6ull * i;
+    const float* b = piece + 9ull * i;
+    const float4 ea = make_float4(e[0], e[1], e[2], 0.f), eb = make_float4(e[3], e[4], e[5], 0.f);
+    const float4 B0 = make_float4(b[0], b[1], b[2], 0.f), B1 = make_float4(b[3], b[4], b[5], 0.f),
+                 B2 = make_float4(b[6], b[7], b[8], 0.f);
+    if (QUAD) {
+        d32[i] = seg_quad_dist_f32(ea, eb, B0, B1, B2);
+        d64[i] = sqrt(seg_quad2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(B0),
+                                        v3cast<double>(B1), v3cast<double>(B2), 48));
+    } else {
+        d32[i] = sqrtf(fmaxf(seg_seg2<float>(v3cast<float>(ea), v3cast<float>(eb), v3cast<float>(B0),
+                                             v3cast<float>(B1)), 0.f));
+        d64[i] = sqrt(seg_seg2<double>(v3cast<double>(ea), v3cast<double>(eb), v3cast<double>(B0),
+                                       v3cast<double>(B1)));
+    }
+}
+
+void launch_probe_sweep(bool quad, const float* d_seg, const float* d_piece, uint32_t n, float* d32, double* d64,
+                        cudaStream_t s) {
+    if (!n) return;
+    if (quad) k_probe_sweep<true><<<(n + 127) / 128, 128, 0, s>>>(d_seg, d_piece, n, d32, d64);
+    else k_probe_sweep<false><<<(n + 127) / 128, 128, 0, s>>>(d_seg, d_piece, n, d32, d64);
+    cuda_check(cudaGetLastError(), "k_probe_sweep");
+}
+
 size_t sweep_staged_smem(bool quad, uint32_t n_links, uint32_t max_wp, uint32_t max_nc, uint32_t max_pieces) {
     const size_t bytes = 48ull * n_links * (max_wp + (quad ? max_nc : 0)) + 4ull * max_pieces;
     return bytes <= kSweepStagedMaxSmem ? ((bytes + 15) & ~size_t(15)) : 0;

@@ -43,7 +43,7 @@ EXPORTS = ['rtcd_abi_version', 'rtcd_last_error', 'rtcd_context_create', 'rtcd_c
            'rtcd_server_get_stats', 'rtcd_server_reset_stats', 'rtcd_detector_autotune', 'rtcd_server_prepare',
            'rtcd_select_flags_u8_noalloc', 'rtcd_quad_fit_weights', 'rtcd_urdf_chain_parse', 'rtcd_obj_load',
            'rtcd_halton_samples', 'rtcd_knn', 'rtcd_check_edges', 'rtcd_selftest_lookback_timeout',
-           'rtcd_loop_edges']
+           'rtcd_loop_edges', 'rtcd_exact_test_probe']
 
 
 class RTCDError(RuntimeError):
@@ -158,6 +158,21 @@ def loop_edges(tris):
     _ok(lib().rtcd_loop_edges(_ptr(tris, C.c_uint32), C.c_uint32(len(tris)), _ptr(out, C.c_uint32),
                               C.c_uint32(n.value), C.byref(n)))
     return out[:n.value]
+
+
+def exact_test_probe(ctx, test, a, b):
+    """The device's FP32 and FP64 results of one exact test on n pairs (numpy in, numpy out):
+    test 0 segment-triangle (class, decision), 1 capsule and 2 quadratic (FP32 and FP64 distances)."""
+    import torch
+    a = torch.from_numpy(_arr(a, np.float32).reshape(-1, 6)).cuda()
+    b = torch.from_numpy(_arr(b, np.float32).reshape(-1, 9)).cuda()
+    n = a.shape[0]
+    f32 = torch.zeros(max(n, 1), dtype=torch.float32, device='cuda')
+    f64 = torch.zeros(max(n, 1), dtype=torch.float64, device='cuda')
+    _ok(lib().rtcd_exact_test_probe(ctx.h, C.c_int(test), _ptr(a, C.c_float), _ptr(b, C.c_float), C.c_uint32(n),
+                                    _ptr(f32, C.c_float), _ptr(f64, C.c_double), None))
+    torch.cuda.synchronize()
+    return f32.cpu().numpy()[:n], f64.cpu().numpy()[:n]
 
 
 def selftest_lookback_timeout(ctx, n, spin_limit):

@@ -254,3 +254,64 @@ def test_graph_with_host_buffers(ctx, panda):
         for q, ref in zip(qs, refs):
             assert np.array_equal(det.check(q, flags=rtcd.CHECK_GRAPH)['flags'], ref['flags'])
         det.close()
+
+
+def test_large_triangle_edges_graze_links(ctx, panda):
+    """The link-side node test of RobotToObs adds the nine edge-cross axes for
+    triangles over 3 cm.  Aim at its boundary: one large triangle per scene
+    whose edge passes through, just inside and just outside a link's vertex
+    (offsets 0, +-50 um, +-1 mm and tangent-parallel), poses jittered around
+    that pose by up to 2 mrad.  Flags and counts equal the FP64 oracle's
+    outside the band."""
+    robot = rtcd.Robot(ctx, panda)
+    rng = np.random.default_rng(21)
+    orob = O.Robot(panda)
+    checked = hits = 0
+    for k in range(8):
+        q0 = scenes.uniform_poses(panda, 1, seed=200 + k)[0]
+        T = O.fk(panda, q0[None])[0]
+        l = 1 + k % 7
+        lv = panda['link_verts'][panda['link_vert_off'][l]:panda['link_vert_off'][l + 1]].astype(np.float64)
+        Tl = T[l].reshape(3, 4)
+        p = lv[rng.integers(len(lv))] @ Tl[:, :3].T + Tl[:, 3]  # a link vertex in the world
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        n = np.cross(d, rng.normal(size=3))
+        n /= np.linalg.norm(n)
+        off = [0.0, 5e-5, -5e-5, 1e-3, -1e-3][k % 5]
+        a = p + off * n - 0.6 * d          # the edge a-b passes off metres from the vertex
+        b = p + off * n + 0.6 * d
+        c = p + off * n + 0.8 * n + 0.1 * d  # the triangle spans to one side of the edge
+        mesh = scenes.Mesh(np.array([a, b, c], np.float32), np.array([[0, 1, 2]], np.uint32),
+                           np.array([0, 1], np.uint32))
+        sc = rtcd.Scene.from_mesh(ctx, mesh)
+        q = (q0[None] + rng.uniform(-2e-3, 2e-3, size=(256, 7))).astype(np.float32)
+        q = np.clip(q, panda['lower'], panda['upper'])
+        det = rtcd.Detector(ctx, 'RobotToObs', robot, sc)
+        ref = O.discrete(O.ROBOT_TO_OBS, orob, O.Scene(mesh), q)
+        _compare(det.check(q, counts=True), ref)
+        assert np.array_equal(det.check(q)['flags'], det.check(q, counts=True)['flags'])
+        checked += int((ref['band'] == 0).sum())
+        hits += int(ref['hit'].sum())
+        det.close()
+        sc.close()
+    assert checked > 1000 and hits > 0
+
+
+def test_plain_path_upstream_shape(setup, panda):
+    """The plain path (frames over several streams and host threads, a host
+    round trip per frame) equals the batched path for frame sizes and stream
+    counts that leave partial frames and partial groups."""
+    robot, scene, _ = setup
+    q = scenes.uniform_poses(panda, 5000, seed=12)
+    base = None
+    for fs, ns in ((1024, 4), (1024, 1), (333, 3), (5000, 2)):
+        det = rtcd.Detector(robot.ctx, 'RobotToObs', robot, scene, frame_size=fs, plain_streams=ns)
+        a = det.check(q, counts=True)
+        b = det.check(q, counts=True, flags=rtcd.CHECK_PLAIN)
+        assert np.array_equal(a['flags'], b['flags']) and np.array_equal(a['counts'], b['counts'])
+        assert det.stats()['work_items'] > 0
+        if base is None:
+            base = a['flags']
+        assert np.array_equal(a['flags'], base)
+        det.close()

@@ -138,3 +138,36 @@ def test_server_rejects_bad_requests(world, panda):
         rtcd._ok(rtcd.lib().rtcd_server_wait(server.h, rtcd.C.c_uint64(12345), rtcd.C.c_int32(0), None, None, None,
                                              None))
     server.close()
+
+
+def test_memory_admission_serialises_launches(world, panda):
+    """Admission by memory: with a budget no larger than one launch, launches
+    run one at a time (the peak of the bytes in flight is one launch's), with
+    a budget of several launches more run at once; every result still equals
+    the request checked alone."""
+    _, dets = world
+    det = dets['r2o_small']
+    qs = [scenes.uniform_poses(panda, 512, seed=100 + i) for i in range(24)]
+    alone = [det.check(q)['flags'] for q in qs]
+
+    def serve(budget):
+        # one request per launch (max_batch_units = the request size) on two bulk slots that could
+        # overlap (the fast slot takes only requests of at most 256 poses: none here)
+        srv = rtcd.Server(det.ctx, slots=3, fast_slots=1, fast_max_units=256, max_batch_units=512,
+                          memory_budget=budget)
+        srv.prepare(det, 512)
+        srv.reset_stats()
+        ts = [srv.submit(det, q) for q in qs]
+        outs = [srv.wait(t)['flags'] for t in ts]
+        st = srv.stats()
+        srv.close()
+        for a, b in zip(outs, alone):
+            assert np.array_equal(a, b)
+        assert st['completed'] == len(qs) and st['batches'] == len(qs)
+        return st['inflight_bytes_peak']
+
+    one = serve(1)                      # smaller than any launch: each is admitted only when none is in flight
+    assert one > 0
+    assert serve(one) == one            # exactly one launch's bytes: still one at a time
+    assert serve(2 * one) <= 2 * one    # two launches at most
+    assert one <= serve(1 << 40) <= 2 * one  # unbounded: as many as the two bulk slots allow
