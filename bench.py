@@ -58,11 +58,24 @@ CONFIGS = {
     'c4': dict(kind='Quadratic', n=4096, scene='sweep', wp=(8, 64),
                workload='Quadratic sweep, 4,096 trajectories of 8-64 waypoints (log-uniform), 64 spheres, '
                         '49,744-tri scene'),
+    'c2_200k': dict(kind='RobotToObs', n=65536, scene='dense200k',
+                    workload='RobotToObs, 65,536 uniform Panda poses, dense scene with level-2 icospheres '
+                             '(64 boxes + 256 level-2 icospheres + 100k-tri noisy sphere, 182,688 tris)'),
+    'c3s': dict(kind='Linear', n=4096, scene='sweep_sparse', wp=32,
+                workload='Linear sweep, 4,096 random-walk trajectories x 32 waypoints, 64 spheres, sparse '
+                         '48,784-tri scene (12 boxes + 38 level-3 icospheres; ~40 % of trajectories collide)'),
+    'c4s': dict(kind='Quadratic', n=4096, scene='sweep_sparse', wp=(8, 64),
+                workload='Quadratic sweep, 4,096 trajectories of 8-64 waypoints (log-uniform), 64 spheres, '
+                         'sparse 48,784-tri scene'),
     # the reference's own benchmark shelves (models/curobo, placements of its scene headers), batch 4096
     'ref_simple_r2o': dict(kind='RobotToObs', n=4096, scene='ref_simple',
                            workload='RobotToObs, 4,096 uniform poses, reference simple shelf (15,008 tris)'),
     'ref_simple_o2r': dict(kind='ObsToRobot', n=4096, scene='ref_simple',
                            workload='ObsToRobot, 4,096 uniform poses, reference simple shelf (15,008 tris)'),
+    'ref_medium_r2o': dict(kind='RobotToObs', n=4096, scene='ref_medium',
+                           workload='RobotToObs, 4,096 uniform poses, reference medium shelf (71,746 tris)'),
+    'ref_medium_o2r': dict(kind='ObsToRobot', n=4096, scene='ref_medium',
+                           workload='ObsToRobot, 4,096 uniform poses, reference medium shelf (71,746 tris)'),
     'ref_dense_r2o': dict(kind='RobotToObs', n=4096, scene='ref_dense',
                           workload='RobotToObs, 4,096 uniform poses, reference dense shelf (202,330 tris)'),
     'ref_dense_o2r': dict(kind='ObsToRobot', n=4096, scene='ref_dense',
@@ -81,7 +94,8 @@ def make_inputs(cfg, rank, scenes):
         mesh = scenes.reference_scene(cfg['scene'][4:])
     else:
         mesh = {'dense': scenes.discrete_dense, 'small': scenes.discrete_small,
-                'sweep': scenes.sweep_scene}[cfg['scene']]()
+                'dense200k': lambda: scenes.discrete_dense(ico_level=2),
+                'sweep': scenes.sweep_scene, 'sweep_sparse': scenes.sweep_scene_sparse}[cfg['scene']]()
     spheres = scenes.synth_spheres(model) if cfg['kind'] in ('Linear', 'Quadratic') else None
     if cfg['kind'] in ('Linear', 'Quadratic'):
         wp = cfg['wp']
@@ -787,7 +801,7 @@ def main():
     achieved = bytes_alg / (t_trav / 1e3) / 1e9
     form = tuned.get('stage_b_form', 0)
     if sweep:
-        span = 'k_sweep + k_sweep_heavy'
+        span = ('k_sweep_traj' if st['path_flags'] & 1 else 'k_sweep') + ' + k_sweep_heavy'
     elif form in (0, 3, 4):
         span = 'k_stage_ab + k_subtree x 2 + k_stage_b (deferred) + k_stage_b_heavy + k_discrete (overflow)'
     else:
@@ -820,7 +834,7 @@ def main():
         return {'flops': flops, 'ms': ms, 'achieved': flops / (ms / 1e3) / 1e12,
                 'frac': flops / (ms / 1e3) / 1e12 / FP32_PEAK_TFLOPS}
     kernels = {'traversal_span': kern(w_span, t_trav),
-               'first_pass': dict(kern(w_first, t_first), kernel='k_sweep (light pass)' if sweep else
+               'first_pass': dict(kern(w_first, t_first), kernel=span.split(' + ')[0] + ' (light pass)' if sweep else
                                   ('k_stage_ab' if form in (0, 3, 4) else 'k_stage_a')),
                'later_passes': dict(kern(max(w_span - w_first, 0.0), t_rest),
                                     kernel='k_sweep_heavy' if sweep else
@@ -857,9 +871,11 @@ def main():
         # discrete: k_fk_poses, k_cull, k_select_u8, then per direction k_stage_ab + k_subtree x 2 + k_stage_b
         # (deferred candidates) or k_stage_a + k_stage_b, k_stage_b_heavy, k_discrete (overflow); (k_contain),
         # k_flags; sweeps: k_fk_spheres, (k_fit), k_sweep, k_sweep_heavy, k_flags x 2
+        # sweeps, staged light pass: k_sweep_traj, k_sweep_heavy, k_flags x 2; unstaged: k_fk_spheres, (k_fit),
+        # k_sweep, k_sweep_heavy, k_flags x 2
         'gpu_launches': args.steps * ((3 + (2 if args.two_way else 1) * (6 if form in (0, 3, 4) else 4)
                                        + (1 if args.containment else 0) + 1) if not sweep
-                                      else (5 if cfg['kind'] == 'Linear' else 6)),
+                                      else 4 if st['path_flags'] & 1 else (5 if cfg['kind'] == 'Linear' else 6)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in spans])),
                       'cull': float(np.mean([s['ms_cull'] for s in spans])), 'traverse': t_trav},
         'roofline': {'bound': 'hbm', 'kernel': span, 'achieved': achieved,
@@ -870,6 +886,42 @@ def main():
                              'read+write of the span\'s kernels (profiles/traffic.json)'},
         'clocks': clocks,
     }
+    if sweep and rank == 0:
+        # the reference's entering-ray semantics beside the solid ones, on the same batch
+        sem = {}
+        for name, f in (('solid', 0), ('solid_no_end_spheres', rtcd.CHECK_NO_ENDPOINTS), ('surface', rtcd.CHECK_SURFACE)):
+            o = det.check(q, off, segments=True, flags=f)
+            sem[name] = o
+        sf, ss = sem['surface'], sem['solid_no_end_spheres']
+        sm = []
+        for k in range(3):
+            flush.fill_(k & 255)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            det.check_device(qd, n, fd, traj_off=off, flags=rtcd.CHECK_SURFACE, stream=sp)
+            torch.cuda.synchronize()
+            sm.append((time.perf_counter() - t0) * 1e3)
+        line['semantics'] = {
+            'traj_hit_rate': {k: float(v['flags'].mean()) for k, v in sem.items()},
+            'seg_hit_rate': {k: float(v['seg_flags'].mean()) for k, v in sem.items()},
+            'traj_solid_only': int(((sem['solid']['flags'] != 0) & (sf['flags'] == 0)).sum()),
+            'seg_solid_only': int(((ss['seg_flags'] != 0) & (sf['seg_flags'] == 0)).sum()),
+            'seg_surface_only': int(((ss['seg_flags'] == 0) & (sf['seg_flags'] != 0)).sum()),
+            'segments': int(len(sf['seg_flags'])),
+            'surface_units_per_s': n / (np.median(sm) / 1e3),
+            'note': 'solid: an obstacle edge within r of the sphere path (round caps; quadratic adds the start/end '
+                    'spheres); surface: the reference semantics, a directed loop edge entering a piece (flat '
+                    'quadratic caps, no end spheres); seg_* compare surface with solid without end spheres'}
+        if not args.no_check:
+            from oracle import oracle as O
+            m = min(len(off) - 1, 128)
+            ref = O.sweep(cfg['kind'] == 'Quadratic', O.Robot(model, spheres=spheres), O.Scene(mesh), q[:off[m]],
+                          off[:m + 1], surface=True)
+            line['semantics']['surface_check'] = {
+                'flag_errors': int(((sf['flags'][:m] != ref['traj_hit']) & (ref['traj_band'] == 0)).sum()),
+                'seg_flag_errors': int(((sf['seg_flags'][:ref['seg_off'][-1]] != ref['seg_hit'])
+                                        & (ref['seg_band'] == 0)).sum()),
+                'checked': m, 'in_band': int(ref['traj_band'].sum())}
     if gathered:
         line['gathered'] = gathered
     if plain:

@@ -306,7 +306,7 @@ typedef struct {
     uint64_t node_tests;   /* BVH child-box tests of the traversal kernels */
     float ms_first_pass;   /* with RTCD_CHECK_TIMING: the first traversal kernel alone (discrete: the fused or
                               stage-A kernel of the first direction; sweeps: the light pass) */
-    uint32_t reserved0;
+    uint32_t path_flags;         /* bit 0: the sweep light pass staged its trajectories in shared memory */
     uint64_t first_node_tests;   /* node_tests of that first kernel (the rest: the passes after it) */
     uint64_t first_exact_tests;  /* exact_tests of that first kernel */
     uint64_t cull_sphere_tests;  /* discrete: bounding-sphere tests of the OBB cull */

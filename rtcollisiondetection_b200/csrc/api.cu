@@ -511,6 +511,7 @@ struct rtcd_detector {
     HostBuf pin_in, pin_out, pin_aux;
     DevBuf hq, hflags, hseg, hcounts;  // device sides of a graph replay with host buffers
     uint64_t last_items = 0, last_culled = 0;
+    uint32_t last_path_flags = 0;  // rtcd_stats.path_flags of the last check
     // plain path: one clone of this detector per stream (own stream and workspace) and their threads
     std::vector<rtcd_detector*> plain_clones;
     std::unique_ptr<PlainPool> plain_pool;
@@ -1459,6 +1460,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     for (uint32_t i = 0; i < n; ++i) max_pieces = std::max(max_pieces, piece_off[i + 1] - piece_off[i]);
     const uint32_t max_nc = quad ? quad_ctrl_count(max_wp) : 0;
     const bool staged = !d->cfg.sweep_unstaged && sweep_staged_smem(quad, R.n_links, max_wp, max_nc, max_pieces) != 0;
+    d->last_path_flags = staged ? 1u : 0u;
     const bool timed = (flags & RTCD_CHECK_TIMING) != 0;
     d->timed = timed;
     if (timed) cuda_check(cudaEventRecord(d->ev[0], s), "event");
@@ -1749,6 +1751,7 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
             cuda_check(cudaMemcpyAsync(&cand, d->wave_counts.p, 4, cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaStreamSynchronize(s), "stats sync");
         for (int k = 0; k < kStatBank; ++k) st[k] = sb[k] + sb[kStatBank + k];
+        out->path_flags = d->last_path_flags;
         out->first_node_tests = sb[7];
         out->first_exact_tests = sb[4];
         out->cull_sphere_tests = sb[kStatCullSpheres];

@@ -74,7 +74,7 @@ class Stats(C.Structure):
                 ('ms_prepare', C.c_float), ('ms_cull', C.c_float), ('ms_traverse', C.c_float),
                 ('ms_total', C.c_float), ('candidates', C.c_uint64), ('exact_tests', C.c_uint64),
                 ('skipped', C.c_uint64), ('node_tests', C.c_uint64), ('ms_first_pass', C.c_float),
-                ('reserved0', C.c_uint32), ('first_node_tests', C.c_uint64), ('first_exact_tests', C.c_uint64),
+                ('path_flags', C.c_uint32), ('first_node_tests', C.c_uint64), ('first_exact_tests', C.c_uint64),
                 ('cull_sphere_tests', C.c_uint64), ('cull_sat_tests', C.c_uint64)]
 
 

@@ -175,6 +175,13 @@ def sweep_scene(seed=0):
     return random_scene(12, 155, 2, seed, ico_r=(0.02, 0.06), box_ext=(0.02, 0.3), workspace=(WIDE_LO, WIDE_HI))
 
 
+def sweep_scene_sparse(seed=0):
+    """12 boxes + 38 level-3 icospheres over the same box (48,784 triangles):
+    fewer, finer obstacles, so about 40 % of the 32-waypoint random walks
+    collide instead of nearly all."""
+    return random_scene(12, 38, 3, seed, ico_r=(0.02, 0.06), box_ext=(0.02, 0.3), workspace=(WIDE_LO, WIDE_HI))
+
+
 def served_large_scene(seed=0):
     """Dense scene plus 225 extra level-2 icospheres (~500k triangles)."""
     base = discrete_dense(seed)

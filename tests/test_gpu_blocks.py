@@ -59,12 +59,14 @@ def test_select_known_answer(ctx, n, p):
     assert np.array_equal(idx.cpu().numpy()[:len(ref)], ref)
 
 
-@pytest.mark.parametrize('which', ['small_tris', 'small_edges', 'dense_tris', 'one', 'two', 'dupes'])
+@pytest.mark.parametrize('which', ['small_tris', 'small_edges', 'dense_tris', 'dense3_tris', 'dense3_edges', 'one', 'two',
+                                   'dupes'])
 def test_lbvh_bit_identical_to_canonical(ctx, which):
-    if which in ('small_tris', 'small_edges', 'dense_tris'):
-        m = scenes.discrete_small() if which != 'dense_tris' else scenes.discrete_dense(ico_level=2)
+    if which in ('small_tris', 'small_edges', 'dense_tris', 'dense3_tris', 'dense3_edges'):
+        m = {'dense_tris': lambda: scenes.discrete_dense(ico_level=2), 'dense3_tris': scenes.discrete_dense,
+             'dense3_edges': scenes.discrete_dense}.get(which, scenes.discrete_small)()
         v = m.verts.astype(np.float32)
-        if which == 'small_edges':
+        if which in ('small_edges', 'dense3_edges'):
             e = O.unique_edges(m.tris)
             P = v[e]
         else:

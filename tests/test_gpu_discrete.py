@@ -315,3 +315,29 @@ def test_plain_path_upstream_shape(setup, panda):
             base = a['flags']
         assert np.array_equal(a['flags'], base)
         det.close()
+
+
+@pytest.fixture(scope='module')
+def dense(ctx, panda):
+    mesh = scenes.discrete_dense()  # the graded 428,448-triangle scene
+    return rtcd.Robot(ctx, panda), rtcd.Scene.from_mesh(ctx, mesh), O.Robot(panda), O.Scene(mesh)
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_graded_dense_scene(dense, panda, name, okind):
+    """The graded RobotToObs / ObsToRobot workload's scene (64 boxes, 256
+    level-3 icospheres, the 100k-triangle noisy sphere: 428,448 triangles) at
+    4,096 uniform poses: flags and upstream counts equal the FP64 oracle's
+    outside the band, with and without the cull, and the two-way union."""
+    robot, scene, orob, osc = dense
+    q = scenes.uniform_poses(panda, 4096, seed=0)
+    ref = O.discrete(okind, orob, osc, q)
+    det = rtcd.Detector(robot.ctx, name, robot, scene)
+    _compare(det.check(q, counts=True), ref)
+    _compare(det.check(q, counts=True, flags=rtcd.CHECK_NO_CULL), ref)
+    assert np.array_equal(det.check(q)['flags'], det.check(q, counts=True)['flags'])
+    other = O.discrete(1 - okind, orob, osc, q)
+    both = det.check(q, flags=rtcd.CHECK_TWO_WAY)['flags']
+    band = (ref['band'] | other['band']).astype(bool)
+    assert not ((both != (ref['hit'] | other['hit'])) & ~band).any()
+    assert 0.3 < ref['hit'].mean() < 0.95
