@@ -150,6 +150,10 @@ typedef struct {
                                         them round-robin and the call waits for every group of plain_streams
                                         frames (upstream NSTREAM = 4 and its thread pool,
                                         RTCD/CollisionDetector/CollisionDetector.h:396-433); 0 = 4, at most 16 */
+    uint32_t top_nodes_shared;       /* discrete fused form: wide scene-tree nodes (breadth-first from the root: its
+                                        top levels) each block copies to shared memory and its descents read
+                                        there; 0 = none, at most 256 (the autotuner tries 0 and 85, the first
+                                        four levels) */
     uint32_t sweep_unstaged;         /* sweeps: 0 = the light pass stages each trajectory's FK (and quadratic fit)
                                         in shared memory when the batch's longest trajectory fits; 1 = sphere
                                         centres and control points go through global memory (separate FK and

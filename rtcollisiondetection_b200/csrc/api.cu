@@ -842,6 +842,8 @@ rtcd_status rtcd_scene_create(rtcd_ctx* ctx, const float* verts, uint32_t n_vert
         dv.tri_cut = sc->tri_cut.as<float4>();
         dv.edge_cut = sc->edge_cut.as<float4>();
         dv.n_tri_cut = (uint32_t) wt.cut.size() / 2;
+        dv.n_tri_wide = wt.nodes;
+        dv.n_edge_wide = we.nodes;
         dv.n_edge_cut = (uint32_t) we.cut.size() / 2;
         // a depth-first lane descent keeps at most 3 siblings per level plus the last node's 4 children
         dv.edge_wide_lane = (kWide - 1) * we.depth + kWide <= (uint32_t) kStack ? 1u : 0u;
@@ -911,6 +913,7 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         if (!d->cfg.frame_size) d->cfg.frame_size = 1024;
         if (!d->cfg.plain_streams) d->cfg.plain_streams = 4;
         RTCD_REQUIRE(d->cfg.plain_streams <= 16, "plain_streams must be at most 16");
+        RTCD_REQUIRE(d->cfg.top_nodes_shared <= 256, "top_nodes_shared must be at most 256");
         int lo_prio = 0, hi_prio = 0;
         cuda_check(cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio), "cudaDeviceGetStreamPriorityRange");
         const int prio = std::min(lo_prio, std::max(hi_prio, (int) d->cfg.stream_priority));
@@ -1008,6 +1011,7 @@ const SceneDev& scene_loop(rtcd_scene* sc) {
     dv.edge_wide_root = w.root;
     dv.edge_cut = sc->loop_cut.as<float4>();
     dv.n_edge_cut = (uint32_t) w.cut.size() / 2;
+    dv.n_edge_wide = w.nodes;
     dv.edge_wide_lane = (kWide - 1) * w.depth + kWide <= (uint32_t) kStack ? 1u : 0u;
     dv.wide_front = std::max(dv.wide_front, wide_frontier(w.depth));
     cuda_check(cudaStreamSynchronize(s), "loop-edge trees");
@@ -1156,6 +1160,7 @@ static void traverse(rtcd_detector* d, bool r2o, const DiscreteArgs& A, uint32_t
     uint32_t* wc = d->wave_counts.as<uint32_t>();
     WaveArgs W{};
     W.d = A;
+    W.top_nodes = d->cfg.top_nodes_shared;
     W.cand = d->cand.as<uint2>();
     W.cand_count = wc;
     W.cand_cap = cap;
@@ -1811,7 +1816,9 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                     apply_launch_shape(d);
                     fail(st, g_last_error);
                 }
-                ms[rep] = stt.ms_traverse;
+                // sweeps: the whole check (the staged light pass runs the FK and fit the unstaged
+                // form leaves to the kernels before it); discrete: the traversal span
+                ms[rep] = discrete ? stt.ms_traverse : stt.ms_total;
             }
             std::sort(ms + 1, ms + 4);
             if (ms[2] < best_t) {
@@ -1838,9 +1845,12 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
             c.light_steps = light;
             time_cfg(c);
         }
-        if (!discrete) {  // the binary or the wide edge tree
+        if (!discrete) {  // the binary or the wide edge tree, then staged or unstaged centres
             rtcd_config c = best;
             c.stage_b_form = best.stage_b_form == 1 ? 0u : 1u;
+            time_cfg(c);
+            c = best;
+            c.sweep_unstaged = best.sweep_unstaged ? 0u : 1u;
             time_cfg(c);
         }
         if (discrete) {
@@ -1854,6 +1864,11 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                     c.stage_b_chunk = form == 2 ? std::max(1u, chunk / 16) : (form >= 3 ? std::max(1u, chunk / 4) : chunk);
                     time_cfg(c);
                 }
+            if (best.stage_b_form == 0 || best.stage_b_form >= 3) {  // the fused form: top levels in shared memory
+                rtcd_config c = best;
+                c.top_nodes_shared = best.top_nodes_shared ? 0u : 85u;  // 1 + 4 + 16 + 64: the first four levels
+                time_cfg(c);
+            }
         }
         d->cfg = best;
         apply_launch_shape(d);

@@ -1022,7 +1022,7 @@ struct ObbTest {
 // warps to hide the node-load latency; measured on the 65,536-pose workload).
 template <bool R2O, bool PACKET>
 __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
-    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front]
+    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front], then W.top_nodes staged wide nodes
     __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
     __shared__ uint32_t s_hits[kAbWarps];  // a lane of the warp's current stage-B step hit its pose
     const DiscreteArgs& A = W.d;
@@ -1038,6 +1038,11 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
     const float4* __restrict__ lp = R2O ? R.edge_prims : R.tri_prims;
     const uint32_t n_items = *A.n_items;
     const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
+    // the tree's top levels in shared memory (its first nodes, breadth-first), read by every descent
+    const uint32_t n_top = min(W.top_nodes, R2O ? S.n_tri_wide : S.n_edge_wide);
+    float4* s_top = reinterpret_cast<float4*>(s_front + ((kAbWarps * S.wide_front + 3u) & ~3u));
+    for (uint32_t k = threadIdx.x; k < n_top * 2 * kWide; k += blockDim.x) s_top[k] = __ldg(wn + k);
+    __syncthreads();
     uint32_t st[kStack];
     unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0, n_cand = 0, n_node = 0;
     while (true) {
@@ -1248,7 +1253,8 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 continue;
             }
             if (sp == 0) break;
-            if (!wide_step(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand)) break;
+            if (!wide_step(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand, s_top, n_top))
+                break;
         }
         if (overflow && lane == 0) mark_overflow(W, item);
         __syncwarp();
@@ -1548,6 +1554,10 @@ void launch_stage_b_heavy(bool r2o, const RobotDev& R, const SceneDev& S, const 
 // The fused kernel's frontier lives in dynamic shared memory, sized from the
 // scene's wide-tree depth.
 static size_t stage_ab_smem(const SceneDev& S) { return sizeof(uint32_t) * kAbWarps * (size_t) S.wide_front; }
+// with top_nodes wide nodes staged after the frontiers (16-byte aligned)
+static size_t stage_ab_smem(const SceneDev& S, uint32_t top_nodes) {
+    return ((stage_ab_smem(S) + 15) & ~size_t(15)) + (size_t) top_nodes * 2 * kWide * sizeof(float4);
+}
 
 template <class K>
 static uint32_t stage_ab_grid(K kernel, size_t smem) {
@@ -1585,8 +1595,13 @@ void launch_subtree(bool r2o, const RobotDev& R, const SceneDev& S, const WaveAr
 
 void launch_stage_ab(bool r2o, bool packets, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t blocks,
                      cudaStream_t s) {
-    stage_ab_blocks(r2o, packets, S);  // sets the shared-memory limit before the first launch
-    const size_t smem = stage_ab_smem(S);
+    const uint32_t top = std::min(W.top_nodes, r2o ? S.n_tri_wide : S.n_edge_wide);
+    const size_t smem = stage_ab_smem(S, top);
+    // sets the shared-memory limit before the first launch, and caps the grid at what fits
+    blocks = std::min(blocks, packets ? (r2o ? stage_ab_grid(k_stage_ab<true, true>, smem)
+                                             : stage_ab_grid(k_stage_ab<false, true>, smem))
+                                      : (r2o ? stage_ab_grid(k_stage_ab<true, false>, smem)
+                                             : stage_ab_grid(k_stage_ab<false, false>, smem)));
     if (packets) {
         if (r2o)
             k_stage_ab<true, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);

@@ -46,6 +46,7 @@ struct SceneDev {
     const float4* edge_cut;
     uint32_t n_tri_cut, n_edge_cut;
     uint32_t edge_wide_lane;  // nonzero when a lane stack of kStack entries holds a wide edge-tree descent
+    uint32_t n_tri_wide, n_edge_wide;  // nodes of the two wide trees
 };
 
 struct DiscreteArgs {
@@ -73,6 +74,7 @@ constexpr int kTravThreads = 128;
 // the buffer are flagged and re-run by the fused kernel.
 struct WaveArgs {
     DiscreteArgs d;
+    uint32_t top_nodes;        // fused form: wide-tree nodes (from the root) each block stages in shared memory
     uint2* cand;               // (item word pose * n_links + link, scene primitive)
     uint32_t* cand_count;      // zeroed before stage A; may exceed cand_cap
     uint32_t cand_cap;

@@ -49,10 +49,14 @@ __device__ __forceinline__ bool wide_round(const float4& a, const float4& b, uin
 // the lanes (4 lanes per node when at most 8 are waiting, 2 when at most 16,
 // else one lane tests all four children of its node, so a step costs about
 // one box test per lane); at most 32 * kWide leaves are appended per step.
+// top / n_top: a shared-memory copy of the tree's first n_top nodes (they are
+// numbered breadth-first, so these are its top levels); records of those
+// nodes are read from it instead of global memory.
 template <class Test>
 __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_t* fr, int& sp, uint32_t* cb, int& nc,
                                           const Test& test, uint32_t front_cap, uint32_t* err,
-                                          unsigned long long& n_node, unsigned long long& n_cand) {
+                                          unsigned long long& n_node, unsigned long long& n_cand,
+                                          const float4* top = nullptr, uint32_t n_top = 0) {
     const int lane = threadIdx.x & 31;
     const int lg = sp <= 8 ? 2 : (sp <= 16 ? 1 : 0), g = 1 << lg;
     const int take = min(sp, 32 >> lg);
@@ -73,9 +77,14 @@ __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_
             ra[r] = make_float4(0.f, 0.f, 0.f, 0.f);
             rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
             if (r0 + r < rounds && node != kNone) {
-                const float4* rec = wn + 2ull * (kWide * (size_t) node + c0 + (r0 + r) * g);
-                ra[r] = __ldg(rec);
-                rb[r] = __ldg(rec + 1);
+                const size_t at = 2ull * (kWide * (size_t) node + c0 + (r0 + r) * g);
+                if (node < n_top) {
+                    ra[r] = top[at];
+                    rb[r] = top[at + 1];
+                } else {
+                    ra[r] = __ldg(wn + at);
+                    rb[r] = __ldg(wn + at + 1);
+                }
             }
         }
 #pragma unroll

@@ -341,3 +341,18 @@ def test_graded_dense_scene(dense, panda, name, okind):
     band = (ref['band'] | other['band']).astype(bool)
     assert not ((both != (ref['hit'] | other['hit'])) & ~band).any()
     assert 0.3 < ref['hit'].mean() < 0.95
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_top_levels_in_shared_memory_agree(dense, panda, name, okind):
+    """The fused kernel with the wide tree's top levels staged in shared memory
+    (85 nodes: the first four levels; 256: more) gives the same flags and
+    counts as without staging."""
+    robot, scene, _, _ = dense
+    q = scenes.uniform_poses(panda, 2048, seed=5)
+    base = rtcd.Detector(robot.ctx, name, robot, scene).check(q, counts=True)
+    for top in (85, 256):
+        det = rtcd.Detector(robot.ctx, name, robot, scene, top_nodes_shared=top)
+        out = det.check(q, counts=True)
+        assert np.array_equal(out['flags'], base['flags']) and np.array_equal(out['counts'], base['counts'])
+        det.close()
