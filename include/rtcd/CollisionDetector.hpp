@@ -127,6 +127,11 @@ public:
         if (!det_) check_status(rtcd_detector_create(ctx_.get(), to_kind(TYPE), robot_->get(), scene_->get(), nullptr, &det_));
     }
     void setNCheck(uint32_t n) { nCheck_ = n; }
+    // The curve detectors follow the reference's semantics by default (its
+    // loop edges counted where they enter a swept piece: RTCD_CHECK_SURFACE);
+    // solid semantics (every obstacle edge within r of a sphere's path, plus
+    // the start and end spheres of quadratic pieces) on request.
+    void setSolidSweeps(bool solid) { solid_ = solid; }
 
     // Runs the staged query; upstream check() (CollisionDetector.h:422-471).
     void check() {
@@ -136,8 +141,10 @@ public:
         uint32_t n = nCheck_ ? nCheck_ : (uint32_t) robot_->staged();
         flags_.assign(n, 0);
         counts_.assign(n, 0);
+        const bool curve = TYPE == LinkType::LINEAR_CURVE || TYPE == LinkType::QUADRATIC_CURVE;
+        const uint32_t sem = curve && !solid_ ? RTCD_CHECK_SURFACE : 0u;
         check_status(rtcd_check(det_, q.data(), off.empty() ? nullptr : off.data(), n, flags_.data(), nullptr,
-                                counts_.data(), RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_COUNTS, nullptr));
+                                counts_.data(), RTCD_CHECK_HOST_BUFFERS | RTCD_CHECK_COUNTS | sem, nullptr));
     }
 
     // Upstream downloadResult(std::vector<uint>&): per-pose (per-trajectory)
@@ -158,6 +165,7 @@ private:
     Scene* scene_;
     rtcd_detector* det_ = nullptr;
     uint32_t nCheck_ = 0;
+    bool solid_ = false;
     std::vector<uint8_t> flags_;
     std::vector<uint32_t> counts_;
 };

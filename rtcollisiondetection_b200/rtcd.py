@@ -487,14 +487,17 @@ class CollisionDetector:
     (``CCRobotWrapper.h:39-46``), ``setNCheck(n)`` sets the query size
     (``CollisionDetector.h:354``), ``check()`` runs it and ``downloadResult``
     returns the per-pose (per-trajectory) upstream hit counts, nonzero = hit
-    (``CollisionDetector.h:62``).
+    (``CollisionDetector.h:62``).  The curve detectors follow the reference's
+    semantics (loop edges entering a swept piece, RTCD_CHECK_SURFACE) unless
+    ``solid_sweeps`` is set.
     """
 
-    def __init__(self, ctx, kind, robot=None, scene=None):
+    def __init__(self, ctx, kind, robot=None, scene=None, solid_sweeps=False):
         self.ctx, self.kind = ctx, KIND_NAMES.get(kind, kind)
         self.robot, self.scene, self.det = robot, scene, None
         self.poses, self.traj_off, self.n = None, None, 0
         self.result = None
+        self.solid_sweeps = solid_sweeps
 
     def setupScene(self, scene):
         self.scene = scene
@@ -522,7 +525,7 @@ class CollisionDetector:
         self.buildSBT()
         if self.det.sweep:
             traj = np.asarray(self.traj_off[:self.n + 1], np.uint32)
-            self.result = self.det.check(self.poses, traj, counts=True)
+            self.result = self.det.check(self.poses, traj, counts=True, surface=not self.solid_sweeps)
         else:
             self.result = self.det.check(self.poses[:self.n], counts=True)
 
