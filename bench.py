@@ -644,8 +644,13 @@ def main():
                     help='requests of the served mix submitted at once to measure saturated throughput (0: skip)')
     ap.add_argument('--dry', action='store_true', help='no GPU: the multi-rank plumbing with the CPU oracle over gloo')
     ap.add_argument('--dry-units', type=int, default=256, help='units per rank of a --dry run')
+    ap.add_argument('--units', type=int, default=0,
+                    help='poses / trajectories per GPU instead of the configuration\'s (a smaller case for profiling)')
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.units:
+        cfg['n'] = args.units
+        cfg['workload'] += ' (%d units per GPU instead)' % args.units
     if args.gpus > 1 and 'WORLD_SIZE' not in os.environ:
         sys.exit(spawn_ranks(args.gpus))
     rank = int(os.environ.get('RANK', 0))

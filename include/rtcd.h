@@ -155,8 +155,9 @@ typedef struct {
                                         there; 0 = none, at most 256 (the autotuner tries 0 and 85, the first
                                         four levels) */
     uint32_t sweep_unstaged;         /* sweeps: 0 = the light pass stages each trajectory's FK (and quadratic fit)
-                                        in shared memory when the batch's longest trajectory fits; 1 = sphere
-                                        centres and control points go through global memory (separate FK and
+                                        in shared memory when the batch's longest trajectory fits and the batch
+                                        has at least four trajectories per resident block; 1 = sphere centres
+                                        and control points always go through global memory (separate FK and
                                         fit kernels) */
 } rtcd_config;
 

@@ -1264,8 +1264,8 @@ static int fit_weights(int nc, int nt, double* W /* nc*nt */) {
             G[i * nc + j] = v / d;
         }
     }
+    double* y = (double*) malloc(sizeof(double) * (size_t) nc);  /* any number of control points */
     for (int t = 0; t < nt; ++t) {
-        double y[256];
         for (int i = 0; i < nc; ++i) {  /* L y = b */
             double v = B[t * nc + i];
             for (int k = 0; k < i; ++k) v -= G[i * nc + k] * y[k];
@@ -1278,6 +1278,7 @@ static int fit_weights(int nc, int nt, double* W /* nc*nt */) {
         }
         for (int i = 0; i < nc; ++i) W[i * nt + t] = y[i];
     }
+    free(y);
     free(B);
     free(G);
     return 0;

@@ -1464,7 +1464,12 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     uint32_t max_pieces = 0;
     for (uint32_t i = 0; i < n; ++i) max_pieces = std::max(max_pieces, piece_off[i + 1] - piece_off[i]);
     const uint32_t max_nc = quad ? quad_ctrl_count(max_wp) : 0;
-    const bool staged = !d->cfg.sweep_unstaged && sweep_staged_smem(quad, R.n_links, max_wp, max_nc, max_pieces) != 0;
+    // A staged block works on one trajectory at a time, so the staged pass needs several trajectories
+    // per resident block to keep the GPU busy: a batch of a few trajectories would run on a few
+    // blocks (one trajectory of 128 waypoints is 8,128 units for one block) where the unstaged pass
+    // spreads its units over the whole grid.
+    const bool staged = !d->cfg.sweep_unstaged && n >= 4 * d->blocks &&
+                        sweep_staged_smem(quad, R.n_links, max_wp, max_nc, max_pieces) != 0;
     d->last_path_flags = staged ? 1u : 0u;
     const bool timed = (flags & RTCD_CHECK_TIMING) != 0;
     d->timed = timed;

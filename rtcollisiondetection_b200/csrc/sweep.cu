@@ -168,7 +168,10 @@ __device__ __forceinline__ T poly3(const T* c, T u) { return ((c[3] * u + c[2]) 
 // Roots in [0, 1] of the cubic c[3] u^3 + ... + c[0]: the derivative's roots
 // split [0, 1] into monotone brackets, each bracket with a sign change is
 // solved by safeguarded Newton (falls back to bisection when a step leaves the
-// bracket).  `iters` Newton steps per bracket.
+// bracket), at most `iters` steps per bracket.  The iteration stops once a
+// step no longer moves u (or u is an exact root): a converged Newton point
+// sits on the bracket's end, and bisecting on from there would throw the
+// root away.
 template <class T>
 __device__ int cubic_roots01(const T* c, T* out, int iters) {
     T br[4];
@@ -195,11 +198,13 @@ __device__ int cubic_roots01(const T* c, T* out, int iters) {
         if ((flo > T(0)) == (fhi > T(0))) continue;
         T u = T(0.5) * (lo + hi);
         for (int it = 0; it < iters; ++it) {
-            T f = poly3(c, u);
+            const T f = poly3(c, u);
+            if (f == T(0)) break;
             if ((f > T(0)) == (flo > T(0))) lo = u; else hi = u;
-            T df = (T(3) * c[3] * u + T(2) * c[2]) * u + c[1];
+            const T df = (T(3) * c[3] * u + T(2) * c[2]) * u + c[1];
             T nu = df != T(0) ? u - f / df : T(0.5) * (lo + hi);
-            if (!(nu > lo && nu < hi)) nu = T(0.5) * (lo + hi);
+            if (!(nu >= lo && nu <= hi)) nu = T(0.5) * (lo + hi);
+            if (nu == u) break;
             u = nu;
         }
         out[n++] = u;

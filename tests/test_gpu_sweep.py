@@ -179,14 +179,17 @@ def test_staged_and_unstaged_light_pass_agree(sweep_setup, panda, kind):
     oracle sees no marginal pair; a batch with a trajectory too long for the
     staging falls back to the unstaged pass with the same results."""
     robot, scene, orob, osc = sweep_setup
-    n_wp = scenes.log_uniform_counts(300, 8, 64, seed=11)
-    n_wp[7] = 700  # longer than the staging holds: the whole batch takes the unstaged pass
-    q, off = scenes.random_walk_trajectories(panda, 300, n_wp, seed=11)
-    staged = rtcd.Detector(robot.ctx, kind, robot, scene)
+    n_wp = scenes.log_uniform_counts(1200, 8, 64, seed=11)
+    n_wp[1100] = 700  # longer than the staging holds: the whole batch takes the unstaged pass
+    q, off = scenes.random_walk_trajectories(panda, 1200, n_wp, seed=11)
+    # one block per SM: 1,100 trajectories are enough for the staged pass (at least 4 per block)
+    staged = rtcd.Detector(robot.ctx, kind, robot, scene, traverse_blocks_per_sm=1)
     unstaged = rtcd.Detector(robot.ctx, kind, robot, scene, sweep_unstaged=1)
     quad = kind == 'Quadratic'
     for surface in (False, True):
-        for a, b in ((q[:off[7]], off[:8]), (q, off)):
+        for a, b, path in ((q[:off[1100]], off[:1101], 1), (q, off, 0)):
+            staged.check(a, b, surface=surface)
+            assert staged.stats()['path_flags'] & 1 == path
             ref = O.sweep(quad, orob, osc, a, b, surface=surface)
             x = staged.check(a, b, segments=True, counts=True, surface=surface)
             y = unstaged.check(a, b, segments=True, counts=True, surface=surface)
