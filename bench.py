@@ -61,6 +61,9 @@ CONFIGS = {
     'c2_200k': dict(kind='RobotToObs', n=65536, scene='dense200k',
                     workload='RobotToObs, 65,536 uniform Panda poses, dense scene with level-2 icospheres '
                              '(64 boxes + 256 level-2 icospheres + 100k-tri noisy sphere, 182,688 tris)'),
+    'c2_cube': dict(kind='RobotToObs', n=65536, scene='dense_cube',
+                    workload='RobotToObs, 65,536 uniform Panda poses, the dense composition (428,448 tris) packed '
+                             'into the 1 m workspace cube in front of the robot (box extents U(0.02, 0.6) m)'),
     'c3s': dict(kind='Linear', n=4096, scene='sweep_sparse', wp=32,
                 workload='Linear sweep, 4,096 random-walk trajectories x 32 waypoints, 64 spheres, sparse '
                          '48,784-tri scene (12 boxes + 38 level-3 icospheres; ~40 % of trajectories collide)'),
@@ -94,7 +97,7 @@ def make_inputs(cfg, rank, scenes):
         mesh = scenes.reference_scene(cfg['scene'][4:])
     else:
         mesh = {'dense': scenes.discrete_dense, 'small': scenes.discrete_small,
-                'dense200k': lambda: scenes.discrete_dense(ico_level=2),
+                'dense200k': lambda: scenes.discrete_dense(ico_level=2), 'dense_cube': scenes.discrete_dense_cube,
                 'sweep': scenes.sweep_scene, 'sweep_sparse': scenes.sweep_scene_sparse}[cfg['scene']]()
     spheres = scenes.synth_spheres(model) if cfg['kind'] in ('Linear', 'Quadratic') else None
     if cfg['kind'] in ('Linear', 'Quadratic'):

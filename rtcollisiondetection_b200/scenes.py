@@ -170,6 +170,13 @@ def discrete_dense(seed=0, ico_level=3):
                         workspace=(WIDE_LO, WIDE_HI))
 
 
+def discrete_dense_cube(seed=0):
+    """The dense composition packed into the 1 m workspace cube of the small
+    scene, as the configuration literally reads (box extents U(0.02, 0.6) m):
+    428,448 triangles in front of the robot, where nearly every pose collides."""
+    return random_scene(64, 256, 3, seed, big_sphere_tris=100_000)
+
+
 def sweep_scene(seed=0):
     """12 boxes + 155 level-2 icospheres: 49,744 triangles."""
     return random_scene(12, 155, 2, seed, ico_r=(0.02, 0.06), box_ext=(0.02, 0.3), workspace=(WIDE_LO, WIDE_HI))
