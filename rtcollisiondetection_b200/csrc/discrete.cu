@@ -137,98 +137,43 @@ __device__ __forceinline__ uint32_t item_word(const DiscreteArgs& A, uint32_t n_
 }
 
 // One thread per (pose, link): the link OBB against every obstacle OBB, with a
-// bounding-sphere reject before the full test.  Few pairs pass the sphere
-// test (on the 65,536-pose dense scene 0.7 M of 92 M), and a 15-axis SAT run
-// by one lane held its whole warp for the SAT's length; so a lane whose pair
-// passes only queues it (warp queue of (lane, obstacle) words), and whenever
-// 32 are queued every lane runs one of them - on another lane's item, whose
-// world OBB the block keeps in shared memory.  A SAT of an item already hit
-// is skipped; the obstacle loop is warp-uniform and ends once every lane of
-// the warp is hit or idle.
-constexpr int kCullThreads = 256, kCullWarps = kCullThreads / 32;
-
-__device__ __forceinline__ ObbW obb_from(const float* v) {
-    ObbW o;
-    o.c = mk(v[0], v[1], v[2]);
-    o.h = mk(v[3], v[4], v[5]);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) o.ax[a] = mk(v[6 + 3 * a], v[7 + 3 * a], v[8 + 3 * a]);
-    return o;
-}
-
-__global__ void __launch_bounds__(kCullThreads) k_cull(const RobotDev R, const float* __restrict__ sobb, uint32_t n_obs,
-                                                      const float4* __restrict__ T, uint32_t n,
-                                                      uint8_t* __restrict__ mask, bool link_major,
-                                                      unsigned long long* stats) {
+// bounding-sphere reject before the full test.
+__global__ void __launch_bounds__(256) k_cull(const RobotDev R, const float* __restrict__ sobb, uint32_t n_obs,
+                                             const float4* __restrict__ T, uint32_t n, uint8_t* __restrict__ mask,
+                                             bool link_major, unsigned long long* stats) {
     __shared__ float s_obb[kCullChunk * 16];
-    __shared__ float s_item[kCullThreads][16];    // world OBB of each thread's item: centre, half sizes, axes
-    __shared__ uint32_t s_queue[kCullWarps][64];  // per warp: queued SATs, lane << 16 | chunk-local obstacle
-    __shared__ volatile uint8_t s_hit[kCullThreads];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t pose = i / R.n_links, link = i % R.n_links;
-    const bool active = pose < n && link >= R.first_link;
-    f3 ac = mk(0.f, 0.f, 0.f);
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t pose = i / R.n_links, link = i % R.n_links;
+    bool active = pose < n && link >= R.first_link;
+    ObbW A;
     float arad = 0.f;
     if (active) {
-        const ObbW A = world_obb(R.obb[link], T + ((size_t) pose * R.n_links + link) * 3);
-        float* v = s_item[threadIdx.x];
-        v[0] = A.c.x; v[1] = A.c.y; v[2] = A.c.z;
-        v[3] = A.h.x; v[4] = A.h.y; v[5] = A.h.z;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            v[6 + 3 * a] = A.ax[a].x; v[7 + 3 * a] = A.ax[a].y; v[8 + 3 * a] = A.ax[a].z;
-        }
-        ac = A.c;
+        A = world_obb(R.obb[link], T + ((size_t) pose * R.n_links + link) * 3);
         arad = sqrtf(dot(A.h, A.h)) + 2e-5f;
     }
-    s_hit[threadIdx.x] = 0;
-    uint32_t* q = s_queue[warp];
-    int qn = 0;
+    bool hit = false;
     unsigned long long n_sphere = 0, n_sat = 0;  // bounding-sphere tests, then the SATs they let through
-    // the warp runs `take` queued SATs, one per lane, then drops them from the queue
-    auto run_queue = [&](int take) {
-        if (lane < take) {
-            const uint32_t e = q[lane];
-            const uint32_t who = (uint32_t) warp * 32 + (e >> 16);
-            if (!s_hit[who]) {
-                ++n_sat;
-                if (obb_overlap(obb_from(s_item[who]), s_obb + (e & 0xffffu) * 16)) s_hit[who] = 1;
-            }
-        }
-        __syncwarp();
-        const uint32_t rest = lane + take < qn ? q[lane + take] : 0u;
-        __syncwarp();
-        if (lane + take < qn) q[lane] = rest;
-        qn -= take;
-        __syncwarp();
-    };
     for (uint32_t base = 0; base < n_obs; base += kCullChunk) {
-        const uint32_t m = min((uint32_t) kCullChunk, n_obs - base);
+        uint32_t m = min((uint32_t) kCullChunk, n_obs - base);
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < m * 16; k += blockDim.x) s_obb[k] = sobb[(size_t) base * 16 + k];
         __syncthreads();
-        for (uint32_t o = 0; o < m; ++o) {
-            if ((o & 7) == 0 && !__any_sync(0xffffffffu, active && !s_hit[threadIdx.x])) break;  // warp-uniform
-            bool want = false;
-            if (active && !s_hit[threadIdx.x]) {
+        if (active && !hit) {
+            for (uint32_t o = 0; o < m; ++o) {
                 const float* B = s_obb + o * 16;
-                const f3 d = mk(B[0], B[1], B[2]) - ac;
-                const float rr = arad + B[15];
+                f3 d = mk(B[0], B[1], B[2]) - A.c;
+                float rr = arad + B[15];
                 ++n_sphere;
-                want = dot(d, d) <= rr * rr;
+                if (dot(d, d) > rr * rr) continue;
+                ++n_sat;
+                if (obb_overlap(A, B)) {
+                    hit = true;
+                    break;
+                }
             }
-            const uint32_t wm = __ballot_sync(0xffffffffu, want);
-            if (want) q[qn + __popc(wm & lt)] = ((uint32_t) lane << 16) | o;
-            qn += __popc(wm);
-            __syncwarp();
-            if (qn >= 32) run_queue(32);
         }
-        while (qn > 0) run_queue(min(qn, 32));  // the queue refers to this chunk's obstacles
     }
-    __syncwarp();
-    if (pose < n) mask[link_major ? (size_t) link_slot(link, R.n_links) * n + pose : i] = s_hit[threadIdx.x] ? 1 : 0;
+    if (pose < n) mask[link_major ? (size_t) link_slot(link, R.n_links) * n + pose : i] = hit ? 1 : 0;
     warp_count(stats + kStatCullSpheres, n_sphere);
     warp_count(stats + kStatCullSats, n_sat);
 }
@@ -237,8 +182,7 @@ void launch_cull(const RobotDev& R, const SceneDev& S, const float4* d_T, uint32
                  unsigned long long* d_stats, cudaStream_t s) {
     uint32_t total = n * R.n_links;
     if (!total) return;
-    k_cull<<<(total + kCullThreads - 1) / kCullThreads, kCullThreads, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask,
-                                                                           link_major, d_stats);
+    k_cull<<<(total + 255) / 256, 256, 0, s>>>(R, S.obbs, S.n_obs, d_T, n, d_mask, link_major, d_stats);
     cuda_check(cudaGetLastError(), "k_cull");
 }
 
