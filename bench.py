@@ -345,8 +345,13 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
            'p99_margin_ms_all': 2.0 - float(np.percentile(lat, 99))}
     if sat:
         out['saturated'] = sat
+    # the slowest requests: what they were and when they arrived (tail diagnosis)
+    scene_of = {id(det): i for i, d in enumerate(dets) for det in d.values()}
+    worst = np.argsort(-lat)[:8]
+    out['slowest'] = [{'ms': round(float(lat[i]), 3), 'arrival_s': round(float(arrivals[i]), 3),
+                       'kind': ['ObsToRobot', 'RobotToObs', 'Linear', 'Quadratic'][reqs[i][0].kind],
+                       'units': int(reqs[i][3]), 'scene': scene_of[id(reqs[i][0])]} for i in worst]
     if details:
-        scene_of = {id(det): i for i, d in enumerate(dets) for det in d.values()}
         out['details'] = {'latency_ms': lat, 'discrete': disc, 'size': sizes,
                           'scene': np.array([scene_of[id(r[0])] for r in reqs]),
                           'kind': [r[0].kind for r in reqs]}
