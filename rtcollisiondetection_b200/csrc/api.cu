@@ -476,6 +476,34 @@ struct PlainPool {
     }
 };
 
+// Copies between the caller's host arrays and the pinned staging: a single
+// thread copies a few GB/s, so a copy of a megabyte or more is split over a
+// process-wide pool of four threads (when another caller holds the pool, the
+// copy runs on the calling thread).
+static void stage_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kSplit = 1u << 20, kParts = 4;
+    if (bytes < kSplit) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    static std::mutex mu;
+    static PlainPool* pool = nullptr;  // lives until exit
+    std::unique_lock<std::mutex> lk(mu, std::try_to_lock);
+    if (!lk.owns_lock()) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    if (!pool) pool = new PlainPool(kParts);
+    const size_t part = (bytes / kParts + 63) & ~size_t(63);
+    std::vector<std::function<void()>> jobs(kParts);
+    for (size_t k = 0; k < kParts; ++k) {
+        const size_t a = std::min(bytes, k * part), b = std::min(bytes, a + part);
+        if (b > a)
+            jobs[k] = [=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); };
+    }
+    pool->run(jobs);
+}
+
 struct rtcd_detector {
     rtcd_ctx* ctx = nullptr;
     rtcd_detector_kind kind = RTCD_OBS_TO_ROBOT;
@@ -1298,7 +1326,7 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
     if (host) {
         d->q.ensure(4ull * n * dof);
         d->pin_in.ensure(4ull * n * dof);
-        std::memcpy(d->pin_in.p, q, 4ull * n * dof);
+        stage_copy(d->pin_in.p, q, 4ull * n * dof);
         cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * n * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
@@ -1450,7 +1478,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     if (host) {
         d->q.ensure(4ull * total_wp * dof);
         d->pin_in.ensure(4ull * total_wp * dof);
-        std::memcpy(d->pin_in.p, q, 4ull * total_wp * dof);
+        stage_copy(d->pin_in.p, q, 4ull * total_wp * dof);
         cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
@@ -1620,7 +1648,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
                     for (uint32_t i = 0; i < n; ++i) n_seg += pieces_of(d->kind, traj_offsets[i + 1] - traj_offsets[i], f);
                 d->pin_in.ensure(std::max<size_t>(in_bytes, 16));
                 d->hq.ensure(std::max<size_t>(in_bytes, 16));
-                std::memcpy(d->pin_in.p, q, in_bytes);
+                stage_copy(d->pin_in.p, q, in_bytes);
                 gq = d->hq.as<float>();
                 d->hflags.ensure(n);
                 gflags = d->hflags.as<uint8_t>();
