@@ -340,6 +340,10 @@ def served_stream(ctx, seconds, rate=2000.0, seed=0, slots=4, plain_seconds=1.0,
            'p50_ms_all': float(np.percentile(lat, 50)), 'p99_ms_all': float(np.percentile(lat, 99)),
            'poses_per_s': poses / wall, 'trajectories_per_s': trajs / wall, 'batches': st['batches'],
            'queue_p50_ms': st['queue_p50_ms'], 'queue_p99_ms': st['queue_p99_ms'], 'run_p99_ms': st['run_p99_ms'],
+           'workspace_grows': st['workspace_grows'], 'grow_ms': st['grow_ms'],
+           'longest_launch': {'ms': st['run_max_ms'], 'at_s': st['run_max_at_s'], 'slot': st['run_max_slot'],
+                              'kind': ['ObsToRobot', 'RobotToObs', 'Linear', 'Quadratic'][st['run_max_kind']],
+                              'units': st['run_max_units'], 'grows': st['run_max_grows']},
            'scenes_tris': [m.n_tris for m in meshes],
            'p99_margin_ms_discrete_le4096': 2.0 - float(np.percentile(lat[disc], 99)),
            'p99_margin_ms_all': 2.0 - float(np.percentile(lat, 99))}

@@ -352,7 +352,15 @@ typedef struct {
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result ready, over completed requests */
     double queue_p50_ms, queue_p99_ms;      /* submit -> its launch started */
     double run_p99_ms;                      /* launch started -> result ready */
-    uint64_t reserved[1];
+    uint64_t workspace_grows;   /* device or pinned workspace re-allocations inside launches (each can
+                                 * synchronise the device, stalling every slot) */
+    double grow_ms;             /* host time those re-allocations took */
+    double run_max_ms;          /* the longest launch ... */
+    uint32_t run_max_kind;      /* ... its detector kind (rtcd_detector_kind) */
+    uint32_t run_max_units;     /* ... its poses or trajectory waypoints */
+    uint32_t run_max_grows;     /* ... re-allocations inside it */
+    uint32_t run_max_slot;      /* ... the slot that ran it (fast slots first) */
+    double run_max_at_s;        /* ... when it started, seconds after the last stats reset */
 } rtcd_server_stats;
 
 #define RTCD_WAIT_FOREVER (-1)
@@ -360,7 +368,10 @@ typedef struct {
 RTCD_API rtcd_status rtcd_server_create(rtcd_ctx* ctx, const rtcd_server_config* config, rtcd_server** out);
 /* Creates every slot's workspace for `det` and sizes it for launches of up to
  * max_units units (0 = the server's max_batch_units), so serving never
- * allocates (an allocation would synchronise the device).  Optional. */
+ * allocates (an allocation would synchronise the device).  Sweep detectors are
+ * prepared for trajectories of up to 128 waypoints, in both sweep semantics
+ * (this builds the scene's loop-edge trees).  Optional; rtcd_server_stats
+ * counts the re-allocations serving still made. */
 RTCD_API rtcd_status rtcd_server_prepare(rtcd_server* server, rtcd_detector* det, uint32_t max_units);
 /* Finishes every accepted request, then stops the workers. */
 RTCD_API rtcd_status rtcd_server_destroy(rtcd_server* server);

@@ -9,6 +9,7 @@
 // 354-471).
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -46,8 +47,26 @@ void DevBuf::release() {
 
 // Growth is geometric (at least 1.5x): cudaFree synchronises the device, so a
 // workspace that follows slowly rising batch sizes must not re-allocate often.
+GrowCounter& thread_grows() {
+    static thread_local GrowCounter c;
+    return c;
+}
+
+namespace {
+// Counts one re-allocation on this thread and the time from construction to destruction.
+struct GrowTimer {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    ~GrowTimer() {
+        GrowCounter& c = thread_grows();
+        ++c.grows;
+        c.ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+}  // namespace
+
 void DevBuf::ensure(size_t n) {
     if (n <= bytes && p) return;
+    GrowTimer timer;
     size_t want = std::max<size_t>(std::max<size_t>(n, 256), bytes + bytes / 2);
     release();
     cuda_check(cudaMalloc(&p, want), "cudaMalloc");
@@ -62,6 +81,7 @@ void HostBuf::release() {
 
 void HostBuf::ensure(size_t n) {
     if (n <= bytes && p) return;
+    GrowTimer timer;
     size_t want = std::max<size_t>(std::max<size_t>(n, 256), bytes + bytes / 2);
     release();
     cuda_check(cudaMallocHost(&p, want), "cudaMallocHost");
@@ -475,34 +495,6 @@ struct PlainPool {
         if (error) std::rethrow_exception(error);
     }
 };
-
-// Copies between the caller's host arrays and the pinned staging: a single
-// thread copies a few GB/s, so a copy of a megabyte or more is split over a
-// process-wide pool of four threads (when another caller holds the pool, the
-// copy runs on the calling thread).
-static void stage_copy(void* dst, const void* src, size_t bytes) {
-    constexpr size_t kSplit = 1u << 20, kParts = 4;
-    if (bytes < kSplit) {
-        std::memcpy(dst, src, bytes);
-        return;
-    }
-    static std::mutex mu;
-    static PlainPool* pool = nullptr;  // lives until exit
-    std::unique_lock<std::mutex> lk(mu, std::try_to_lock);
-    if (!lk.owns_lock()) {
-        std::memcpy(dst, src, bytes);
-        return;
-    }
-    if (!pool) pool = new PlainPool(kParts);
-    const size_t part = (bytes / kParts + 63) & ~size_t(63);
-    std::vector<std::function<void()>> jobs(kParts);
-    for (size_t k = 0; k < kParts; ++k) {
-        const size_t a = std::min(bytes, k * part), b = std::min(bytes, a + part);
-        if (b > a)
-            jobs[k] = [=] { std::memcpy(static_cast<char*>(dst) + a, static_cast<const char*>(src) + a, b - a); };
-    }
-    pool->run(jobs);
-}
 
 struct rtcd_detector {
     rtcd_ctx* ctx = nullptr;
@@ -1326,7 +1318,7 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
     if (host) {
         d->q.ensure(4ull * n * dof);
         d->pin_in.ensure(4ull * n * dof);
-        stage_copy(d->pin_in.p, q, 4ull * n * dof);
+        std::memcpy(d->pin_in.p, q, 4ull * n * dof);
         cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * n * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
@@ -1478,7 +1470,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     if (host) {
         d->q.ensure(4ull * total_wp * dof);
         d->pin_in.ensure(4ull * total_wp * dof);
-        stage_copy(d->pin_in.p, q, 4ull * total_wp * dof);
+        std::memcpy(d->pin_in.p, q, 4ull * total_wp * dof);
         cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
@@ -1648,7 +1640,7 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
                     for (uint32_t i = 0; i < n; ++i) n_seg += pieces_of(d->kind, traj_offsets[i + 1] - traj_offsets[i], f);
                 d->pin_in.ensure(std::max<size_t>(in_bytes, 16));
                 d->hq.ensure(std::max<size_t>(in_bytes, 16));
-                stage_copy(d->pin_in.p, q, in_bytes);
+                std::memcpy(d->pin_in.p, q, in_bytes);
                 gq = d->hq.as<float>();
                 d->hflags.ensure(n);
                 gflags = d->hflags.as<uint8_t>();

@@ -20,6 +20,14 @@ struct Error {
 void set_last_error(const std::string& msg);  // the message rtcd_last_error returns on this thread
 void cuda_check(cudaError_t e, const char* what);
 
+// Re-allocations made by DevBuf::ensure / HostBuf::ensure on the calling
+// thread, and the host milliseconds they took (release + allocation).
+struct GrowCounter {
+    uint64_t grows = 0;
+    double ms = 0;
+};
+GrowCounter& thread_grows();
+
 // Grow-only device allocation.
 struct DevBuf {
     void* p = nullptr;

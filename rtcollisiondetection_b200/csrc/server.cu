@@ -58,8 +58,15 @@ struct Request {
 
 bool is_sweep(int kind) { return kind == RTCD_LINEAR_SWEEP || kind == RTCD_QUAD_SWEEP; }
 
+uint64_t units_of(const std::vector<Request*>& batch) {
+    uint64_t u = 0;
+    for (const Request* r : batch) u += r->units;
+    return u;
+}
+
 struct Slot {
     bool fast = false;
+    uint32_t index = 0;
     std::mutex mu;                                      // held while the slot runs a launch or is prepared
     std::map<rtcd_detector*, rtcd_detector*> clones;    // user detector -> this slot's clone
 };
@@ -78,6 +85,10 @@ struct rtcd_server {
     uint64_t inflight_bytes = 0;
     uint64_t submitted = 0, completed = 0, failed = 0, units_completed = 0, batches = 0, inflight_peak = 0;
     std::vector<double> latencies, queue_ms, run_ms;
+    uint64_t workspace_grows = 0;
+    double grow_ms = 0, run_max_ms = 0, run_max_at_s = 0;
+    uint32_t run_max_kind = 0, run_max_units = 0, run_max_grows = 0, run_max_slot = 0;
+    Clock::time_point stats_since = Clock::now();
     std::vector<std::unique_ptr<Slot>> slots;
     std::vector<std::thread> workers;
 };
@@ -222,16 +233,30 @@ void worker(rtcd_server* S, Slot* slot) {
         std::string msg;
         rtcd_status st;
         const auto started = Clock::now();
+        const rtcd::GrowCounter g0 = rtcd::thread_grows();
         {
             std::lock_guard<std::mutex> sl(slot->mu);
             st = run_launch(S, *slot, r0->det, r0->kind, q, off, (uint32_t) n, r0->flags, flags, seg, counts, msg);
         }
+        const rtcd::GrowCounter& g1 = rtcd::thread_grows();
+        const uint64_t grows = g1.grows - g0.grows;
+        const double grow_ms = g1.ms - g0.ms;
         const bool want_counts = (r0->flags & RTCD_CHECK_COUNTS) != 0;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             size_t p = 0, sp = 0;
             const auto now = Clock::now();
             const double run = std::chrono::duration<double, std::milli>(now - started).count();
+            S->workspace_grows += grows;
+            S->grow_ms += grow_ms;
+            if (run > S->run_max_ms) {
+                S->run_max_ms = run;
+                S->run_max_kind = (uint32_t) r0->kind;
+                S->run_max_units = (uint32_t) units_of(batch);
+                S->run_max_grows = (uint32_t) grows;
+                S->run_max_slot = slot->index;
+                S->run_max_at_s = std::chrono::duration<double>(started - S->stats_since).count();
+            }
             for (Request* r : batch) {
                 r->status = st;
                 r->error = msg;
@@ -304,6 +329,7 @@ rtcd_status rtcd_server_create(rtcd_ctx* ctx, const rtcd_server_config* config, 
         for (uint32_t i = 0; i < c.slots; ++i) {
             S->slots.emplace_back(new Slot());
             S->slots.back()->fast = i < c.fast_slots;
+            S->slots.back()->index = i;
         }
         for (auto& sl : S->slots) S->workers.emplace_back(worker, S.get(), sl.get());
         *out = S.release();
@@ -337,28 +363,41 @@ rtcd_status rtcd_server_prepare(rtcd_server* S, rtcd_detector* det, uint32_t max
         uint32_t nl, ns, dof;
         rtcd::detector_info(det, &c, &kind, &rb, &sc, &dc, &nl, &ns, &dof);
         if (c != S->ctx) rtcd::fail(RTCD_ERR_INVALID_ARGUMENT, "detector belongs to another context");
+        // Synthetic launches (zero poses, zero trajectories) that reach every workspace a launch of up
+        // to `units` units can need.  Discrete: one launch of `units` poses.  Sweeps: `units` waypoints
+        // in three shapes - the shortest trajectories (the most trajectories and pieces), 16-waypoint
+        // ones (many trajectories: the staged light pass), and 128-waypoint ones (the longest the weight
+        // tables are prebuilt for, and few enough trajectories that the unstaged kernels and their
+        // sphere-centre buffers run) - each flags-only and counting, in both sweep semantics (the
+        // reference semantics also build the scene's loop-edge trees).
+        const bool sweep = is_sweep(kind);
+        const std::vector<uint32_t> lens =
+            sweep ? std::vector<uint32_t>{kind == RTCD_QUAD_SWEEP ? 3u : 2u, 16u, 128u} : std::vector<uint32_t>{1u};
+        std::vector<uint32_t> modes = {0u, (uint32_t) RTCD_CHECK_COUNTS};
+        if (sweep) {
+            modes.push_back(RTCD_CHECK_SURFACE);
+            modes.push_back(RTCD_CHECK_SURFACE | RTCD_CHECK_COUNTS);
+        }
         for (auto& sl : S->slots) {
             uint32_t units = max_units ? max_units : S->cfg.max_batch_units;
             if (sl->fast) units = std::min(units, std::max(S->cfg.fast_max_units, 1u) * 2);
-            // a synthetic launch of that size: the zero pose (or 16-waypoint zero trajectories)
-            std::vector<uint32_t> off;
-            uint32_t n = units;
-            if (is_sweep(kind)) {
-                n = std::max(1u, units / 16);
-                off.resize(n + 1);
-                for (uint32_t i = 0; i <= n; ++i) off[i] = 16 * i;
-                units = 16 * n;
-            }
-            std::vector<float> q((size_t) units * dof, 0.0f);
-            std::vector<uint8_t> fl(n), seg;
-            std::vector<uint32_t> cnt(n);
-            if (is_sweep(kind)) seg.resize((size_t) units + 2 * n);
-            std::string msg;
             std::lock_guard<std::mutex> lk(sl->mu);
-            // flags-only and counting launches size different buffers
-            for (uint32_t fl_mode : {0u, (uint32_t) RTCD_CHECK_COUNTS}) {
-                rtcd_status st = run_launch(S, *sl, det, kind, q, off, n, fl_mode, fl, seg, cnt, msg);
-                if (st != RTCD_OK) rtcd::fail(st, msg);
+            for (uint32_t len : lens) {
+                const uint32_t n = std::max(1u, units / len);
+                const uint32_t u = sweep ? len * n : n;
+                std::vector<uint32_t> off;
+                if (sweep) {
+                    off.resize(n + 1);
+                    for (uint32_t i = 0; i <= n; ++i) off[i] = len * i;
+                }
+                std::vector<float> q((size_t) u * dof, 0.0f);
+                std::vector<uint8_t> fl(n), seg(sweep ? (size_t) u + 2 * n : 0);
+                std::vector<uint32_t> cnt(n);
+                std::string msg;
+                for (uint32_t mode : modes) {
+                    rtcd_status st = run_launch(S, *sl, det, kind, q, off, n, mode, fl, seg, cnt, msg);
+                    if (st != RTCD_OK) rtcd::fail(st, msg);
+                }
             }
         }
     });
@@ -484,6 +523,15 @@ rtcd_status rtcd_server_get_stats(rtcd_server* S, rtcd_server_stats* out) {
         out->queue_p50_ms = pct(qms, 0.50);
         out->queue_p99_ms = pct(qms, 0.99);
         out->run_p99_ms = pct(rms, 0.99);
+        std::lock_guard<std::mutex> lk(S->mu);
+        out->workspace_grows = S->workspace_grows;
+        out->grow_ms = S->grow_ms;
+        out->run_max_ms = S->run_max_ms;
+        out->run_max_kind = S->run_max_kind;
+        out->run_max_units = S->run_max_units;
+        out->run_max_grows = S->run_max_grows;
+        out->run_max_slot = S->run_max_slot;
+        out->run_max_at_s = S->run_max_at_s;
     });
 }
 
@@ -496,6 +544,10 @@ rtcd_status rtcd_server_reset_stats(rtcd_server* S) {
         S->latencies.clear();
         S->queue_ms.clear();
         S->run_ms.clear();
+        S->workspace_grows = 0;
+        S->grow_ms = S->run_max_ms = S->run_max_at_s = 0;
+        S->run_max_kind = S->run_max_units = S->run_max_grows = S->run_max_slot = 0;
+        S->stats_since = Clock::now();
     });
 }
 

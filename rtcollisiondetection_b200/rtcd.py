@@ -551,7 +551,9 @@ class ServerStats(C.Structure):
                 ('queue_depth', C.c_uint32), ('reserved0', C.c_uint32), ('p50_ms', C.c_double),
                 ('p99_ms', C.c_double), ('mean_ms', C.c_double), ('max_ms', C.c_double),
                 ('queue_p50_ms', C.c_double), ('queue_p99_ms', C.c_double), ('run_p99_ms', C.c_double),
-                ('reserved', C.c_uint64 * 1)]
+                ('workspace_grows', C.c_uint64), ('grow_ms', C.c_double), ('run_max_ms', C.c_double),
+                ('run_max_kind', C.c_uint32), ('run_max_units', C.c_uint32), ('run_max_grows', C.c_uint32),
+                ('run_max_slot', C.c_uint32), ('run_max_at_s', C.c_double)]
 
 
 class Server:

@@ -121,6 +121,47 @@ def test_server_fast_lane_prepared(world, panda):
             assert np.array_equal(got['seg_flags'], alone['seg_flags']), k
 
 
+def test_prepared_server_serves_without_reallocation(world, panda):
+    """After rtcd_server_prepare, requests of any shape within the prepared
+    size - discrete batches, sweeps of 1 to 60 trajectories of 2/3 to 128
+    waypoints (staged and unstaged light passes), flags-only and counting,
+    solid and reference semantics - run without a workspace re-allocation
+    (each would synchronise the device and stall every slot), and their
+    results equal the requests checked alone."""
+    _, dets = world
+    server = rtcd.Server(dets['lin'].ctx, slots=3, max_batch_units=8192, fast_slots=1, fast_max_units=256)
+    for k in ('r2o_small', 'o2r_small', 'lin', 'quad'):
+        server.prepare(dets[k], 8192)
+    server.reset_stats()
+    rng = np.random.default_rng(21)
+    reqs = []
+    for i in range(48):
+        k = ['r2o_small', 'o2r_small', 'lin', 'quad'][i % 4]
+        counts = bool(rng.integers(0, 2))
+        surface = bool(rng.integers(0, 2))
+        if k in ('lin', 'quad'):
+            nt = int(rng.integers(1, 61))
+            lo = 2 if k == 'lin' else 3
+            wp = np.minimum(scenes.log_uniform_counts(nt, lo, 128, seed=700 + i), 8192 // nt)
+            q, off = scenes.random_walk_trajectories(panda, nt, np.maximum(wp, lo), seed=700 + i)
+        else:
+            q, off, surface = scenes.uniform_poses(panda, int(rng.integers(1, 4097)), seed=900 + i), None, False
+        reqs.append((k, q, off, counts, surface))
+    tickets = [server.submit(dets[k], q, off, counts=c, surface=sf) for k, q, off, c, sf in reqs]
+    outs = [server.wait(t, timeout_ms=120000) for t in tickets]
+    st = server.stats()
+    server.close()
+    assert st['completed'] == len(reqs) and st['failed'] == 0
+    assert st['workspace_grows'] == 0, st
+    for (k, q, off, c, sf), got in zip(reqs, outs):
+        alone = dets[k].check(q, off, segments=dets[k].sweep, counts=c, surface=sf)
+        assert np.array_equal(got['flags'], alone['flags']), k
+        if c:
+            assert np.array_equal(got['counts'], alone['counts']), k
+        if dets[k].sweep:
+            assert np.array_equal(got['seg_flags'], alone['seg_flags']), k
+
+
 def test_server_rejects_bad_config(world):
     _, dets = world
     with pytest.raises(rtcd.RTCDError):
