@@ -159,6 +159,12 @@ typedef struct {
                                         has at least four trajectories per resident block; 1 = sphere centres
                                         and control points always go through global memory (separate FK and
                                         fit kernels) */
+    uint32_t sweep_group;            /* sweeps, staged light pass: trajectories a block stages and works through
+                                        together (one FK and fit phase and one hand-over barrier per group
+                                        instead of per trajectory); 0 = about 1,024 (piece, sphere) units a
+                                        group (short trajectories are grouped, long ones staged one at a
+                                        time), within the block's share of the SM's shared memory and at
+                                        least four groups per resident block (at most 8); 1 = one at a time */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream

@@ -1020,9 +1020,12 @@ struct ObbTest {
 
 // Capped at 5 resident blocks per SM worth of registers (a few spills, more
 // warps to hide the node-load latency; measured on the 65,536-pose workload).
-template <bool R2O, bool PACKET>
+// TOP: the first W.top_nodes wide nodes are staged in shared memory after the
+// frontiers and read from there (a separate instantiation, so the default
+// kernel's node loads carry no branch).
+template <bool R2O, bool PACKET, bool TOP>
 __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
-    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front], then W.top_nodes staged wide nodes
+    extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front], then (TOP) the staged wide nodes
     __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
     __shared__ uint32_t s_hits[kAbWarps];  // a lane of the warp's current stage-B step hit its pose
     const DiscreteArgs& A = W.d;
@@ -1039,10 +1042,12 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
     const uint32_t n_items = *A.n_items;
     const uint32_t budget = W.light_steps ? W.light_steps : 0xFFFFFFFFu;
     // the tree's top levels in shared memory (its first nodes, breadth-first), read by every descent
-    const uint32_t n_top = min(W.top_nodes, R2O ? S.n_tri_wide : S.n_edge_wide);
+    const uint32_t n_top = TOP ? min(W.top_nodes, R2O ? S.n_tri_wide : S.n_edge_wide) : 0u;
     float4* s_top = reinterpret_cast<float4*>(s_front + ((kAbWarps * S.wide_front + 3u) & ~3u));
-    for (uint32_t k = threadIdx.x; k < n_top * 2 * kWide; k += blockDim.x) s_top[k] = __ldg(wn + k);
-    __syncthreads();
+    if (TOP) {
+        for (uint32_t k = threadIdx.x; k < n_top * 2 * kWide; k += blockDim.x) s_top[k] = __ldg(wn + k);
+        __syncthreads();
+    }
     uint32_t st[kStack];
     unsigned long long n_acc = 0, n_skip = 0, n_rej = 0, n_leaf = 0, n_cand = 0, n_node = 0;
     while (true) {
@@ -1253,7 +1258,7 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
                 continue;
             }
             if (sp == 0) break;
-            if (!wide_step(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand, s_top, n_top))
+            if (!wide_step<TOP>(wn, fr, sp, cb, nc, ObbTest{ob, ext}, S.wide_front, A.err, n_node, n_cand, s_top, n_top))
                 break;
         }
         if (overflow && lane == 0) mark_overflow(W, item);
@@ -1571,10 +1576,20 @@ static uint32_t stage_ab_grid(K kernel, size_t smem) {
     return (uint32_t) std::max(1, per_sm) * (uint32_t) device_sm_count();
 }
 
+// Runs f with the k_stage_ab instantiation for (r2o, packets, top).
+template <class F>
+static auto with_stage_ab(bool r2o, bool packets, bool top, F&& f) {
+    if (top) {
+        if (packets) return r2o ? f(k_stage_ab<true, true, true>) : f(k_stage_ab<false, true, true>);
+        return r2o ? f(k_stage_ab<true, false, true>) : f(k_stage_ab<false, false, true>);
+    }
+    if (packets) return r2o ? f(k_stage_ab<true, true, false>) : f(k_stage_ab<false, true, false>);
+    return r2o ? f(k_stage_ab<true, false, false>) : f(k_stage_ab<false, false, false>);
+}
+
 uint32_t stage_ab_blocks(bool r2o, bool packets, const SceneDev& S) {
     const size_t smem = stage_ab_smem(S);
-    if (packets) return r2o ? stage_ab_grid(k_stage_ab<true, true>, smem) : stage_ab_grid(k_stage_ab<false, true>, smem);
-    return r2o ? stage_ab_grid(k_stage_ab<true, false>, smem) : stage_ab_grid(k_stage_ab<false, false>, smem);
+    return with_stage_ab(r2o, packets, false, [&](auto kernel) { return stage_ab_grid(kernel, smem); });
 }
 
 void launch_subtree(bool r2o, const RobotDev& R, const SceneDev& S, const WaveArgs& W, uint32_t share, cudaStream_t s) {
@@ -1597,22 +1612,12 @@ void launch_stage_ab(bool r2o, bool packets, const RobotDev& R, const SceneDev& 
                      cudaStream_t s) {
     const uint32_t top = std::min(W.top_nodes, r2o ? S.n_tri_wide : S.n_edge_wide);
     const size_t smem = stage_ab_smem(S, top);
-    // sets the shared-memory limit before the first launch, and caps the grid at what fits
-    blocks = std::min(blocks, packets ? (r2o ? stage_ab_grid(k_stage_ab<true, true>, smem)
-                                             : stage_ab_grid(k_stage_ab<false, true>, smem))
-                                      : (r2o ? stage_ab_grid(k_stage_ab<true, false>, smem)
-                                             : stage_ab_grid(k_stage_ab<false, false>, smem)));
-    if (packets) {
-        if (r2o)
-            k_stage_ab<true, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
-        else
-            k_stage_ab<false, true><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
-    } else {
-        if (r2o)
-            k_stage_ab<true, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
-        else
-            k_stage_ab<false, false><<<blocks, kAbWarps * 32, smem, s>>>(R, S, W);
-    }
+    with_stage_ab(r2o, packets, top != 0, [&](auto kernel) {
+        // sets the shared-memory limit before the first launch, and caps the grid at what fits
+        const uint32_t b = std::min(blocks, stage_ab_grid(kernel, smem));
+        kernel<<<b, kAbWarps * 32, smem, s>>>(R, S, W);
+        return 0;
+    });
     cuda_check(cudaGetLastError(), "k_stage_ab");
 }
 

@@ -173,13 +173,15 @@ struct SweepArgs {
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // units appended (may exceed heavy_cap: those stayed in the light pass)
     uint32_t* heavy_work;      // heavy-pass work counter
-    // the staged light pass (k_sweep_traj): a block takes one trajectory at a time from work_counter,
-    // runs its FK (and quadratic fit) into shared memory and its units from there
+    // the staged light pass (k_sweep_traj): a block takes `group` consecutive trajectories at a time
+    // from work_counter, runs their FK (and quadratic fit) into shared memory and their units from there
     const float* q;            // [waypoint][dof] joint values
     const float* W;            // quadratic fit tables, W_off[n] = the table of n waypoints
     const uint32_t* W_off;
     uint32_t max_wp, max_nc, max_pieces;  // largest trajectory of the batch (shared-memory sizing)
+    uint32_t group;            // staged: trajectories per claim, 0 = chosen at launch (1..kSweepMaxGroup)
 };
+constexpr uint32_t kSweepMaxGroup = 8;
 
 void launch_fk_spheres(const RobotDev& R, const float* d_q, uint32_t n_wp, float4* d_centers, cudaStream_t s);
 void launch_fit(const float4* d_centers, const uint32_t* d_wp_off, const uint32_t* d_ctrl_off, const float* d_W,

@@ -791,11 +791,17 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
     k_sweep_traj(const SceneDev S, const RobotDev R, const SweepArgs A) {
     extern __shared__ float4 s_dyn[];
     const uint32_t L = R.n_links, ns = R.n_spheres, L12 = L * 12;
-    float* s_T = reinterpret_cast<float*>(s_dyn);                   // [max_wp][L][12]
-    float* s_C = s_T + (size_t) A.max_wp * L12;                     // [max_nc][L][12] (quadratic)
-    volatile uint32_t* s_piece = reinterpret_cast<volatile uint32_t*>(s_C + (QUAD ? (size_t) A.max_nc * L12 : 0));
-    __shared__ uint32_t s_tr, s_next;
-    __shared__ volatile uint32_t s_hit;
+    // one slot per trajectory of a group: T [max_wp][L][12] | C [max_nc][L][12] (quadratic) | piece
+    // flags [max_pieces], each slot rounded to 16 bytes (the host sizes the same)
+    const uint32_t c_at = A.max_wp * L12, f_at = c_at + (QUAD ? A.max_nc * L12 : 0u);
+    const uint32_t slot_words = (f_at + A.max_pieces + 3u) & ~3u;
+    float* s_slots = reinterpret_cast<float*>(s_dyn);
+    __shared__ uint32_t s_tr0, s_ng, s_next;
+    __shared__ uint32_t s_wp0[kSweepMaxGroup], s_nwp[kSweepMaxGroup], s_p0[kSweepMaxGroup];
+    // prefixes over the group's valid trajectories: waypoints, units, fit outputs, pieces
+    __shared__ uint32_t s_wb[kSweepMaxGroup + 1], s_ub[kSweepMaxGroup + 1], s_cb[kSweepMaxGroup + 1],
+        s_pb[kSweepMaxGroup + 1];
+    __shared__ volatile uint32_t s_hit[kSweepMaxGroup];
     const float4* __restrict__ en = WIDE ? S.edge_wide : S.edge_nodes;
     const float4* __restrict__ ep = S.edge_prims;
     const uint32_t root = WIDE ? S.edge_wide_root : S.edge_root;
@@ -803,43 +809,77 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
     unsigned long long n_acc = 0, n_skip = 0, n_leaf = 0, n_roots = 0, n_node = 0;
     const uint32_t budget = A.light_steps ? A.light_steps : 0xFFFFFFFFu;
     const int dof = R.chain.dof;
+    const uint32_t group = max(1u, min(A.group, kSweepMaxGroup));
+    // the group member g whose prefix range [b[g], b[g + 1]) holds i (i < b[ng])
+    auto member = [](const uint32_t* b, uint32_t i) {
+        uint32_t g = 0;
+        while (i >= b[g + 1]) ++g;
+        return g;
+    };
 
     while (true) {
-        __syncthreads();  // the previous trajectory's shared state is no longer read
+        __syncthreads();  // the previous group's shared state is no longer read
         if (threadIdx.x == 0) {
-            s_tr = atomicAdd(A.work_counter, 1u);
+            const uint32_t t0 = atomicAdd(A.work_counter, group);
+            const uint32_t ng = t0 < A.n_traj ? min(group, A.n_traj - t0) : 0u;
+            uint32_t wb = 0, ub = 0, cb = 0, pb = 0;
+            for (uint32_t g = 0; g < ng; ++g) {
+                const uint32_t tr = t0 + g;
+                const uint32_t w0 = A.traj_wp_off[tr], nwp = A.traj_wp_off[tr + 1] - w0;
+                const uint32_t p0 = A.traj_piece_off[tr], np = A.traj_piece_off[tr + 1] - p0;
+                const uint32_t nc = QUAD ? A.traj_ctrl_off[tr + 1] - A.traj_ctrl_off[tr] : 0u;
+                const bool fits = nwp <= A.max_wp && np <= A.max_pieces && (!QUAD || nc <= A.max_nc);
+                if (!fits) atomicOr(A.err, kErrRange);  // sized by the host: cannot happen
+                s_wp0[g] = w0;
+                s_nwp[g] = nwp;
+                s_p0[g] = p0;
+                s_wb[g] = wb;
+                s_ub[g] = ub;
+                s_cb[g] = cb;
+                s_pb[g] = pb;
+                s_hit[g] = 0;
+                if (fits) {
+                    wb += nwp;
+                    ub += np * ns;
+                    cb += nc * L12;
+                    pb += np;
+                }
+            }
+            s_wb[ng] = wb;
+            s_ub[ng] = ub;
+            s_cb[ng] = cb;
+            s_pb[ng] = pb;
+            s_tr0 = t0;
+            s_ng = ng;
             s_next = 0;
-            s_hit = 0;
         }
         __syncthreads();
-        const uint32_t tr = s_tr;
-        if (tr >= A.n_traj) break;
-        const uint32_t w0 = A.traj_wp_off[tr], nwp = A.traj_wp_off[tr + 1] - w0;
-        const uint32_t p0 = A.traj_piece_off[tr], np = A.traj_piece_off[tr + 1] - p0;
-        const uint32_t nc = QUAD ? A.traj_ctrl_off[tr + 1] - A.traj_ctrl_off[tr] : 0;
-        if (nwp > A.max_wp || np > A.max_pieces || (QUAD && nc + 0u * nwp > A.max_nc)) {  // sized by the host
-            if (threadIdx.x == 0) atomicOr(A.err, kErrRange);
-            continue;
-        }
-        for (uint32_t w = threadIdx.x; w < nwp; w += BLOCK) {
+        const uint32_t ng = s_ng;
+        if (ng == 0) break;
+        for (uint32_t i = threadIdx.x; i < s_wb[ng]; i += BLOCK) {
+            const uint32_t g = member(s_wb, i), w = i - s_wb[g];
             float qq[kMaxDof];
-            for (int k = 0; k < dof; ++k) qq[k] = __ldg(A.q + (size_t) (w0 + w) * dof + k);
-            fk_chain(R.chain, qq, reinterpret_cast<float(*)[12]>(s_T + (size_t) w * L12));
+            for (int k = 0; k < dof; ++k) qq[k] = __ldg(A.q + (size_t) (s_wp0[g] + w) * dof + k);
+            fk_chain(R.chain, qq, reinterpret_cast<float(*)[12]>(s_slots + (size_t) g * slot_words + (size_t) w * L12));
         }
-        for (uint32_t k = threadIdx.x; k < np; k += BLOCK) s_piece[k] = 0;
+        for (uint32_t i = threadIdx.x; i < s_pb[ng]; i += BLOCK) {
+            const uint32_t g = member(s_pb, i);
+            reinterpret_cast<uint32_t*>(s_slots + (size_t) g * slot_words + f_at)[i - s_pb[g]] = 0;
+        }
         __syncthreads();
         if (QUAD) {
-            const float* Wn = A.W + A.W_off[nwp];
-            for (uint32_t idx = threadIdx.x; idx < nc * L12; idx += BLOCK) {
-                const uint32_t k = idx / L12, le = idx - k * L12;
-                const float* wr = Wn + (size_t) k * nwp;
+            for (uint32_t i = threadIdx.x; i < s_cb[ng]; i += BLOCK) {
+                const uint32_t g = member(s_cb, i), idx = i - s_cb[g];
+                const uint32_t nwp = s_nwp[g], k = idx / L12, le = idx - k * L12;
+                const float* wr = A.W + A.W_off[nwp] + (size_t) k * nwp;
+                const float* sT = s_slots + (size_t) g * slot_words;
                 float acc = 0.f;
-                for (uint32_t t = 0; t < nwp; ++t) acc = fmaf(__ldg(wr + t), s_T[(size_t) t * L12 + le], acc);
-                s_C[idx] = acc;
+                for (uint32_t t = 0; t < nwp; ++t) acc = fmaf(__ldg(wr + t), sT[(size_t) t * L12 + le], acc);
+                s_slots[(size_t) g * slot_words + c_at + idx] = acc;
             }
             __syncthreads();
         }
-        const uint32_t units = np * ns;
+        const uint32_t units = s_ub[ng];
         // world centre of sphere s under a staged 3x4 transform M
         auto at = [](const float* M, float4 p) {
             return make_float4(M[0] * p.x + M[1] * p.y + M[2] * p.z + M[3], M[4] * p.x + M[5] * p.y + M[6] * p.z + M[7],
@@ -847,41 +887,50 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
         };
         int sp = 0;
         bool busy = false;
-        uint32_t steps = 0, u_hits = 0, piece = 0;
+        uint32_t steps = 0, u_hits = 0, piece = 0, g = 0;
         SweepUnit U;
         SweepCull c;
-        U.traj = tr;
-        U.piece_g = p0;
+        U.traj = s_tr0;
+        U.piece_g = 0;
         while (true) {
             while (!busy) {
                 const uint32_t u = atomicAdd(&s_next, 1u);
                 if (u >= units) break;
-                piece = u / ns;
-                const uint32_t s = u - piece * ns;
-                if (!A.want_counts && (A.want_pieces ? s_piece[piece] : s_hit)) {
+                g = member(s_ub, u);
+                const uint32_t local = u - s_ub[g];
+                piece = local / ns;
+                const uint32_t s = local - piece * ns;
+                const volatile uint32_t* pf = reinterpret_cast<const volatile uint32_t*>(s_slots + (size_t) g * slot_words + f_at);
+                if (!A.want_counts && (A.want_pieces ? pf[piece] : s_hit[g])) {
                     ++n_skip;
                     continue;
                 }
+                const float* sT = s_slots + (size_t) g * slot_words;
                 const float4 sp4 = __ldg(R.spheres + s);
                 const uint32_t link = __ldg(R.sphere_link + s);
-                U.piece_g = p0 + piece;
+                U.traj = s_tr0 + g;
+                U.piece_g = s_p0[g] + piece;
                 U.r = sp4.w;
                 if constexpr (!QUAD) {
-                    U.P0 = at(s_T + (size_t) (piece * L + link) * 12, sp4);
-                    U.P1 = at(s_T + (size_t) ((piece + 1) * L + link) * 12, sp4);
+                    U.P0 = at(sT + (size_t) (piece * L + link) * 12, sp4);
+                    U.P1 = at(sT + (size_t) ((piece + 1) * L + link) * 12, sp4);
                     U.P2 = U.P1;
-                } else if (piece + 2 < nc) {
-                    const float4 a = at(s_C + (size_t) (piece * L + link) * 12, sp4);
-                    const float4 b = at(s_C + (size_t) ((piece + 1) * L + link) * 12, sp4);
-                    const float4 cc = at(s_C + (size_t) ((piece + 2) * L + link) * 12, sp4);
-                    U.P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), sp4.w);
-                    U.P1 = b;
-                    U.P2 = make_float4(0.5f * (b.x + cc.x), 0.5f * (b.y + cc.y), 0.5f * (b.z + cc.z), sp4.w);
-                } else {  // the start / end sphere
-                    const uint32_t w = (piece + 2 == nc) ? 0 : nwp - 1;
-                    U.P0 = at(s_T + (size_t) (w * L + link) * 12, sp4);
-                    U.P1 = U.P0;
-                    U.P2 = U.P0;
+                } else {
+                    const uint32_t nc = (s_cb[g + 1] - s_cb[g]) / L12;
+                    if (piece + 2 < nc) {
+                        const float* sC = sT + c_at;
+                        const float4 a = at(sC + (size_t) (piece * L + link) * 12, sp4);
+                        const float4 b = at(sC + (size_t) ((piece + 1) * L + link) * 12, sp4);
+                        const float4 cc = at(sC + (size_t) ((piece + 2) * L + link) * 12, sp4);
+                        U.P0 = make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), sp4.w);
+                        U.P1 = b;
+                        U.P2 = make_float4(0.5f * (b.x + cc.x), 0.5f * (b.y + cc.y), 0.5f * (b.z + cc.z), sp4.w);
+                    } else {  // the start / end sphere
+                        const uint32_t w = (piece + 2 == nc) ? 0 : s_nwp[g] - 1;
+                        U.P0 = at(sT + (size_t) (w * L + link) * 12, sp4);
+                        U.P1 = U.P0;
+                        U.P2 = U.P0;
+                    }
                 }
                 if (root == kNone) continue;
                 make_cull<QUAD>(U, c);
@@ -893,24 +942,25 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
                 ++n_acc;
             }
             if (!busy) break;
+            volatile uint32_t* pf = reinterpret_cast<volatile uint32_t*>(s_slots + (size_t) g * slot_words + f_at);
             // flags only: drop the unit once its piece (or trajectory) is decided
-            if (!A.want_counts && (A.want_pieces ? s_piece[piece] : s_hit)) sp = 0;
+            if (!A.want_counts && (A.want_pieces ? pf[piece] : s_hit[g])) sp = 0;
             const uint32_t leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err);
             if (leaf != kNone) {
                 ++n_leaf;
                 if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots)
                          : leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
                     if (A.want_pieces) {
-                        s_piece[piece] = 1u;
+                        pf[piece] = 1u;
                         atomicExch(A.piece_hit + U.piece_g, 1u);
                     }
                     if (A.want_counts) {
-                        A.traj_hit[tr] = 1u;
+                        A.traj_hit[U.traj] = 1u;
                         ++u_hits;
                     } else {
-                        if (!s_hit) {
-                            s_hit = 1u;
-                            atomicExch(A.traj_hit + tr, 1u);
+                        if (!s_hit[g]) {
+                            s_hit[g] = 1u;
+                            atomicExch(A.traj_hit + U.traj, 1u);
                         }
                         sp = 0;  // this unit is decided
                     }
@@ -927,7 +977,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
             }
             if (sp == 0) {
                 busy = false;
-                if (u_hits) atomicAdd(A.counts + tr, u_hits);
+                if (u_hits) atomicAdd(A.counts + U.traj, u_hits);
             }
         }
     }
@@ -1115,10 +1165,14 @@ static uint32_t heavy_blocks() {
     return blocks;
 }
 
-// The staged light pass at `threads` per block with `smem` bytes of shared
-// memory per block, on at most as many blocks as fit.
+// The staged light pass at BLOCK threads per block, `slot` bytes of shared
+// memory per trajectory, on at most as many blocks as fit.  Trajectories per
+// group (A.group, 0 = chosen here): about 1,024 (piece, sphere) units a
+// group, within the slots that fit in the block's share of the SM at the
+// occupancy one slot allows (and in kSweepStagedMaxSmem), leaving at least
+// four groups per block, at most kSweepMaxGroup.
 template <bool QUAD, int BLOCK, bool WIDE, bool SURF>
-static void launch_staged(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, size_t smem,
+static void launch_staged(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, size_t slot,
                           cudaStream_t s) {
     auto kern = k_sweep_traj<QUAD, BLOCK, WIDE, SURF>;
     static bool attr = false;
@@ -1127,11 +1181,43 @@ static void launch_staged(const SceneDev& S, const RobotDev& R, const SweepArgs&
                    "cudaFuncSetAttribute");
         attr = true;
     }
+    const uint32_t sms = device_sm_count();
     int per_sm = 0;
-    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, smem), "occupancy");
-    blocks = std::min<uint32_t>(blocks, (uint32_t) std::max(1, per_sm) * device_sm_count());
-    blocks = std::min<uint32_t>(blocks, std::max<uint32_t>(A.n_traj, 1));
-    kern<<<blocks, BLOCK, smem, s>>>(S, R, A);
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, slot), "occupancy");
+    blocks = std::min<uint32_t>(blocks, (uint32_t) std::max(1, per_sm) * sms);
+    SweepArgs G = A;
+    if (!G.group) {
+        int dev = 0, sm_bytes = 0, reserved = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        const long per_sm_used = (long) std::max<uint32_t>(1, (blocks + sms - 1) / sms);
+        // the block's share of the SM's shared memory, less the per-block reserve and static arrays
+        const long avail = (long) sm_bytes / per_sm_used - (long) reserved - 2048;
+        const size_t share = std::min<size_t>(kSweepStagedMaxSmem, (size_t) std::max<long>(avail, (long) slot));
+        const uint32_t by_smem = (uint32_t) std::max<size_t>(1, share / slot);
+        const uint32_t by_work = std::max<uint32_t>(1, A.n_traj / (4 * std::max(1u, blocks)));
+        // about 1,024 units a group: grouping pays for short trajectories (their FK and fit
+        // phases and hand-over barriers are a large share), while a group of long ones only
+        // lengthens the last group's tail (measured: linear 32-waypoint trajectories of 1,984
+        // units are 5 % slower in pairs, quadratic 8-16-waypoint ones 8 % faster in threes)
+        const uint64_t tu = std::max<uint64_t>(A.total_units, 1);
+        const uint32_t by_units = (uint32_t) std::max<uint64_t>(1, (1024ull * A.n_traj + tu / 2) / tu);
+        G.group = std::min(kSweepMaxGroup, std::min(by_smem, std::min(by_work, by_units)));
+    }
+    G.group = std::max(1u, std::min(G.group, kSweepMaxGroup));
+    while (G.group > 1 && G.group * slot > kSweepStagedMaxSmem) --G.group;
+    // the group's shared memory must not lower the occupancy one slot allows
+    while (G.group > 1) {
+        int per_sm_g = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g, kern, BLOCK, G.group * slot), "occupancy");
+        if ((uint32_t) std::max(1, per_sm_g) * sms >= blocks) break;
+        --G.group;
+    }
+    const size_t smem = G.group * slot;
+    const uint32_t groups = (A.n_traj + G.group - 1) / G.group;
+    blocks = std::min<uint32_t>(blocks, std::max<uint32_t>(groups, 1));
+    kern<<<blocks, BLOCK, smem, s>>>(S, R, G);
 }
 
 template <bool QUAD, bool SURF>

@@ -49,10 +49,11 @@ __device__ __forceinline__ bool wide_round(const float4& a, const float4& b, uin
 // the lanes (4 lanes per node when at most 8 are waiting, 2 when at most 16,
 // else one lane tests all four children of its node, so a step costs about
 // one box test per lane); at most 32 * kWide leaves are appended per step.
-// top / n_top: a shared-memory copy of the tree's first n_top nodes (they are
-// numbered breadth-first, so these are its top levels); records of those
-// nodes are read from it instead of global memory.
-template <class Test>
+// TOP: top / n_top are a shared-memory copy of the tree's first n_top nodes
+// (they are numbered breadth-first, so these are its top levels), and records
+// of those nodes are read from it instead of global memory; without TOP the
+// loads are plain global loads with no branch between them.
+template <bool TOP = false, class Test>
 __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_t* fr, int& sp, uint32_t* cb, int& nc,
                                           const Test& test, uint32_t front_cap, uint32_t* err,
                                           unsigned long long& n_node, unsigned long long& n_cand,
@@ -78,7 +79,7 @@ __device__ __forceinline__ bool wide_step(const float4* __restrict__ wn, uint32_
             rb[r] = make_float4(0.f, 0.f, __uint_as_float(kNone), 0.f);
             if (r0 + r < rounds && node != kNone) {
                 const size_t at = 2ull * (kWide * (size_t) node + c0 + (r0 + r) * g);
-                if (node < n_top) {
+                if (TOP && node < n_top) {
                     ra[r] = top[at];
                     rb[r] = top[at + 1];
                 } else {

@@ -199,3 +199,33 @@ def test_staged_and_unstaged_light_pass_agree(sweep_setup, panda, kind):
             # centres): they may differ only on segments the oracle puts in the band
             diff = x['seg_flags'] != y['seg_flags']
             assert not (diff & (ref['seg_band'] == 0)).any()
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_grouped_staging_matches_one_at_a_time(sweep_setup, panda, kind):
+    """The staged light pass working through groups of trajectories (2, 3 or
+    8 staged together, the batch not a multiple of the group) gives exactly
+    the flags, segment flags and counts of one trajectory at a time: each
+    trajectory's FK and fit run the same arithmetic in its own slot."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(1201, 3, 64, seed=12)
+    q, off = scenes.random_walk_trajectories(panda, 1201, n_wp, seed=12)
+    one = rtcd.Detector(robot.ctx, kind, robot, scene, traverse_blocks_per_sm=1, sweep_group=1)
+    for surface in (False, True):
+        x = one.check(q, off, segments=True, counts=True, surface=surface)
+        assert one.stats()['path_flags'] & 1 == 1
+        xf = one.check(q, off, segments=True, surface=surface)
+        for group in (2, 3, 8):
+            det = rtcd.Detector(robot.ctx, kind, robot, scene, traverse_blocks_per_sm=1, sweep_group=group)
+            y = det.check(q, off, segments=True, counts=True, surface=surface)
+            assert det.stats()['path_flags'] & 1 == 1
+            for k in ('flags', 'seg_flags', 'counts'):
+                assert np.array_equal(x[k], y[k]), (group, k)
+            yf = det.check(q, off, segments=True, surface=surface)
+            for k in ('flags', 'seg_flags'):
+                assert np.array_equal(xf[k], yf[k]), (group, k)
+            det.close()
+    ref = O.sweep(kind == 'Quadratic', orob, osc, q[:off[64]], off[:65])
+    got = one.check(q[:off[64]], off[:65], segments=True, counts=True)
+    _cmp(got, ref)
+    one.close()
