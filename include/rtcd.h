@@ -165,6 +165,11 @@ typedef struct {
                                         group (short trajectories are grouped, long ones staged one at a
                                         time), within the block's share of the SM's shared memory and at
                                         least four groups per resident block (at most 8); 1 = one at a time */
+    uint32_t sweep_heavy_steps;      /* sweeps: frontier steps (each expands up to 32 edge-tree nodes) a heavy-pass
+                                        unit runs before the nodes still open on its frontier (once there are
+                                        four or more) go, one per warp, to a split pass, so a few units with
+                                        very large traversals do not hold the pass while the rest of the GPU
+                                        idles; 0 = 32, 0xFFFFFFFF = never */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream
@@ -323,6 +328,8 @@ typedef struct {
     uint64_t cull_sphere_tests;  /* discrete: bounding-sphere tests of the OBB cull */
     uint64_t cull_sat_tests;     /* discrete: 15-axis SATs the cull evaluated (after the sphere reject, up to each
                                     item's first overlap) */
+    uint64_t deferred;           /* work the light pass handed to the heavy pass: sweep (piece, sphere) units,
+                                    discrete (item, primitive) candidates */
 } rtcd_stats;
 RTCD_API rtcd_status rtcd_last_stats(rtcd_detector* det, rtcd_stats* out);
 

@@ -522,7 +522,7 @@ struct rtcd_detector {
     uint32_t threads = 128;  // traversal launch shape (stage B / sweep kernel)
     ScanScratch scan;
     // sweep workspace
-    DevBuf centers, ctrl, aux, piece_hit, W, W_off, heavy;
+    DevBuf centers, ctrl, aux, piece_hit, W, W_off, heavy, split;
     DevBuf edge_q, edge_pose_flags;  // edge checks: interpolated configurations, per-configuration flags
     std::vector<uint32_t> edge_off;
     std::vector<float> W_host;
@@ -949,7 +949,7 @@ rtcd_status rtcd_detector_create(rtcd_ctx* ctx, rtcd_detector_kind kind, rtcd_ro
         apply_launch_shape(d.get());
         d->err.ensure(4);
         d->stats.ensure(8 * kStatWords);
-        d->work.ensure(16);  // [0] work counter, [1] heavy units appended, [2] heavy-pass counter
+        d->work.ensure(32);  // [0] work counter, [1] heavy units appended, [2] heavy-pass counter, [3..4] split pass
         d->count.ensure(4);
         cuda_check(cudaMemset(d->err.p, 0, 4), "memset");
         cuda_check(cudaMemset(d->stats.p, 0, 8 * kStatWords), "memset");
@@ -1515,7 +1515,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         d_counts = d->counts.as<uint32_t>();
         cuda_check(cudaMemsetAsync(d_counts, 0, 4ull * n, s), "memset");
     }
-    cuda_check(cudaMemsetAsync(d->work.p, 0, 12, s), "memset");
+    cuda_check(cudaMemsetAsync(d->work.p, 0, 20, s), "memset");  // [0..4]: the sweep passes' counters
     SweepArgs A{};
     A.centers = staged ? nullptr : d->centers.as<float4>();
     A.ctrl = quad && !staged ? d->ctrl.as<float4>() : nullptr;
@@ -1555,6 +1555,15 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
         A.heavy_cap = cap;
         A.heavy_count = d->work.as<uint32_t>() + 1;
         A.heavy_work = d->work.as<uint32_t>() + 2;
+        // the split pass: room for one frontier entry per unit the light pass could defer
+        A.heavy_steps = d->cfg.sweep_heavy_steps == 0xFFFFFFFFu ? 0u
+                        : d->cfg.sweep_heavy_steps                ? d->cfg.sweep_heavy_steps
+                                                                      : 32u;
+        d->split.ensure(sizeof(uint2) * cap);
+        A.split = d->split.as<uint2>();
+        A.split_cap = cap;
+        A.split_count = d->work.as<uint32_t>() + 3;
+        A.split_work = d->work.as<uint32_t>() + 4;
     }
     d->last_items = A.total_units;
     if (timed) {
@@ -1777,10 +1786,16 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
         cudaStream_t s = d->last_stream ? d->last_stream : d->stream;
         cuda_check(cudaMemcpyAsync(sb, d->stats.p, sizeof(sb), cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaMemcpyAsync(&cnt, d->count.p, 4, cudaMemcpyDeviceToHost, s), "stats");
-        uint32_t cand = 0;
+        const bool discrete = d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS;
+        uint32_t cand = 0, wave[4] = {0, 0, 0, 0}, work[2] = {0, 0};
         if (d->wave_counts.p)
-            cuda_check(cudaMemcpyAsync(&cand, d->wave_counts.p, 4, cudaMemcpyDeviceToHost, s), "stats");
+            cuda_check(cudaMemcpyAsync(wave, d->wave_counts.p, sizeof(wave), cudaMemcpyDeviceToHost, s), "stats");
+        if (!discrete && d->work.p)
+            cuda_check(cudaMemcpyAsync(work, d->work.p, sizeof(work), cudaMemcpyDeviceToHost, s), "stats");
         cuda_check(cudaStreamSynchronize(s), "stats sync");
+        cand = wave[0];
+        // the heavy list's append counter: [3] of the discrete wave counters, [1] of the sweep work words
+        out->deferred = discrete ? wave[3] : work[1];
         for (int k = 0; k < kStatBank; ++k) st[k] = sb[k] + sb[kStatBank + k];
         out->path_flags = d->last_path_flags;
         out->first_node_tests = sb[7];
@@ -1789,7 +1804,7 @@ rtcd_status rtcd_last_stats(rtcd_detector* d, rtcd_stats* out) {
         out->cull_sat_tests = sb[kStatCullSats];
         out->fp64_retests = st[0];
         // discrete: the candidate buffer's count, or the fused form's in-warp count
-        out->candidates = (d->kind == RTCD_OBS_TO_ROBOT || d->kind == RTCD_ROBOT_TO_OBS) ? (st[6] ? st[6] : cand) : st[5];
+        out->candidates = discrete ? (st[6] ? st[6] : cand) : st[5];
         out->exact_tests = st[4];
         out->skipped = st[2];
         out->node_tests = st[7];

@@ -1044,7 +1044,7 @@ __global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R,
     // the tree's top levels in shared memory (its first nodes, breadth-first), read by every descent
     const uint32_t n_top = TOP ? min(W.top_nodes, R2O ? S.n_tri_wide : S.n_edge_wide) : 0u;
     float4* s_top = reinterpret_cast<float4*>(s_front + ((kAbWarps * S.wide_front + 3u) & ~3u));
-    if (TOP) {
+    if constexpr (TOP) {
         for (uint32_t k = threadIdx.x; k < n_top * 2 * kWide; k += blockDim.x) s_top[k] = __ldg(wn + k);
         __syncthreads();
     }

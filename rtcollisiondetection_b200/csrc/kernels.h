@@ -173,6 +173,12 @@ struct SweepArgs {
     uint32_t heavy_cap;
     uint32_t* heavy_count;     // units appended (may exceed heavy_cap: those stayed in the light pass)
     uint32_t* heavy_work;      // heavy-pass work counter
+    uint32_t heavy_steps;      // frontier steps a heavy unit takes before its open frontier goes to the split
+                               // pass (0: never)
+    uint2* split;              // [split_cap] (heavy record, edge-tree node) pairs for the split pass
+    uint32_t split_cap;
+    uint32_t* split_count;     // pairs appended (past split_cap: the unit was finished by its warp)
+    uint32_t* split_work;      // split-pass work counter
     // the staged light pass (k_sweep_traj): a block takes `group` consecutive trajectories at a time
     // from work_counter, runs their FK (and quadratic fit) into shared memory and their units from there
     const float* q;            // [waypoint][dof] joint values

@@ -996,7 +996,17 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
 constexpr int kHeavyWarps = 4;
 constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
 
-template <bool QUAD, bool SURF>
+// SPLIT = false: the heavy pass over the light pass's deferred units, each
+// from the root.  A unit still open after A.heavy_steps frontier steps, once
+// its frontier holds kSplitMinFront nodes or more, finishes its pending
+// leaves, appends its open frontier nodes to A.split and stops (A.heavy_steps
+// == 0: never), so the few units with very large traversals do not hold the
+// pass while the other warps idle.  SPLIT = true: the split pass, one warp
+// per (unit, node) pair of A.split, each descending that node's subtree to
+// the end.  Every node is expanded exactly once either way, so flags and
+// counts do not depend on where a unit split.
+constexpr int kSplitMinFront = 4;
+template <bool QUAD, bool SURF, bool SPLIT>
 __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev S, const SweepArgs A) {
     __shared__ uint32_t s_front[kHeavyWarps][kFrontier];
     __shared__ uint32_t s_leaf[kHeavyWarps][kLeafBuf];
@@ -1004,23 +1014,30 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
     uint32_t* fr = s_front[threadIdx.x >> 5];
     uint32_t* lf = s_leaf[threadIdx.x >> 5];
     const uint32_t lt = (1u << lane) - 1u;
-    const uint32_t n_heavy = min(*A.heavy_count, A.heavy_cap);
+    const uint32_t n_work = SPLIT ? min(*A.split_count, A.split_cap) : min(*A.heavy_count, A.heavy_cap);
     unsigned long long n_leaf = 0, n_roots = 0, n_node = 0;
     while (true) {
         uint32_t h = 0;
-        if (lane == 0) h = atomicAdd(A.heavy_work, 1u);
+        if (lane == 0) h = atomicAdd(SPLIT ? A.split_work : A.heavy_work, 1u);
         h = __shfl_sync(0xffffffffu, h, 0);
-        if (h >= n_heavy) break;
+        if (h >= n_work) break;
+        uint32_t rec = h, start = S.edge_root;
+        if (SPLIT) {
+            const uint2 item = A.split[h];
+            rec = item.x;
+            start = item.y;
+        }
         SweepUnit U;
-        load_rec(A.heavy + h, U);
+        load_rec(A.heavy + rec, U);
         SweepCull c;
         make_cull<QUAD>(U, c);
-        if (lane == 0) fr[0] = S.edge_root;
+        if (lane == 0) fr[0] = start;
         __syncwarp();
         int sp = 1, nl = 0, step = 0;
-        uint32_t hits = 0;
+        uint32_t hits = 0, warp_steps = 0;
+        bool budgeted = !SPLIT && A.heavy_steps != 0, handing = false;
         while (true) {
-            if (nl >= 32 || (sp == 0 && nl > 0)) {  // leaf step
+            if (nl >= 32 || (sp == 0 && nl > 0) || (handing && nl > 0)) {  // leaf step
                 const int take = min(nl, 32);
                 nl -= take;
                 const uint32_t leaf = lane < take ? lf[nl + lane] : kNone;
@@ -1047,6 +1064,21 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
                 continue;
             }
             if (sp == 0) break;
+            if (handing) {  // no leaves pending: the open frontier goes to the split pass
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(A.split_count, (uint32_t) sp);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if ((uint64_t) base + (uint64_t) sp <= A.split_cap) {
+                    for (int k = lane; k < sp; k += 32) A.split[base + k] = make_uint2(rec, fr[k]);
+                    break;
+                }
+                handing = false;  // no room: this warp finishes the unit
+                budgeted = false;
+            }
+            if (budgeted && ++warp_steps >= A.heavy_steps && sp >= kSplitMinFront) {
+                handing = true;
+                continue;
+            }
             if (!A.want_counts && (++step & 7) == 0) {  // decided meanwhile by another unit?
                 uint32_t dec = 0;
                 if (lane == 0) dec = A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj);
@@ -1159,7 +1191,7 @@ static uint32_t heavy_blocks() {
     static uint32_t blocks = 0;
     if (!blocks) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD, SURF>, kHeavyWarps * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD, SURF, false>, kHeavyWarps * 32, 0);
         blocks = (uint32_t) std::max(1, per_sm) * device_sm_count();
     }
     return blocks;
@@ -1259,8 +1291,12 @@ static void sweep_dispatch(const SceneDev& S, const RobotDev& R, const SweepArgs
         SweepArgs H = A;
         H.stats = A.stats + kStatBank;
         const uint32_t hb = std::max(1u, heavy_blocks<QUAD, SURF>() * heavy_share / 100);
-        k_sweep_heavy<QUAD, SURF><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
+        k_sweep_heavy<QUAD, SURF, false><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
         cuda_check(cudaGetLastError(), "k_sweep_heavy");
+        if (A.heavy_steps) {
+            k_sweep_heavy<QUAD, SURF, true><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
+            cuda_check(cudaGetLastError(), "k_sweep_heavy (split)");
+        }
     }
 }
 

@@ -67,7 +67,7 @@ class Config(C.Structure):
                 ('stream_priority', C.c_int32), ('residency_percent', C.c_uint32), ('light_steps', C.c_uint32),
                 ('stage_b_form', C.c_uint32), ('stage_b_chunk', C.c_uint32), ('plain_streams', C.c_uint32),
                 ('top_nodes_shared', C.c_uint32), ('sweep_unstaged', C.c_uint32),
-                ('sweep_group', C.c_uint32)]
+                ('sweep_group', C.c_uint32), ('sweep_heavy_steps', C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -76,7 +76,7 @@ class Stats(C.Structure):
                 ('ms_total', C.c_float), ('candidates', C.c_uint64), ('exact_tests', C.c_uint64),
                 ('skipped', C.c_uint64), ('node_tests', C.c_uint64), ('ms_first_pass', C.c_float),
                 ('path_flags', C.c_uint32), ('first_node_tests', C.c_uint64), ('first_exact_tests', C.c_uint64),
-                ('cull_sphere_tests', C.c_uint64), ('cull_sat_tests', C.c_uint64)]
+                ('cull_sphere_tests', C.c_uint64), ('cull_sat_tests', C.c_uint64), ('deferred', C.c_uint64)]
 
 
 _lib = None
@@ -384,7 +384,8 @@ class Detector:
 
     def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
                  stream_priority=0, residency_percent=0, light_steps=0, stage_b_form=0, stage_b_chunk=0,
-                 plain_streams=0, top_nodes_shared=0, sweep_unstaged=0, sweep_group=0):
+                 plain_streams=0, top_nodes_shared=0, sweep_unstaged=0, sweep_group=0,
+                 sweep_heavy_steps=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -401,6 +402,7 @@ class Detector:
         cfg.top_nodes_shared = top_nodes_shared
         cfg.sweep_unstaged = sweep_unstaged
         cfg.sweep_group = sweep_group
+        cfg.sweep_heavy_steps = sweep_heavy_steps
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 

@@ -229,3 +229,33 @@ def test_grouped_staging_matches_one_at_a_time(sweep_setup, panda, kind):
     got = one.check(q[:off[64]], off[:65], segments=True, counts=True)
     _cmp(got, ref)
     one.close()
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_heavy_split_pass_keeps_results(sweep_setup, panda, kind):
+    """Heavy-pass units that hand their open frontier to the split pass after
+    1, 4 or the default 32 frontier steps, or never: the same flags, segment
+    flags and counts (every node is expanded exactly once), in both
+    semantics."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(600, 3, 64, seed=13)
+    q, off = scenes.random_walk_trajectories(panda, 600, n_wp, seed=13)
+    never = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=4, sweep_heavy_steps=0xFFFFFFFF)
+    for surface in (False, True):
+        x = never.check(q, off, segments=True, counts=True, surface=surface)
+        assert never.stats()['deferred'] > 0
+        xf = never.check(q, off, segments=True, surface=surface)
+        for steps in (1, 4, 0):
+            det = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=4, sweep_heavy_steps=steps)
+            y = det.check(q, off, segments=True, counts=True, surface=surface)
+            for k in ('flags', 'seg_flags', 'counts'):
+                assert np.array_equal(x[k], y[k]), (steps, k)
+            yf = det.check(q, off, segments=True, surface=surface)
+            for k in ('flags', 'seg_flags'):
+                assert np.array_equal(xf[k], yf[k]), (steps, k)
+            det.close()
+    ref = O.sweep(kind == 'Quadratic', orob, osc, q[:off[100]], off[:101])
+    det = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=4, sweep_heavy_steps=1)
+    _cmp(det.check(q[:off[100]], off[:101], segments=True, counts=True), ref)
+    det.close()
+    never.close()
