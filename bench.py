@@ -12,9 +12,12 @@ events on the launching stream (max over ranks for N > 1, weak scaling:
 every rank checks its own batch).  ``e2e`` repeats the step through the
 public C ABI with host buffers (pose upload and flag download inside the
 timed call; the step replayed as one CUDA graph that holds the copies
-between the pinned staging and the device, unless ``--no-graph``).  ``plain`` is the same engine driven the upstream way: frames
-of 64 poses with a host round trip per frame.  ``cpu_baseline`` times the
-FP64 oracle (flags only, every host thread) on a bounded sample.
+between the pinned staging and the device, unless ``--no-graph``).
+``plain`` is the same engine driven the upstream way: frames of 1,024 poses
+round-robin over 4 streams, one host thread per stream, the culled item count
+read back per frame (``plain_frame64``: 64-pose frames on one stream).
+``cpu_baseline`` times the FP64 oracle (flags only, every host thread) on a
+bounded sample.
 
 ``--impl reference`` times the CPU restatement of the reference path (the
 oracle port; the upstream OptiX path needs RT cores and the OptiX SDK) on the
@@ -818,7 +821,7 @@ def main():
     achieved = bytes_alg / (t_trav / 1e3) / 1e9
     form = tuned.get('stage_b_form', 0)
     if sweep:
-        span = ('k_sweep_traj' if st['path_flags'] & 1 else 'k_sweep') + ' + k_sweep_heavy'
+        span = ('k_sweep_traj' if st['path_flags'] & 1 else 'k_sweep') + ' + k_sweep_heavy x 2 (heavy, split)'
     elif form in (0, 3, 4):
         span = 'k_stage_ab + k_subtree x 2 + k_stage_b (deferred) + k_stage_b_heavy + k_discrete (overflow)'
     else:
@@ -892,7 +895,8 @@ def main():
         # k_sweep, k_sweep_heavy, k_flags x 2
         'gpu_launches': args.steps * ((3 + (2 if args.two_way else 1) * (6 if form in (0, 3, 4) else 4)
                                        + (1 if args.containment else 0) + 1) if not sweep
-                                      else 4 if st['path_flags'] & 1 else (5 if cfg['kind'] == 'Linear' else 6)),
+                                      # sweeps: light pass, heavy pass, its split pass, two flag gathers (+ FK and fit unstaged)
+                                      else 5 if st['path_flags'] & 1 else (6 if cfg['kind'] == 'Linear' else 7)),
         'stages_ms': {'prepare': float(np.mean([s['ms_prepare'] for s in spans])),
                       'cull': float(np.mean([s['ms_cull'] for s in spans])), 'traverse': t_trav},
         'roofline': {'bound': 'hbm', 'kernel': span, 'achieved': achieved,

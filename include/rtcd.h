@@ -284,10 +284,14 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
  * chunk lengths from 1 to 256 candidates, for the sweeps the binary and the
  * 4-wide edge tree (coordinate descent; sweeps are timed with segment flags
  * on)
- * - times the traversal with device events (median of three after a
- * warm-up run), keeps the fastest configuration in the detector and
- * writes it to best_out (optional).  The upstream picks its batch size per
- * experiment by hand (CollisionDetector.h:365-394). */
+ * - times each candidate's whole check replayed as a CUDA graph with device
+ * events, after a write of twice the L2 size when free memory allows (median
+ * of three replays after a warm-up run; the three fastest candidates are
+ * timed again over nine), keeps the fastest configuration in the detector
+ * and writes it to best_out and its time to best_ms (both optional).  The
+ * call allocates its flag buffers and that flush buffer for its duration.
+ * The upstream picks its batch size per experiment by hand
+ * (CollisionDetector.h:365-394). */
 RTCD_API rtcd_status rtcd_detector_autotune(rtcd_detector* det, const float* q_dev, const uint32_t* traj_offsets,
                                             uint32_t n, void* stream, rtcd_config* best_out, float* best_ms);
 

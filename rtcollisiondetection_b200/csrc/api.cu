@@ -1843,24 +1843,53 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
         rtcd_config best = saved;
         float best_t = 3.0e38f;
         std::vector<std::pair<float, rtcd_config>> tried;
-        // median of `reps` timed runs after a warm-up run
+        // Each candidate is timed as a caller running a stream of checks sees it: the whole check
+        // replayed as a CUDA graph (no host launch gaps, which dominate small batches when kernels
+        // are launched one by one), after a write larger than the L2 (the previous check's tree
+        // nodes are not left cached) when the device has the memory to spare for it.
+        DevBuf flush;
+        size_t flush_bytes = 0;
+        {
+            int l2 = 0;
+            cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, d->ctx->device);
+            size_t free_b = 0, total_b = 0;
+            cudaMemGetInfo(&free_b, &total_b);
+            const size_t want = 2ull * (size_t) std::max(l2, 0);
+            if (want && free_b > 8 * want) {
+                flush.ensure(want);
+                flush_bytes = want;
+            }
+        }
+        // a graph captured under another configuration must not be replayed for this one
+        auto retire_graph = [&] {
+            std::lock_guard<std::mutex> lock(d->mu);
+            if (!d->graph_exec) return;
+            cuda_check(cudaStreamSynchronize(s), "graph retire");
+            cudaGraphExecDestroy(d->graph_exec);
+            cudaGraphDestroy(d->graph);
+            d->graph_exec = nullptr;
+            d->graph = nullptr;
+        };
+        // median of `reps` timed replays after a warm-up run (which captures the graph)
         auto measure = [&](const rtcd_config& c, int reps) {
+            retire_graph();
             d->cfg = c;
             apply_launch_shape(d);
             float ms[16];
             for (int rep = 0; rep <= reps; ++rep) {
+                if (flush_bytes) cuda_check(cudaMemsetAsync(flush.p, rep & 255, flush_bytes, s), "L2 flush");
                 rtcd_status st = rtcd_check(d, q_dev, traj_offsets, n, flags.as<uint8_t>(),
-                                            discrete ? nullptr : seg.as<uint8_t>(), nullptr, RTCD_CHECK_TIMING, s);
+                                            discrete ? nullptr : seg.as<uint8_t>(), nullptr,
+                                            RTCD_CHECK_TIMING | RTCD_CHECK_GRAPH, s);
                 rtcd_stats stt;
                 if (st == RTCD_OK) st = rtcd_last_stats(d, &stt);
                 if (st != RTCD_OK) {
+                    retire_graph();
                     d->cfg = saved;
                     apply_launch_shape(d);
                     fail(st, g_last_error);
                 }
-                // sweeps: the whole check (the staged light pass runs the FK and fit the unstaged
-                // form leaves to the kernels before it); discrete: the traversal span
-                ms[rep] = discrete ? stt.ms_traverse : stt.ms_total;
+                ms[rep] = stt.ms_total;
             }
             std::sort(ms + 1, ms + reps + 1);
             return ms[1 + reps / 2];
@@ -1934,6 +1963,7 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 best = tried[k].second;
             }
         }
+        retire_graph();
         d->cfg = best;
         apply_launch_shape(d);
         if (best_out) *best_out = best;
