@@ -282,8 +282,9 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
  * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
  * then, for the discrete kinds, the four stage B forms, the first two at
  * chunk lengths from 1 to 256 candidates, for the sweeps the binary and the
- * 4-wide edge tree (coordinate descent; sweeps are timed with segment flags
- * on)
+ * 4-wide edge tree, staged or unstaged centres and grouped or single
+ * trajectories; then the launch shapes again under the settings found
+ * (coordinate descent; sweeps are timed with segment flags on)
  * - times each candidate's whole check replayed as a CUDA graph with device
  * events, after a write of twice the L2 size when free memory allows (median
  * of three replays after a warm-up run; the three fastest candidates are

@@ -1902,20 +1902,24 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 best = c;
             }
         };
-        // coordinate descent: the launch shape, then the light-pass budget,
-        // then the stage B form and its chunk length (discrete) or the tree (sweeps)
-        for (uint32_t t : {64u, 128u, 256u}) {
-            uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
-                                    : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
-            std::vector<uint32_t> shapes = {std::max(1u, fit / 4), std::max(1u, fit / 2), fit};
-            shapes.erase(std::unique(shapes.begin(), shapes.end()), shapes.end());
-            for (uint32_t per_sm : shapes) {
-                rtcd_config c = saved;
-                c.traverse_threads = t;
-                c.traverse_blocks_per_sm = per_sm;
-                time_cfg(c);
+        // coordinate descent: the launch shape, then the light-pass budget, then the stage B
+        // form and its chunk length (discrete) or the tree and staging (sweeps), then the launch
+        // shape again under the settings found (the best shape depends on them)
+        auto shape_pass = [&](const rtcd_config& base) {
+            for (uint32_t t : {64u, 128u, 256u}) {
+                uint32_t fit = discrete ? stage_b_max_blocks_per_sm(d->kind == RTCD_ROBOT_TO_OBS, t)
+                                        : sweep_max_blocks_per_sm(d->kind == RTCD_QUAD_SWEEP, t);
+                std::vector<uint32_t> shapes = {std::max(1u, fit / 4), std::max(1u, fit / 2), fit};
+                shapes.erase(std::unique(shapes.begin(), shapes.end()), shapes.end());
+                for (uint32_t per_sm : shapes) {
+                    rtcd_config c = base;
+                    c.traverse_threads = t;
+                    c.traverse_blocks_per_sm = per_sm;
+                    time_cfg(c);
+                }
             }
-        }
+        };
+        shape_pass(saved);
         for (uint32_t light : {16u, 32u, 64u}) {
             rtcd_config c = best;
             c.light_steps = light;
@@ -1949,6 +1953,7 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 time_cfg(c);
             }
         }
+        shape_pass(best);
         // run-to-run noise is of the order of the differences between the leading shapes: the
         // three fastest are timed again, longer, and the fastest of that round is kept
         std::stable_sort(tried.begin(), tried.end(),
