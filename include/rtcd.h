@@ -279,12 +279,13 @@ RTCD_API rtcd_status rtcd_sync(rtcd_detector* det, void* stream);
 /* Autotuner: runs the given device-resident batch (q_dev; traj_offsets on the
  * host for sweeps) with every traversal launch shape - 64, 128 and 256
  * threads per block, each at a quarter, half and all of the blocks per SM
- * that fit; then light-pass budgets (light_steps) of 16, 32 and 64 visits;
- * then, for the discrete kinds, the four stage B forms, the first two at
- * chunk lengths from 1 to 256 candidates, for the sweeps the binary and the
- * 4-wide edge tree, staged or unstaged centres and grouped or single
- * trajectories; then the launch shapes again under the settings found
- * (coordinate descent; sweeps are timed with segment flags on)
+ * that fit; then light-pass budgets (light_steps) of the default, 16, 32 and
+ * 64 visits; then, for the discrete kinds, the four stage B forms at chunk
+ * lengths from 1 to 256 candidates and the shared-memory top levels, for the
+ * sweeps the binary and the 4-wide edge tree, staged or unstaged centres and
+ * grouped or single trajectories; then the launch shapes again - rounds of
+ * this coordinate descent until one changes nothing (at most three; sweeps
+ * are timed with segment flags on)
  * - times each candidate's whole check replayed as a CUDA graph with device
  * events, after a write of twice the L2 size when free memory allows (median
  * of three replays after a warm-up run; the three fastest candidates are

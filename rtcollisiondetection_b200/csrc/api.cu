@@ -1919,25 +1919,26 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 }
             }
         };
-        shape_pass(saved);
-        for (uint32_t light : {16u, 32u, 64u}) {
-            rtcd_config c = best;
-            c.light_steps = light;
-            time_cfg(c);
-        }
-        if (!discrete) {  // the binary or the wide edge tree, then staged or unstaged centres
-            rtcd_config c = best;
-            c.stage_b_form = best.stage_b_form == 1 ? 0u : 1u;
-            time_cfg(c);
-            c = best;
-            c.sweep_unstaged = best.sweep_unstaged ? 0u : 1u;
-            time_cfg(c);
-            c = best;  // staged: grouped trajectories or one at a time
-            c.sweep_group = best.sweep_group == 1 ? 0u : 1u;
-            time_cfg(c);
-        }
-        if (discrete) {
-            const rtcd_config base = best;
+        auto light_pass = [&](const rtcd_config& base) {
+            for (uint32_t light : {0u, 16u, 32u, 64u}) {  // 0: the kind's default budget
+                rtcd_config c = base;
+                c.light_steps = light;
+                time_cfg(c);
+            }
+        };
+        auto form_pass = [&](const rtcd_config& base) {
+            if (!discrete) {  // the binary or the wide edge tree, staged or unstaged centres, grouping
+                rtcd_config c = base;
+                c.stage_b_form = base.stage_b_form == 1 ? 0u : 1u;
+                time_cfg(c);
+                c = base;
+                c.sweep_unstaged = base.sweep_unstaged ? 0u : 1u;
+                time_cfg(c);
+                c = base;
+                c.sweep_group = base.sweep_group == 1 ? 0u : 1u;
+                time_cfg(c);
+                return;
+            }
             for (uint32_t form : {1u, 2u, 3u, 4u})
                 for (uint32_t chunk : {1u, 16u, 64u, 256u}) {
                     rtcd_config c = base;
@@ -1952,8 +1953,17 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 c.top_nodes_shared = best.top_nodes_shared ? 0u : 85u;  // 1 + 4 + 16 + 64: the first four levels
                 time_cfg(c);
             }
+        };
+        // rounds of descent over the three groups of settings until a round changes nothing (the
+        // best light budget and stage-B form depend on the launch shape and back)
+        shape_pass(saved);
+        for (int round = 0; round < 3; ++round) {
+            const rtcd_config start = best;
+            light_pass(best);
+            form_pass(best);
+            shape_pass(best);
+            if (std::memcmp(&start, &best, sizeof(rtcd_config)) == 0) break;
         }
-        shape_pass(best);
         // run-to-run noise is of the order of the differences between the leading shapes: the
         // three fastest are timed again, longer, and the fastest of that round is kept
         std::stable_sort(tried.begin(), tried.end(),
