@@ -356,3 +356,32 @@ def test_top_levels_in_shared_memory_agree(dense, panda, name, okind):
         out = det.check(q, counts=True)
         assert np.array_equal(out['flags'], base['flags']) and np.array_equal(out['counts'], base['counts'])
         det.close()
+
+
+@pytest.mark.parametrize('name,okind', KINDS)
+def test_cull_keeps_every_hit_many_obstacles(ctx, panda, name, okind):
+    """A scene of 165 obstacles: 90 random boxes and icospheres plus a lattice
+    of small boxes.  With the OBB cull, flags and upstream counts equal the
+    run without it exactly (no item with a hit is dropped) and the FP64
+    oracle's outside the band."""
+    base = scenes.random_scene(50, 40, 1, seed=5, box_ext=(0.02, 0.3))
+    lattice = [scenes.box_mesh((x, y, z), (0.03, 0.03, 0.03))
+               for x in np.linspace(-0.9, 0.9, 5) for y in np.linspace(-0.9, 0.9, 5) for z in (0.2, 0.6, 1.0)]
+    verts, tris, off = [base.verts], [base.tris], list(base.obstacle_tri_off)
+    nv = len(base.verts)
+    for v, t in lattice:
+        verts.append(v)
+        tris.append(t + nv)
+        nv += len(v)
+        off.append(off[-1] + len(t))
+    mesh = scenes.Mesh(np.concatenate(verts), np.concatenate(tris), np.asarray(off, np.uint32))
+    assert mesh.n_obstacles == 165
+    scene = rtcd.Scene.from_mesh(ctx, mesh)
+    robot = rtcd.Robot(ctx, panda)
+    q = scenes.uniform_poses(panda, 2048, seed=17)
+    det = rtcd.Detector(ctx, name, robot, scene)
+    a = det.check(q, counts=True)
+    b = det.check(q, counts=True, flags=rtcd.CHECK_NO_CULL)
+    assert np.array_equal(a['flags'], b['flags']) and np.array_equal(a['counts'], b['counts'])
+    _compare(a, O.discrete(okind, O.Robot(panda), O.Scene(mesh), q))
+    assert a['flags'].any()
