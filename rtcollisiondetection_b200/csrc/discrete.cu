@@ -1018,13 +1018,15 @@ struct ObbTest {
     __device__ __forceinline__ bool operator()(const Box& b) const { return obb_aabb(b, ob, ext); }
 };
 
-// Capped at 5 resident blocks per SM worth of registers (a few spills, more
-// warps to hide the node-load latency; measured on the 65,536-pose workload).
+// Register caps (measured on the 65,536-pose dense workload and the dense
+// shelf): RobotToObs at 5 resident blocks per SM (96 registers, a few spills;
+// more warps to hide the node-load latency: 4 blocks at 128 registers was 7 %
+// slower), ObsToRobot at 4 (128 registers, no spills: 2-4 % faster than 5).
 // TOP: the first W.top_nodes wide nodes are staged in shared memory after the
 // frontiers and read from there (a separate instantiation, so the default
 // kernel's node loads carry no branch).
 template <bool R2O, bool PACKET, bool TOP>
-__global__ void __launch_bounds__(kAbWarps * 32, 5) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
+__global__ void __launch_bounds__(kAbWarps * 32, R2O ? 5 : 4) k_stage_ab(const RobotDev R, const SceneDev S, const WaveArgs W) {
     extern __shared__ uint32_t s_front[];  // [kAbWarps][S.wide_front], then (TOP) the staged wide nodes
     __shared__ uint32_t s_cand[kAbWarps][kCandBuf];
     __shared__ uint32_t s_hits[kAbWarps];  // a lane of the warp's current stage-B step hit its pose
