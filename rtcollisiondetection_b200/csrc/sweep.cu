@@ -1024,6 +1024,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
         uint32_t rec = h, start = S.edge_root;
         if (SPLIT) {
             const uint2 item = A.split[h];
+            if (item.x == kNone) continue;  // a blanked slot of a reservation that did not fit
             rec = item.x;
             start = item.y;
         }
@@ -1072,7 +1073,11 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
                     for (int k = lane; k < sp; k += 32) A.split[base + k] = make_uint2(rec, fr[k]);
                     break;
                 }
-                handing = false;  // no room: this warp finishes the unit
+                // no room: this warp finishes the unit, and the reserved slots below the capacity
+                // are blanked (the split pass reads every slot up to it)
+                for (int k = lane; k < sp && (uint64_t) base + (uint64_t) k < A.split_cap; k += 32)
+                    A.split[base + k] = make_uint2(kNone, kNone);
+                handing = false;
                 budgeted = false;
             }
             if (budgeted && ++warp_steps >= A.heavy_steps && sp >= kSplitMinFront) {

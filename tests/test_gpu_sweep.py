@@ -259,3 +259,34 @@ def test_heavy_split_pass_keeps_results(sweep_setup, panda, kind):
     _cmp(det.check(q[:off[100]], off[:101], segments=True, counts=True), ref)
     det.close()
     never.close()
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_split_list_overflow_keeps_results(sweep_setup, panda, kind):
+    """A batch whose split list (one slot per unit the light pass can defer)
+    cannot hold every frontier handed to it: 64 trajectories parked at the
+    pose that collides most (every waypoint the same), counted (no early
+    exit), a light budget of one visit and heavy units splitting after one
+    step.  A reservation that does not fit stays with its warp and its slots
+    below the capacity are blanked, so the flags, segment flags and counts
+    equal the never-splitting run's, on fresh and on reused device memory
+    (repeated detectors)."""
+    robot, scene, orob, osc = sweep_setup
+    cand = scenes.uniform_poses(panda, 512, seed=22)
+    probe = rtcd.Detector(robot.ctx, 'Linear', robot, scene)
+    pairs = np.repeat(cand, 2, axis=0)
+    hits = probe.check(pairs, np.arange(0, 2 * len(cand) + 1, 2, dtype=np.uint32), counts=True)['counts']
+    probe.close()
+    pose = cand[int(np.argmax(hits))]
+    q = np.tile(pose, (64 * 16, 1)).astype(np.float32)
+    off = np.arange(0, 64 * 16 + 1, 16, dtype=np.uint32)
+    never = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=1, sweep_heavy_steps=0xFFFFFFFF)
+    x = never.check(q, off, segments=True, counts=True)
+    assert x['flags'].all() and never.stats()['deferred'] > 10000
+    for _ in range(3):
+        det = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=1, sweep_heavy_steps=1)
+        y = det.check(q, off, segments=True, counts=True)
+        for k in ('flags', 'seg_flags', 'counts'):
+            assert np.array_equal(x[k], y[k]), k
+        det.close()
+    never.close()
