@@ -59,7 +59,10 @@ typedef enum {
 
 /* rtcd_check flags */
 #define RTCD_CHECK_COUNTS (1u << 0)        /* also produce the upstream hit counts (no early exit) */
-#define RTCD_CHECK_HOST_BUFFERS (1u << 1)  /* q, traj offsets and outputs are host memory */
+#define RTCD_CHECK_HOST_BUFFERS (1u << 1)  /* q, traj offsets and outputs are host memory; a q in page-locked
+                                              memory (cudaHostAlloc, cudaHostRegister) is uploaded by DMA
+                                              directly, pageable memory is copied into the detector's pinned
+                                              staging first */
 #define RTCD_CHECK_NO_CULL (1u << 2)       /* skip the OBB prefilter of the discrete detectors (every item goes to
                                               the traversal, whose first step rejects the far ones: up to 9 % faster at
                                               a few thousand poses, slower at tens of thousands) */
@@ -88,7 +91,9 @@ typedef enum {
                                               with these pointers, sizes, flags and - for sweeps - trajectory
                                               offsets; any other call on the detector retires it).  With
                                               RTCD_CHECK_HOST_BUFFERS the graph holds the upload from the
-                                              detector's pinned staging, the kernels and the download back to it;
+                                              detector's pinned staging (from a page-locked q itself, whose
+                                              address then joins the replay key), the kernels and the download
+                                              back to the staging;
                                               only the copies between the caller's arrays and the staging run
                                               outside it, and the call returns with the results in place */
 

@@ -1139,6 +1139,18 @@ void ensure_weights(rtcd_detector* d, uint32_t max_wp) {
     cuda_check(cudaStreamSynchronize(d->stream), "weights upload");
 }
 
+// True when p is page-locked host memory (cudaHostAlloc, cudaMallocHost,
+// cudaHostRegister): the upload then reads it by DMA directly instead of
+// copying it into the detector's pinned staging first.
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 void check_device_errors(rtcd_detector* d, cudaStream_t s) {
     uint32_t e = 0;
     cuda_check(cudaMemcpyAsync(&e, d->err.p, 4, cudaMemcpyDeviceToHost, s), "error readback");
@@ -1317,9 +1329,13 @@ void check_discrete(rtcd_detector* d, const float* q, uint32_t n, uint8_t* flags
     const float* d_q = q;
     if (host) {
         d->q.ensure(4ull * n * dof);
-        d->pin_in.ensure(4ull * n * dof);
-        std::memcpy(d->pin_in.p, q, 4ull * n * dof);
-        cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * n * dof, cudaMemcpyHostToDevice, s), "q upload");
+        const void* src = q;
+        if (!host_pinned(q)) {
+            d->pin_in.ensure(4ull * n * dof);
+            std::memcpy(d->pin_in.p, q, 4ull * n * dof);
+            src = d->pin_in.p;
+        }
+        cuda_check(cudaMemcpyAsync(d->q.p, src, 4ull * n * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
     d->pose_hit.ensure(4ull * n);
@@ -1469,9 +1485,13 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     const float* d_q = q;
     if (host) {
         d->q.ensure(4ull * total_wp * dof);
-        d->pin_in.ensure(4ull * total_wp * dof);
-        std::memcpy(d->pin_in.p, q, 4ull * total_wp * dof);
-        cuda_check(cudaMemcpyAsync(d->q.p, d->pin_in.p, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
+        const void* src = q;
+        if (!host_pinned(q)) {
+            d->pin_in.ensure(4ull * total_wp * dof);
+            std::memcpy(d->pin_in.p, q, 4ull * total_wp * dof);
+            src = d->pin_in.p;
+        }
+        cuda_check(cudaMemcpyAsync(d->q.p, src, 4ull * total_wp * dof, cudaMemcpyHostToDevice, s), "q upload");
         d_q = d->q.as<float>();
     }
     if (!capturing) cuda_check(cudaEventRecord(d->staged, s), "event");
@@ -1644,13 +1664,19 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
             uint8_t* gseg = seg_flags_out;
             uint32_t* gcounts = counts_out;
             size_t in_bytes = 0, n_seg = 0, seg_at = 0, counts_at = 0, err_at = 0;
+            const void* up_src = nullptr;  // host: the caller's page-locked array or the pinned staging
             if (host) {
                 in_bytes = 4ull * (discrete ? n : traj_offsets[n]) * d->robot->dof;
                 if (seg_flags_out)
                     for (uint32_t i = 0; i < n; ++i) n_seg += pieces_of(d->kind, traj_offsets[i + 1] - traj_offsets[i], f);
-                d->pin_in.ensure(std::max<size_t>(in_bytes, 16));
                 d->hq.ensure(std::max<size_t>(in_bytes, 16));
-                std::memcpy(d->pin_in.p, q, in_bytes);
+                if (host_pinned(q)) {  // the graph's upload reads the caller's page-locked array itself
+                    up_src = q;
+                } else {
+                    d->pin_in.ensure(std::max<size_t>(in_bytes, 16));
+                    std::memcpy(d->pin_in.p, q, in_bytes);
+                    up_src = d->pin_in.p;
+                }
                 gq = d->hq.as<float>();
                 d->hflags.ensure(n);
                 gflags = d->hflags.as<uint8_t>();
@@ -1667,15 +1693,14 @@ rtcd_status rtcd_check(rtcd_detector* d, const float* q, const uint32_t* traj_of
                 counts_at = seg_at + ((n_seg + 15) & ~size_t(15));
                 err_at = counts_at + (counts_out ? 4ull * n : 0);
                 d->pin_out.ensure(err_at + 16);
-                for (uint64_t v : {(uint64_t) d->pin_in.p, (uint64_t) d->pin_out.p}) h = (h ^ v) * 1099511628211ull;
+                for (uint64_t v : {(uint64_t) up_src, (uint64_t) d->pin_out.p}) h = (h ^ v) * 1099511628211ull;
             }
             const uint64_t key[8] = {(uint64_t) gq, n, (uint64_t) gflags, (uint64_t) gcounts, f, (uint64_t) s,
                                      (uint64_t) gseg, h};
             uint8_t* po = d->pin_out.as<uint8_t>();
             auto run = [&] {
                 const uint32_t fd = f & ~RTCD_CHECK_HOST_BUFFERS;
-                if (host)
-                    cuda_check(cudaMemcpyAsync(d->hq.p, d->pin_in.p, in_bytes, cudaMemcpyHostToDevice, s), "q upload");
+                if (host) cuda_check(cudaMemcpyAsync(d->hq.p, up_src, in_bytes, cudaMemcpyHostToDevice, s), "q upload");
                 if (discrete)
                     check_discrete(d, gq, n, gflags, gcounts, fd, s);
                 else

@@ -385,3 +385,37 @@ def test_cull_keeps_every_hit_many_obstacles(ctx, panda, name, okind):
     assert np.array_equal(a['flags'], b['flags']) and np.array_equal(a['counts'], b['counts'])
     _compare(a, O.discrete(okind, O.Robot(panda), O.Scene(mesh), q))
     assert a['flags'].any()
+
+
+def _pinned(a):
+    """A page-locked copy of a (torch's pinned allocator), as a numpy view."""
+    import torch
+    p = torch.empty(a.shape, dtype=torch.float32).pin_memory().numpy()
+    p[...] = a
+    return p
+
+
+def test_page_locked_poses_match_pageable(ctx, panda):
+    """Host calls whose poses sit in page-locked memory upload them by DMA
+    directly, in the direct path and in the graph (captured with the caller's
+    array as the copy source): flags and counts equal the pageable calls', a
+    pinned array rewritten in place is read afresh on replay, and a switch
+    between pinned and pageable arrays re-captures."""
+    mesh = scenes.discrete_small(seed=5)
+    robot = rtcd.Robot(ctx, panda)
+    scene = rtcd.Scene.from_mesh(ctx, mesh)
+    qs = [scenes.uniform_poses(panda, 900, seed=seed) for seed in (3, 4)]
+    for kind in ('RobotToObs', 'ObsToRobot'):
+        det = rtcd.Detector(ctx, kind, robot, scene)
+        refs = [det.check(q, counts=True) for q in qs]
+        assert any(r['flags'].any() for r in refs)
+        pin = _pinned(qs[0])
+        for graph in (0, rtcd.CHECK_GRAPH):
+            for i in (0, 1, 0, 1):
+                pin[...] = qs[i]     # same page-locked array, new values
+                got = det.check(pin, counts=True, flags=graph)
+                assert np.array_equal(got['flags'], refs[i]['flags'])
+                assert np.array_equal(got['counts'], refs[i]['counts'])
+                got = det.check(qs[1 - i], counts=True, flags=graph)   # pageable in between
+                assert np.array_equal(got['flags'], refs[1 - i]['flags'])
+        det.close()

@@ -290,3 +290,29 @@ def test_split_list_overflow_keeps_results(sweep_setup, panda, kind):
             assert np.array_equal(x[k], y[k]), k
         det.close()
     never.close()
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_page_locked_waypoints_match_pageable(sweep_setup, panda, kind):
+    """Sweep host calls with waypoints in page-locked memory (direct DMA, in
+    the direct path and in the graph) give the pageable calls' trajectory and
+    segment flags; a pinned array rewritten in place is read afresh."""
+    import torch
+    robot, scene, _, _ = sweep_setup
+    n_wp = scenes.log_uniform_counts(160, 8, 48, seed=7)
+    walks = [scenes.random_walk_trajectories(panda, 160, n_wp, seed=s) for s in (7, 8)]
+    off = walks[0][1]
+    assert all(np.array_equal(w[1], off) for w in walks)
+    det = rtcd.Detector(robot.ctx, kind, robot, scene)
+    refs = [det.check(q, off, segments=True) for q, _ in walks]
+    assert any(r['flags'].any() for r in refs)
+    pin = torch.empty(walks[0][0].shape, dtype=torch.float32).pin_memory().numpy()
+    for graph in (0, rtcd.CHECK_GRAPH):
+        for i in (0, 1, 0):
+            pin[...] = walks[i][0]
+            got = det.check(pin, off, segments=True, flags=graph)
+            assert np.array_equal(got['flags'], refs[i]['flags'])
+            assert np.array_equal(got['seg_flags'], refs[i]['seg_flags'])
+            got = det.check(walks[1 - i][0], off, flags=graph)
+            assert np.array_equal(got['flags'], refs[1 - i]['flags'])
+    det.close()
