@@ -590,13 +590,20 @@ __device__ __forceinline__ bool leaf_hit_surface(const float4* __restrict__ ep, 
 // One lane's descent to its next leaf over the obstacle-edge tree (WIDE: the
 // 4-wide copy, children pushed far to near; else the binary tree, the child
 // met first along the chord visited first).  Returns the leaf, or kNone when
-// the stack ran empty.
+// the stack ran empty.  The nearest overlapping child of a node is carried
+// to the next step in a register instead of being pushed and popped at once
+// (the stack lives in local memory, so that round trip sat on every step's
+// dependent chain); the visit order is the same.
 template <bool QUAD, bool WIDE>
 __device__ __forceinline__ uint32_t sweep_descend(const float4* __restrict__ en, uint32_t* st, int& sp, uint32_t& steps,
                                                   const SweepCull& c, unsigned long long& n_node, uint32_t* err) {
     uint32_t leaf = kNone;
-    while (sp > 0) {
-        const uint32_t ref = st[--sp];
+    uint32_t ref = kNone;  // the node to visit next, when not on the stack
+    while (true) {
+        if (ref == kNone) {
+            if (sp <= 0) break;
+            ref = st[--sp];
+        }
         ++steps;
         if (ref & kLeaf) {
             leaf = ref & ~kLeaf;
@@ -634,13 +641,15 @@ __device__ __forceinline__ uint32_t sweep_descend(const float4* __restrict__ en,
                 }
             };
             cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+            ref = kNone;
             if (sp + kWide > kStack) {  // cannot happen: the wide form runs only on shallow enough trees
                 atomicOr(err, kErrStack);
                 sp = 0;
             } else {
 #pragma unroll
-                for (int j = 0; j < kWide; ++j)
+                for (int j = 0; j < kWide - 1; ++j)
                     if (t[j] < 2.f) st[sp++] = cr[j];
+                if (t[kWide - 1] < 2.f) ref = cr[kWide - 1];  // the nearest: visited next
             }
             continue;
         }
@@ -655,13 +664,15 @@ __device__ __forceinline__ uint32_t sweep_descend(const float4* __restrict__ en,
             hr = hl = false;
             sp = 0;
         }
-        // the child met first along the chord is visited first
-        if (hr && hl && tr < tl) {
-            st[sp++] = rl;
-            st[sp++] = rr;
-        } else {
-            if (hr) st[sp++] = rr;
-            if (hl) st[sp++] = rl;
+        // the child met first along the chord is visited first (next), the other stacked
+        ref = kNone;
+        if (hr && hl) {
+            st[sp++] = tr < tl ? rl : rr;
+            ref = tr < tl ? rr : rl;
+        } else if (hr) {
+            ref = rr;
+        } else if (hl) {
+            ref = rl;
         }
     }
     return leaf;
