@@ -962,7 +962,8 @@ def main():
                             retests_per_step=st['fp64_retests'],
                             root_findings_per_step=st['candidates'] if cfg['kind'] == 'Quadratic' else None,
                             in_band_of_checked=line['check']['in_band'])
-    if args.serve_seconds > 0 and rank == 0 and args.config == 'c2':
+    # the served stream is a one-GPU measurement: a scaling run (N > 1) skips it
+    if args.serve_seconds > 0 and rank == 0 and world == 1 and args.config == 'c2':
         line['served'] = served_stream(ctx, args.serve_seconds, saturate_requests=args.saturate_requests)
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         line['cpu_baseline'] = cpu_baseline(cfg, model, mesh, spheres, q, off)
