@@ -175,6 +175,11 @@ typedef struct {
                                         four or more) go, one per warp, to a split pass, so a few units with
                                         very large traversals do not hold the pass while the rest of the GPU
                                         idles; 0 = 32, 0xFFFFFFFF = never */
+    uint32_t sweep_descend_cap;      /* sweeps, light pass: node visits a lane makes in one descent before the
+                                        warp's lanes without work take new units (the descent then resumes
+                                        where it stopped), so a lane that finished a short unit does not wait
+                                        out a long one; 0 = 3, 0xFFFFFFFF = every descent runs to its next
+                                        leaf (the autotuner tries 2, 3, 4 and 6) */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream

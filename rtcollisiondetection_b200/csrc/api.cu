@@ -1567,6 +1567,9 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                     : d->cfg.light_steps                ? d->cfg.light_steps
                                                               : 16u;
+    A.descend_cap = d->cfg.sweep_descend_cap == 0xFFFFFFFFu ? 0u
+                    : d->cfg.sweep_descend_cap                ? d->cfg.sweep_descend_cap
+                                                                  : 3u;
     if (A.light_steps) {
         // room for every unit (near dense geometry most units of a piece can spill)
         const uint32_t cap = (uint32_t) std::min<uint64_t>(std::max<uint64_t>(pieces * ns, 1024), 1u << 20);
@@ -1962,6 +1965,11 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 c = base;
                 c.sweep_group = base.sweep_group == 1 ? 0u : 1u;
                 time_cfg(c);
+                for (uint32_t cap : {2u, 4u, 6u}) {  // visits per descent (0: the default, 3)
+                    c = base;
+                    c.sweep_descend_cap = base.sweep_descend_cap == cap ? 0u : cap;
+                    time_cfg(c);
+                }
                 return;
             }
             for (uint32_t form : {1u, 2u, 3u, 4u})

@@ -168,6 +168,8 @@ struct SweepArgs {
     int want_counts;
     int want_pieces;
     uint32_t light_steps;      // visits before a unit moves to the heavy pass; 0 = no heavy pass
+    uint32_t descend_cap;      // light pass: visits a lane makes per descent before the warp's lanes
+                               // without work take new units (its descent resumes after); 0 = until a leaf
     int binary_tree;           // light pass on the binary edge tree (else the 4-wide one where the scene allows)
     SweepRec* heavy;           // [heavy_cap] units handed to the heavy pass
     uint32_t heavy_cap;

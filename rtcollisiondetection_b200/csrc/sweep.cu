@@ -596,13 +596,19 @@ __device__ __forceinline__ bool leaf_hit_surface(const float4* __restrict__ ep, 
 // dependent chain); the visit order is the same.
 template <bool QUAD, bool WIDE>
 __device__ __forceinline__ uint32_t sweep_descend(const float4* __restrict__ en, uint32_t* st, int& sp, uint32_t& steps,
-                                                  const SweepCull& c, unsigned long long& n_node, uint32_t* err) {
+                                                  const SweepCull& c, unsigned long long& n_node, uint32_t* err,
+                                                  uint32_t cap) {
     uint32_t leaf = kNone;
     uint32_t ref = kNone;  // the node to visit next, when not on the stack
-    while (true) {
+    if (cap == 0) cap = 0xFFFFFFFFu;  // every call makes at least one visit
+    for (uint32_t visits = 0;; ++visits) {
         if (ref == kNone) {
             if (sp <= 0) break;
             ref = st[--sp];
+        }
+        if (visits == cap) {  // hand the lane back; the stack holds the rest (the last push left room)
+            st[sp++] = ref;
+            break;
         }
         ++steps;
         if (ref & kLeaf) {
@@ -747,7 +753,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
             checked = steps;
             if (A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj)) sp = 0;
         }
-        leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err);
+        leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err, A.descend_cap);
         if (leaf != kNone) {
             ++n_leaf;
             if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots) : leaf_hit<QUAD>(ep, leaf, U, A.stats, n_roots)) {
@@ -956,7 +962,7 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
             volatile uint32_t* pf = reinterpret_cast<volatile uint32_t*>(s_slots + (size_t) g * slot_words + f_at);
             // flags only: drop the unit once its piece (or trajectory) is decided
             if (!A.want_counts && (A.want_pieces ? pf[piece] : s_hit[g])) sp = 0;
-            const uint32_t leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err);
+            const uint32_t leaf = sweep_descend<QUAD, WIDE>(en, st, sp, steps, c, n_node, A.err, A.descend_cap);
             if (leaf != kNone) {
                 ++n_leaf;
                 if (SURF ? leaf_hit_surface<QUAD>(ep, leaf, U, A.stats, n_roots)

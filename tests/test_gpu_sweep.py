@@ -316,3 +316,26 @@ def test_page_locked_waypoints_match_pageable(sweep_setup, panda, kind):
             got = det.check(walks[1 - i][0], off, flags=graph)
             assert np.array_equal(got['flags'], refs[1 - i]['flags'])
     det.close()
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+def test_descend_cap_keeps_results(sweep_setup, panda, kind):
+    """The light pass's per-descent visit cap only changes when idle lanes
+    take new units: trajectory flags, segment flags and counts are the same
+    at caps 1, 3 (the default), 4 and none, with and without the heavy pass."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(200, 8, 40, seed=11)
+    q, off = scenes.random_walk_trajectories(panda, 200, n_wp, seed=11)
+    ref = O.sweep(kind == 'Quadratic', orob, osc, q, off)
+    outs = []
+    for light in (0, 0xFFFFFFFF):
+        for cap in (1, 0, 4, 0xFFFFFFFF):
+            det = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=light, sweep_descend_cap=cap)
+            seg = det.check(q, off, segments=True)
+            cnt = det.check(q, off, counts=True)
+            _cmp(seg, ref)
+            _cmp(cnt, ref)
+            outs.append((seg['flags'], seg['seg_flags'], cnt['counts']))
+            det.close()
+    for o in outs[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(o, outs[0]))
