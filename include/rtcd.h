@@ -180,6 +180,11 @@ typedef struct {
                                         where it stopped), so a lane that finished a short unit does not wait
                                         out a long one; 0 = 3, 0xFFFFFFFF = every descent runs to its next
                                         leaf (the autotuner tries 2, 3, 4 and 6) */
+    uint32_t sweep_heavy_wide;       /* sweeps: 1 = the heavy and split passes expand the scene's 4-wide edge tree,
+                                        four lanes per node (half the levels; faster where many units reach
+                                        the heavy pass near dense geometry), 0 = the binary tree, one lane
+                                        per node (fewer boxes tested: faster on thin geometry); the
+                                        autotuner tries both */
 } rtcd_config;
 
 /* Replaces the OptiX context + streams of createContextStream

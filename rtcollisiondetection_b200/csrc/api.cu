@@ -1567,6 +1567,7 @@ void check_sweep(rtcd_detector* d, const float* q, const uint32_t* traj_off, uin
     A.light_steps = d->cfg.light_steps == 0xFFFFFFFFu ? 0u
                     : d->cfg.light_steps                ? d->cfg.light_steps
                                                               : 16u;
+    A.heavy_wide = d->cfg.sweep_heavy_wide ? 1 : 0;
     A.descend_cap = d->cfg.sweep_descend_cap == 0xFFFFFFFFu ? 0u
                     : d->cfg.sweep_descend_cap                ? d->cfg.sweep_descend_cap
                                                                   : 3u;
@@ -1964,6 +1965,9 @@ rtcd_status rtcd_detector_autotune(rtcd_detector* d, const float* q_dev, const u
                 time_cfg(c);
                 c = base;
                 c.sweep_group = base.sweep_group == 1 ? 0u : 1u;
+                time_cfg(c);
+                c = base;
+                c.sweep_heavy_wide = base.sweep_heavy_wide ? 0u : 1u;
                 time_cfg(c);
                 for (uint32_t cap : {2u, 4u, 6u}) {  // visits per descent (0: the default, 3)
                     c = base;

@@ -177,6 +177,7 @@ struct SweepArgs {
     uint32_t* heavy_work;      // heavy-pass work counter
     uint32_t heavy_steps;      // frontier steps a heavy unit takes before its open frontier goes to the split
                                // pass (0: never)
+    int heavy_wide;            // heavy and split passes on the 4-wide edge tree (else the binary one)
     uint2* split;              // [split_cap] (heavy record, edge-tree node) pairs for the split pass
     uint32_t split_cap;
     uint32_t* split_count;     // pairs appended (past split_cap: the unit was finished by its warp)

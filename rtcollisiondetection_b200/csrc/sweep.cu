@@ -1009,7 +1009,11 @@ __global__ void __launch_bounds__(BLOCK, QUAD ? 5 * 128 / BLOCK : 6 * 128 / BLOC
 // LBVH through a shared LIFO frontier (up to 32 nodes a step, survivors
 // pushed), collects leaf survivors in a shared buffer and tests them 32 at a
 // time, one leaf per lane.  The unit's serial depth drops from its node count
-// to about its node count / 32 plus the tree depth.
+// to about its node count / 32 plus the tree depth.  WIDE: the frontier holds
+// nodes of the scene's 4-wide edge tree instead, up to 8 a step with four
+// lanes per node, each lane loading and testing one child record (half the
+// levels of the binary tree; more boxes tested in all, which the reference's
+// thin shelf boards do not repay: SweepArgs.heavy_wide chooses).
 constexpr int kHeavyWarps = 4;
 constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
 
@@ -1023,7 +1027,7 @@ constexpr int kLeafBuf = 96;  // < 32 waiting + up to 64 added by one node step
 // the end.  Every node is expanded exactly once either way, so flags and
 // counts do not depend on where a unit split.
 constexpr int kSplitMinFront = 4;
-template <bool QUAD, bool SURF, bool SPLIT>
+template <bool QUAD, bool SURF, bool SPLIT, bool WIDE>
 __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev S, const SweepArgs A) {
     __shared__ uint32_t s_front[kHeavyWarps][kFrontier];
     __shared__ uint32_t s_leaf[kHeavyWarps][kLeafBuf];
@@ -1038,7 +1042,7 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
         if (lane == 0) h = atomicAdd(SPLIT ? A.split_work : A.heavy_work, 1u);
         h = __shfl_sync(0xffffffffu, h, 0);
         if (h >= n_work) break;
-        uint32_t rec = h, start = S.edge_root;
+        uint32_t rec = h, start = WIDE ? S.edge_wide_root : S.edge_root;
         if (SPLIT) {
             const uint2 item = A.split[h];
             if (item.x == kNone) continue;  // a blanked slot of a reservation that did not fit
@@ -1105,6 +1109,49 @@ __global__ void __launch_bounds__(kHeavyWarps * 32) k_sweep_heavy(const SceneDev
                 uint32_t dec = 0;
                 if (lane == 0) dec = A.want_pieces ? ldflag(A.piece_hit + U.piece_g) : ldflag(A.traj_hit + U.traj);
                 if (__shfl_sync(0xffffffffu, dec, 0)) break;
+            }
+            if constexpr (WIDE) {
+                // up to 8 wide nodes a step, four lanes per node, one child record per lane
+                const int take = min(sp, 32 / kWide);
+                sp -= take;
+                const int slot = lane / kWide, j = lane % kWide;
+                const uint32_t ref = slot < take ? fr[sp + slot] : kNone;
+                __syncwarp();
+                bool hc = false;
+                uint32_t rc = kNone;
+                if (ref != kNone) {
+                    if (ref & kLeaf) {  // a one-edge scene: the root itself is a leaf
+                        if (j == 0) {
+                            hc = true;
+                            rc = ref;
+                        }
+                    } else {
+                        const float4* r = S.edge_wide + 2ull * kWide * ref + 2 * j;
+                        const float4 ra = __ldg(r), rb = __ldg(r + 1);
+                        rc = __float_as_uint(rb.z);
+                        if (rc != kNone) {  // an empty slot of a node with fewer than four children
+                            ++n_node;
+                            Box bx;
+                            bx.lo[0] = ra.x; bx.lo[1] = ra.y; bx.lo[2] = ra.z;
+                            bx.hi[0] = ra.w; bx.hi[1] = rb.x; bx.hi[2] = rb.y;
+                            float t;
+                            hc = cull_box<QUAD>(c, bx, t);
+                        }
+                    }
+                }
+                const bool pc = hc && !(rc & kLeaf), ec = hc && (rc & kLeaf);
+                const uint32_t mpc = __ballot_sync(0xffffffffu, pc), mec = __ballot_sync(0xffffffffu, ec);
+                const int npush = __popc(mpc);
+                if (sp + npush > kFrontier) {  // cannot happen for trees within the depth limit
+                    if (lane == 0) atomicOr(A.err, kErrStack);
+                    break;
+                }
+                if (pc) fr[sp + __popc(mpc & lt)] = rc;
+                sp += npush;
+                if (ec) lf[nl + __popc(mec & lt)] = rc & ~kLeaf;
+                nl += __popc(mec);
+                __syncwarp();
+                continue;
             }
             const int take = min(sp, 32);
             sp -= take;
@@ -1208,12 +1255,12 @@ uint32_t sweep_max_blocks_per_sm(bool quad, uint32_t threads) {
 
 uint32_t sweep_persistent_blocks(bool quad) { return sweep_max_blocks_per_sm(quad, kTravThreads) * device_sm_count(); }
 
-template <bool QUAD, bool SURF>
+template <bool QUAD, bool SURF, bool WIDE>
 static uint32_t heavy_blocks() {
     static uint32_t blocks = 0;
     if (!blocks) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD, SURF, false>, kHeavyWarps * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_heavy<QUAD, SURF, false, WIDE>, kHeavyWarps * 32, 0);
         blocks = (uint32_t) std::max(1, per_sm) * device_sm_count();
     }
     return blocks;
@@ -1274,6 +1321,19 @@ static void launch_staged(const SceneDev& S, const RobotDev& R, const SweepArgs&
     kern<<<blocks, BLOCK, smem, s>>>(S, R, G);
 }
 
+// The heavy pass over the light pass's deferred units, then (A.heavy_steps)
+// the split pass over the frontier nodes the heavy pass handed on.
+template <bool QUAD, bool SURF, bool WIDE>
+static void launch_heavy(const SceneDev& S, const SweepArgs& H, uint32_t heavy_share, cudaStream_t s) {
+    const uint32_t hb = std::max(1u, heavy_blocks<QUAD, SURF, WIDE>() * heavy_share / 100);
+    k_sweep_heavy<QUAD, SURF, false, WIDE><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
+    cuda_check(cudaGetLastError(), "k_sweep_heavy");
+    if (H.heavy_steps) {
+        k_sweep_heavy<QUAD, SURF, true, WIDE><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
+        cuda_check(cudaGetLastError(), "k_sweep_heavy (split)");
+    }
+}
+
 template <bool QUAD, bool SURF>
 static void sweep_dispatch(const SceneDev& S, const RobotDev& R, const SweepArgs& A, uint32_t blocks, uint32_t threads,
                            uint32_t heavy_share, bool staged, cudaStream_t s, cudaEvent_t ev_light) {
@@ -1306,19 +1366,11 @@ static void sweep_dispatch(const SceneDev& S, const RobotDev& R, const SweepArgs
     }
     cuda_check(cudaGetLastError(), staged ? "k_sweep_traj" : "k_sweep");
     if (ev_light) cuda_check(cudaEventRecord(ev_light, s), "event");
-    // the heavy pass stays on the binary tree: for a thin capsule its inner boxes cull more than a
-    // wide node's four child boxes (the wide warp descent tested 25-40 % more boxes, measured on
-    // the 4,096-trajectory sweeps)
     if (A.light_steps) {
         SweepArgs H = A;
         H.stats = A.stats + kStatBank;
-        const uint32_t hb = std::max(1u, heavy_blocks<QUAD, SURF>() * heavy_share / 100);
-        k_sweep_heavy<QUAD, SURF, false><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
-        cuda_check(cudaGetLastError(), "k_sweep_heavy");
-        if (A.heavy_steps) {
-            k_sweep_heavy<QUAD, SURF, true><<<hb, kHeavyWarps * 32, 0, s>>>(S, H);
-            cuda_check(cudaGetLastError(), "k_sweep_heavy (split)");
-        }
+        if (A.heavy_wide) launch_heavy<QUAD, SURF, true>(S, H, heavy_share, s);
+        else launch_heavy<QUAD, SURF, false>(S, H, heavy_share, s);
     }
 }
 

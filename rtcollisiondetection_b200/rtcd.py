@@ -68,7 +68,7 @@ class Config(C.Structure):
                 ('stage_b_form', C.c_uint32), ('stage_b_chunk', C.c_uint32), ('plain_streams', C.c_uint32),
                 ('top_nodes_shared', C.c_uint32), ('sweep_unstaged', C.c_uint32),
                 ('sweep_group', C.c_uint32), ('sweep_heavy_steps', C.c_uint32),
-                ('sweep_descend_cap', C.c_uint32)]
+                ('sweep_descend_cap', C.c_uint32), ('sweep_heavy_wide', C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -386,7 +386,7 @@ class Detector:
     def __init__(self, ctx, kind, robot, scene, frame_size=0, traverse_threads=0, traverse_blocks_per_sm=0,
                  stream_priority=0, residency_percent=0, light_steps=0, stage_b_form=0, stage_b_chunk=0,
                  plain_streams=0, top_nodes_shared=0, sweep_unstaged=0, sweep_group=0,
-                 sweep_heavy_steps=0, sweep_descend_cap=0):
+                 sweep_heavy_steps=0, sweep_descend_cap=0, sweep_heavy_wide=0):
         if isinstance(kind, str):
             kind = KIND_NAMES[kind]
         self.ctx, self.kind, self.robot, self.scene = ctx, kind, robot, scene
@@ -405,6 +405,7 @@ class Detector:
         cfg.sweep_group = sweep_group
         cfg.sweep_heavy_steps = sweep_heavy_steps
         cfg.sweep_descend_cap = sweep_descend_cap
+        cfg.sweep_heavy_wide = sweep_heavy_wide
         self.h = VP()
         _ok(lib().rtcd_detector_create(ctx.h, C.c_int(kind), robot.h, scene.h, C.byref(cfg), C.byref(self.h)))
 
@@ -466,7 +467,8 @@ class Detector:
                 'light_steps': best.light_steps, 'stage_b_form': best.stage_b_form,
                 'stage_b_chunk': best.stage_b_chunk, 'top_nodes_shared': best.top_nodes_shared,
                 'sweep_unstaged': best.sweep_unstaged, 'sweep_group': best.sweep_group,
-                'sweep_descend_cap': best.sweep_descend_cap, 'traverse_ms': ms.value}
+                'sweep_descend_cap': best.sweep_descend_cap, 'sweep_heavy_wide': best.sweep_heavy_wide,
+                'traverse_ms': ms.value}
 
     def stats(self):
         s = Stats()

@@ -339,3 +339,30 @@ def test_descend_cap_keeps_results(sweep_setup, panda, kind):
             det.close()
     for o in outs[1:]:
         assert all(np.array_equal(a, b) for a, b in zip(o, outs[0]))
+
+
+@pytest.mark.parametrize('kind', ['Linear', 'Quadratic'])
+@pytest.mark.parametrize('surface', [False, True])
+def test_wide_heavy_pass_keeps_results(sweep_setup, panda, kind, surface):
+    """The heavy and split passes on the 4-wide edge tree (four lanes per
+    node) give the binary tree's trajectory flags, segment flags and counts,
+    with a light budget small enough to send most units there and the split
+    pass forced on; the solid semantics also match the oracle."""
+    robot, scene, orob, osc = sweep_setup
+    n_wp = scenes.log_uniform_counts(160, 8, 40, seed=13)
+    q, off = scenes.random_walk_trajectories(panda, 160, n_wp, seed=13)
+    outs = []
+    for wide in (0, 1):
+        for heavy_steps in (1, 0xFFFFFFFF):
+            det = rtcd.Detector(robot.ctx, kind, robot, scene, light_steps=2, sweep_heavy_steps=heavy_steps,
+                                sweep_heavy_wide=wide)
+            seg = det.check(q, off, segments=True, surface=surface)
+            cnt = det.check(q, off, counts=True, surface=surface)
+            assert det.stats()['deferred'] > 0
+            outs.append((seg['flags'], seg['seg_flags'], cnt['counts']))
+            det.close()
+    for o in outs[1:]:
+        assert all(np.array_equal(a, b) for a, b in zip(o, outs[0]))
+    if not surface:
+        ref = O.sweep(kind == 'Quadratic', orob, osc, q, off)
+        _cmp({'flags': outs[0][0], 'counts': outs[0][2]}, ref)
